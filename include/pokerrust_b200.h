@@ -1,0 +1,109 @@
+/*
+ * pokerrust_b200: C ABI of the B200 river-subtree CFR solver.
+ *
+ * The first seven functions are the drop-in boundary: the same unmangled symbols, argument
+ * meaning and call protocol as the reference's CUDA library (src/cuda/interface.cu:9-122),
+ * as its Rust FFI binds them (src/cuda_interface.rs:8-31). The C side of the reference
+ * spells the 64-bit and 16-bit arguments `long` / `short`; on LP64 those are the same
+ * types as uint64_t / uint16_t here, which is how the Rust side declares them.
+ *
+ * The pr_* functions are extensions with no counterpart in the reference: status codes,
+ * device-resident entry points, state access for tests and checkpoints.
+ *
+ * Error convention: the reference prints CUDA errors and carries on. The drop-in symbols
+ * keep that (a line on stderr) and also record a sticky status that pr_last_error()
+ * returns; the pr_* functions return that status directly (0 = success).
+ */
+#ifndef POKERRUST_B200_H
+#define POKERRUST_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- drop-in boundary (src/cuda_interface.rs:8-31, src/cuda/interface.cu:9-122) ---- */
+
+/* Replaces init_builder (interface.cu:72-85, cuda_interface.rs:9): returns a
+ * library-owned builder. The reference sizes it for 63*49*9 subgames; this one grows as
+ * build_river_cuda adds subgames. */
+void *init_builder(void);
+
+/* Replaces upload_c (interface.cu:87-89, cuda_interface.rs:11): copies 1326 floats (the
+ * opponent range at river root `index`) into the builder's pinned staging. Safe to call
+ * from many threads at once for distinct indexes, as state.rs:340-341,380-387 does. */
+void upload_c(void *builder, int index, const float *v);
+
+/* Replaces download_c (interface.cu:91-93, cuda_interface.rs:12): copies the 1326 result
+ * values of river root `index` out of the staging. Thread-safe across distinct indexes. */
+void download_c(void *builder, int index, float *v);
+
+/* Replaces build_river_cuda (interface.cu:95-121, builder.cu:123-138,
+ * cuda_interface.rs:13): adds one river subgame (4-card board `cards`, equal bets `bet`)
+ * with zero regrets; returns its index, increasing from 0. Single-threaded init only. */
+int build_river_cuda(uint64_t cards, float bet, void *builder);
+
+/* Replaces transfer_flop_eval_cuda (interface.cu:50-68, cuda_interface.rs:14-21): takes
+ * the reference's packed per-board tables for `flop` (1326 slots of 1326+512 eval, 52*51
+ * collision and 1326 bucket entries, cuda_interface.rs:444-479) and returns an opaque
+ * handle to device tables. Caller buffers are copied, not kept. */
+void *transfer_flop_eval_cuda(uint64_t flop, const uint64_t *card_order,
+                              const uint16_t *card_indexes, const uint16_t *eval,
+                              const uint16_t *coll_vec, const uint16_t *abstractions);
+
+/* Replaces free_eval_cuda (interface.cu:69-71, cuda_interface.rs:22). */
+void free_eval_cuda(void *eval);
+
+/* Replaces evaluate_cuda (interface.cu:11-49, cuda_interface.rs:24-29): synchronous. Reads
+ * every subgame's opponent range from the staging, runs the river pass for
+ * `updating_player` (0 small, 1 big) and overwrites the staging with the results.
+ * calc_exploit = false: counterfactual values and a regret update of the updater's edges;
+ * true: best-response values, regrets untouched. */
+void evaluate_cuda(void *builder, void *eval, uint16_t updating_player, bool calc_exploit);
+
+/* ---- extensions (no counterpart in the reference) ---- */
+
+/* Sticky status of the last failing call on this process (0 = none), and its text. */
+int pr_last_error(void);
+const char *pr_error_string(int status);
+void pr_clear_error(void);
+
+/* evaluate_cuda with a status code. */
+int pr_evaluate(void *builder, void *eval, int updating_player, int calc_exploit);
+
+/* Device-resident pass: ranges / results are device pointers to n rows of 1328 floats
+ * (n = pr_builder_count), stream is a cudaStream_t (NULL = the builder's stream).
+ * Asynchronous: returns after the launch. */
+int pr_evaluate_device(void *builder, void *eval, int updating_player, int calc_exploit,
+                       const float *d_ranges, float *d_results, void *stream);
+
+/* Batch forms of upload_c / download_c for rows first .. first+count-1; v holds count
+ * rows of 1326 floats (the same copies the reference's caller makes one call at a time). */
+int pr_upload_batch(void *builder, int first, int count, const float *v);
+int pr_download_batch(void *builder, int first, int count, float *v);
+
+/* Number of river subgames in the builder, and the row stride (floats) of pr_* buffers. */
+int pr_builder_count(void *builder);
+int pr_range_stride(void);
+
+/* Bucket regrets, count * 26 * 256 floats in the reference's edge order
+ * (src/cuda/builder.cu:85-97 numbering). Host buffers; synchronous. */
+int pr_get_regrets(void *builder, float *out);
+int pr_set_regrets(void *builder, const float *in);
+
+/* Releases a builder (the reference never frees it). */
+void pr_free_builder(void *builder);
+
+/* Status of a table handle: 0, or the bit set of table inconsistencies found on upload. */
+int pr_eval_status(void *eval);
+
+/* Shared memory bytes the river kernel uses per CTA. */
+size_t pr_river_smem_bytes(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

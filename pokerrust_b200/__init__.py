@@ -1,0 +1,20 @@
+"""B200-native river-subtree CFR for the fixed-flop limit hold'em game of pokerrust.
+
+The CUDA library sits behind the reference's C ABI (include/pokerrust_b200.h);
+`pokerrust_b200.interface` mirrors the reference's Rust FFI wrapper
+(src/cuda_interface.rs) on top of it.
+"""
+from .interface import (  # noqa: F401
+    HANDS,
+    RANGE_STRIDE,
+    Builder,
+    PokerLibError,
+    build_river,
+    download_gpu,
+    evaluate_gpu,
+    free_eval,
+    initialize_builder,
+    lib,
+    transfer_flop_eval,
+    upload_gpu,
+)

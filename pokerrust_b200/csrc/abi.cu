@@ -1,0 +1,506 @@
+// C ABI of the solver: the reference's seven symbols (src/cuda/interface.cu:9-122) and the
+// pr_* extensions declared in include/pokerrust_b200.h.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "../../include/pokerrust_b200.h"
+#include "device_common.cuh"
+#include "layout.h"
+#include "pack_boards.h"
+#include "river_cfr.h"
+#include "river_tree.h"
+
+namespace prb {
+namespace {
+
+enum Status {
+    kOk = 0,
+    kErrCuda = 1,
+    kErrArg = 2,
+    kErrTables = 3,
+    kErrTree = 4,
+    kErrAlloc = 5,
+};
+
+std::atomic<int> g_status{0};
+std::atomic<int> g_cuda_error{0};
+
+int fail(int status, const char *what, cudaError_t e = cudaSuccess) {
+    g_status.store(status);
+    if (e != cudaSuccess) {
+        g_cuda_error.store((int)e);
+        fprintf(stderr, "pokerrust_b200: %s: %s\n", what, cudaGetErrorString(e));
+    } else {
+        fprintf(stderr, "pokerrust_b200: %s\n", what);
+    }
+    fflush(stderr);
+    return status;
+}
+
+// The river tree rebuilt from the reference's builder rules (src/cuda/builder.cu:8-121):
+// checks that the compiled tables of river_tree.h describe the same tree.
+struct HostState {
+    int terminal, action, actor, parent, nchild, child[3], edge[3];
+    float sb, bb;
+    bool dealt;
+};
+
+bool river_tree_matches() {
+    enum { Fold, Check, Call, Raise, DealRiver };
+    HostState st[kStates];
+    int nst = 1, ned = 0;
+    st[0] = HostState{kRiver, Call, 0, -1, 0, {-1, -1, -1}, {-1, -1, -1}, 0.f, 0.f, false};
+    struct Rec {
+        static void build(HostState *st, int *nst, int *ned, int s, int raises) {
+            int acts[3], na = 0;
+            switch (st[s].action) {
+                case Check: acts[0] = Call; acts[1] = Raise; na = 2; break;
+                case Call: if (!st[s].dealt) { acts[0] = DealRiver; na = 1; } break;
+                case Raise:
+                    acts[0] = Fold; acts[1] = Call; na = 2;
+                    if (raises < 4) acts[na++] = Raise;
+                    break;
+                case DealRiver: acts[0] = Check; acts[1] = Raise; na = 2; break;
+                default: break;
+            }
+            for (int i = 0; i < na; i++) {
+                if (*nst >= kStates) return;
+                HostState t = st[s];
+                const int a = acts[i];
+                t.actor = st[s].actor == 0 ? 1 : 0;
+                t.action = a;
+                t.nchild = 0;
+                t.parent = s;
+                const float other = st[s].actor == 0 ? st[s].bb : st[s].sb;
+                switch (a) {
+                    case Fold: t.terminal = st[s].actor == 0 ? kBBWins : kSBWins; break;
+                    case Check: t.terminal = kNonTerminal; break;
+                    case Call: t.terminal = st[s].dealt ? kShowdown : kRiver; t.sb = t.bb = other; break;
+                    case Raise:
+                        t.terminal = kNonTerminal;
+                        if (st[s].actor == 0) t.sb = st[s].bb + 2.0f; else t.bb = st[s].sb + 2.0f;
+                        break;
+                    case DealRiver: t.actor = 0; t.terminal = kNonTerminal; t.dealt = true; break;
+                }
+                const int c = (*nst)++;
+                st[c] = t;
+                build(st, nst, ned, c, a == Raise ? raises + 1 : 0);
+                const int k = st[s].nchild++;
+                st[s].child[k] = c;
+                st[s].edge[k] = st[s].terminal == kNonTerminal ? (*ned)++ : -1;
+            }
+        }
+    };
+    Rec::build(st, &nst, &ned, 0, 0);
+    if (nst != kStates || ned != kEdges) return false;
+    for (int s = 0; s < kStates; s++) {
+        if (st[s].terminal != kTerm(s) || st[s].parent != kParent(s) ||
+            st[s].nchild != kNChild(s) || st[s].sb != kSbOff(s) || st[s].bb != kBbOff(s))
+            return false;
+        if (st[s].terminal == kNonTerminal && st[s].actor != kActor(s)) return false;
+        for (int k = 0; k < st[s].nchild; k++)
+            if (st[s].child[k] != kChild(s, k) || st[s].edge[k] != kEdge(s, k)) return false;
+    }
+    return true;
+}
+
+struct Builder {
+    std::vector<SubgameDesc> desc;
+    int capacity = 0;
+    float *comm = nullptr;  // pinned staging, capacity rows of kRangeStride
+    // device state
+    int dev_count = 0, dev_capacity = 0;
+    SubgameDesc *d_desc = nullptr;
+    float *d_regrets = nullptr;
+    float *d_ranges = nullptr;
+    float *d_results = nullptr;
+    cudaStream_t stream = nullptr;
+    unsigned long long checked_flop = 0;  // boards validated against this flop
+    int checked_count = -1;
+};
+
+struct EvalTables {
+    unsigned long long flop = 0;
+    BoardPack *packs = nullptr;
+    uint16_t *d_eval = nullptr;
+    uint16_t *d_abstr = nullptr;
+    int *d_err = nullptr;
+    int status = 0;
+};
+
+// One table set kept for reuse: the reference transfers and frees the tables on every
+// iteration (game.rs:71,180), so allocations are recycled instead of repeated.
+std::mutex g_cache_mu;
+EvalTables *g_cache = nullptr;
+
+bool grow_staging(Builder *b, int need) {
+    if (need <= b->capacity) return true;
+    int cap = b->capacity ? b->capacity : 1024;
+    while (cap < need) cap *= 2;
+    float *fresh = nullptr;
+    cudaError_t e = cudaHostAlloc((void **)&fresh, (size_t)cap * kRangeStride * sizeof(float),
+                                  cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        fail(kErrAlloc, "pinned staging allocation", e);
+        return false;
+    }
+    memset(fresh, 0, (size_t)cap * kRangeStride * sizeof(float));
+    if (b->comm) {
+        memcpy(fresh, b->comm, (size_t)b->capacity * kRangeStride * sizeof(float));
+        cudaFreeHost(b->comm);
+    }
+    b->comm = fresh;
+    b->capacity = cap;
+    return true;
+}
+
+// Brings the device arrays up to the host's subgame count; new regrets start at zero
+// (interface.cu:78 zeroes them once at start-up).
+int sync_device(Builder *b) {
+    const int n = (int)b->desc.size();
+    cudaError_t e;
+    if (!b->stream) {
+        e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return fail(kErrCuda, "stream creation", e);
+    }
+    if (n > b->dev_capacity) {
+        int cap = b->dev_capacity ? b->dev_capacity : 1024;
+        while (cap < n) cap *= 2;
+        SubgameDesc *nd = nullptr;
+        float *nr = nullptr, *nrg = nullptr, *nres = nullptr;
+        const size_t rows = (size_t)cap * kRangeStride * sizeof(float);
+        const size_t regb = (size_t)cap * kEdges * kBuckets * sizeof(float);
+        if ((e = cudaMalloc(&nd, (size_t)cap * sizeof(SubgameDesc))) != cudaSuccess ||
+            (e = cudaMalloc(&nr, rows)) != cudaSuccess || (e = cudaMalloc(&nres, rows)) != cudaSuccess ||
+            (e = cudaMalloc(&nrg, regb)) != cudaSuccess) {
+            cudaFree(nd);
+            cudaFree(nr);
+            cudaFree(nres);
+            cudaFree(nrg);
+            return fail(kErrAlloc, "device allocation", e);
+        }
+        cudaMemsetAsync(nrg, 0, regb, b->stream);
+        if (b->d_regrets)
+            cudaMemcpyAsync(nrg, b->d_regrets, (size_t)b->dev_count * kEdges * kBuckets * sizeof(float),
+                            cudaMemcpyDeviceToDevice, b->stream);
+        cudaStreamSynchronize(b->stream);
+        cudaFree(b->d_desc);
+        cudaFree(b->d_ranges);
+        cudaFree(b->d_results);
+        cudaFree(b->d_regrets);
+        b->d_desc = nd;
+        b->d_ranges = nr;
+        b->d_results = nres;
+        b->d_regrets = nrg;
+        b->dev_capacity = cap;
+    }
+    if (n != b->dev_count) {
+        e = cudaMemcpyAsync(b->d_desc, b->desc.data(), (size_t)n * sizeof(SubgameDesc),
+                            cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) return fail(kErrCuda, "descriptor upload", e);
+        b->dev_count = n;
+    }
+    return kOk;
+}
+
+int evaluate_impl(Builder *b, EvalTables *t, int player, int exploit, const float *d_in, float *d_out,
+                  cudaStream_t stream, bool staged) {
+    if (!b || !t) return fail(kErrArg, "evaluate: null builder or tables");
+    if (t->status) return fail(kErrTables, "evaluate: tables failed validation on upload");
+    if (player != 0 && player != 1) return fail(kErrArg, "evaluate: updating_player must be 0 or 1");
+    if (b->checked_flop != t->flop || b->checked_count != (int)b->desc.size()) {
+        // every river root must extend the tables' flop by one turn card, so that each
+        // {turn, river} slot the kernel reads is one the re-pack filled
+        for (const SubgameDesc &d : b->desc)
+            if ((d.board4 & t->flop) != t->flop || __builtin_popcountll(d.board4) != 4)
+                return fail(kErrArg, "evaluate: a river root's board does not contain the flop");
+        b->checked_flop = t->flop;
+        b->checked_count = (int)b->desc.size();
+    }
+    int st = sync_device(b);
+    if (st) return st;
+    const int n = b->dev_count;
+    if (n == 0) return kOk;
+    cudaStream_t s = stream ? stream : b->stream;
+    cudaError_t e;
+    if (staged) {
+        e = cudaMemcpyAsync(b->d_ranges, b->comm, (size_t)n * kRangeStride * sizeof(float),
+                            cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return fail(kErrCuda, "range upload", e);
+        d_in = b->d_ranges;
+        d_out = b->d_results;
+    }
+    e = launch_river(exploit ? kModeBR : kModeCFR, b->d_desc, n, d_in, d_out, b->d_regrets, t->packs,
+                     t->flop, player, s);
+    if (e != cudaSuccess) return fail(kErrCuda, "river kernel launch", e);
+    if (staged) {
+        e = cudaMemcpyAsync(b->comm, b->d_results, (size_t)n * kRangeStride * sizeof(float),
+                            cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) return fail(kErrCuda, "result download", e);
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return fail(kErrCuda, "river pass", e);
+    }
+    return kOk;
+}
+
+bool card_order_ok(const uint64_t *card_order, const uint16_t *card_indexes) {
+    // The kernels index hands by the colex order of their two cards (evaluator.rs:29-40)
+    // and the per-card lists by card_indexes (evaluator.rs:159-172).
+    int n = 0, fill[52] = {0};
+    for (int hi = 1; hi < 52; hi++)
+        for (int lo = 0; lo < hi; lo++, n++)
+            if (card_order[n] != ((1ull << lo) | (1ull << hi))) return false;
+    for (int i = 0; i < kHands; i++) {
+        const int lo = ctz64(card_order[i]);
+        const int hi = ctz64(card_order[i] & (card_order[i] - 1));
+        if (card_indexes[lo * 51 + fill[lo]++] != i) return false;
+        if (card_indexes[hi * 51 + fill[hi]++] != i) return false;
+    }
+    return true;
+}
+
+}  // namespace
+}  // namespace prb
+
+using namespace prb;
+
+extern "C" {
+
+void *init_builder(void) {
+    if (!river_tree_matches()) {
+        fail(kErrTree, "river tree tables disagree with the builder rules");
+        return nullptr;
+    }
+    Builder *b = new Builder();
+    if (!grow_staging(b, 1)) {
+        delete b;
+        return nullptr;
+    }
+    return b;
+}
+
+void upload_c(void *builder, int index, const float *v) {
+    Builder *b = (Builder *)builder;
+    if (!b || index < 0 || index >= (int)b->desc.size() || !v) {
+        fail(kErrArg, "upload_c: bad builder or index");
+        return;
+    }
+    memcpy(b->comm + (size_t)index * kRangeStride, v, kHands * sizeof(float));
+}
+
+void download_c(void *builder, int index, float *v) {
+    Builder *b = (Builder *)builder;
+    if (!b || index < 0 || index >= (int)b->desc.size() || !v) {
+        fail(kErrArg, "download_c: bad builder or index");
+        return;
+    }
+    memcpy(v, b->comm + (size_t)index * kRangeStride, kHands * sizeof(float));
+}
+
+int build_river_cuda(uint64_t cards, float bet, void *builder) {
+    Builder *b = (Builder *)builder;
+    if (!b) {
+        fail(kErrArg, "build_river_cuda: null builder");
+        return -1;
+    }
+    if (__builtin_popcountll(cards) != 4 || (cards >> 52)) {
+        fail(kErrArg, "build_river_cuda: a river root needs a 4-card board");
+        return -1;
+    }
+    const int idx = (int)b->desc.size();
+    if (!grow_staging(b, idx + 1)) return -1;
+    SubgameDesc d;
+    d.board4 = cards;
+    d.bet = bet;
+    d.pad = 0;
+    b->desc.push_back(d);
+    return idx;
+}
+
+void *transfer_flop_eval_cuda(uint64_t flop, const uint64_t *card_order, const uint16_t *card_indexes,
+                              const uint16_t *eval, const uint16_t *coll_vec, const uint16_t *abstractions) {
+    (void)coll_vec;  // rebuilt on the device from the sort order
+    EvalTables *t = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        t = g_cache;
+        g_cache = nullptr;
+    }
+    cudaError_t e;
+    if (!t) {
+        t = new EvalTables();
+        if ((e = cudaMalloc(&t->packs, (size_t)kSlotsPerBoard * sizeof(BoardPack))) != cudaSuccess ||
+            (e = cudaMalloc(&t->d_eval, (size_t)kSlotsPerBoard * (1326 + 512) * sizeof(uint16_t))) !=
+                cudaSuccess ||
+            (e = cudaMalloc(&t->d_abstr, (size_t)kSlotsPerBoard * kHands * sizeof(uint16_t))) !=
+                cudaSuccess ||
+            (e = cudaMalloc(&t->d_err, sizeof(int))) != cudaSuccess) {
+            fail(kErrAlloc, "table allocation", e);
+            t->status = -1;
+            return t;
+        }
+        // slots the re-pack never writes (pairs that overlap the flop) stay all-zero
+        if ((e = cudaMemset(t->packs, 0, (size_t)kSlotsPerBoard * sizeof(BoardPack))) != cudaSuccess) {
+            fail(kErrCuda, "table initialisation", e);
+            t->status = -1;
+            return t;
+        }
+    }
+    t->flop = flop;
+    t->status = 0;
+    if (__builtin_popcountll(flop) != 3 || (flop >> 52) || !card_order || !card_indexes || !eval ||
+        !abstractions) {
+        fail(kErrArg, "transfer_flop_eval_cuda: bad flop or null table");
+        t->status = 32;
+        return t;
+    }
+    if (!card_order_ok(card_order, card_indexes)) {
+        fail(kErrTables, "transfer_flop_eval_cuda: card_order / card_indexes not in colex order");
+        t->status = 64;
+        return t;
+    }
+    if ((e = cudaMemcpy(t->d_eval, eval, (size_t)kSlotsPerBoard * (1326 + 512) * sizeof(uint16_t),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(t->d_abstr, abstractions, (size_t)kSlotsPerBoard * kHands * sizeof(uint16_t),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemset(t->d_err, 0, sizeof(int))) != cudaSuccess) {
+        fail(kErrCuda, "table upload", e);
+        t->status = -1;
+        return t;
+    }
+    launch_pack_boards(flop, t->d_eval, t->d_abstr, t->packs, t->d_err, 0);
+    int err = 0;
+    if ((e = cudaMemcpy(&err, t->d_err, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+        fail(kErrCuda, "table re-pack", e);
+        t->status = -1;
+        return t;
+    }
+    if (err) {
+        fail(kErrTables, "transfer_flop_eval_cuda: tables are not a consistent rank order");
+        t->status = err;
+    }
+    return t;
+}
+
+void free_eval_cuda(void *eval) {
+    EvalTables *t = (EvalTables *)eval;
+    if (!t) return;
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (!g_cache && t->packs) {
+        g_cache = t;
+        return;
+    }
+    cudaFree(t->packs);
+    cudaFree(t->d_eval);
+    cudaFree(t->d_abstr);
+    cudaFree(t->d_err);
+    delete t;
+}
+
+void evaluate_cuda(void *builder, void *eval, uint16_t updating_player, bool calc_exploit) {
+    evaluate_impl((Builder *)builder, (EvalTables *)eval, (int)updating_player, calc_exploit ? 1 : 0,
+                  nullptr, nullptr, nullptr, true);
+}
+
+int pr_last_error(void) { return g_status.load(); }
+
+void pr_clear_error(void) {
+    g_status.store(0);
+    g_cuda_error.store(0);
+}
+
+const char *pr_error_string(int status) {
+    switch (status) {
+        case kOk: return "ok";
+        case kErrCuda: return cudaGetErrorString((cudaError_t)g_cuda_error.load());
+        case kErrArg: return "invalid argument";
+        case kErrTables: return "inconsistent hand-rank tables";
+        case kErrTree: return "river tree tables disagree with the builder rules";
+        case kErrAlloc: return "allocation failed";
+        default: return "unknown status";
+    }
+}
+
+int pr_evaluate(void *builder, void *eval, int updating_player, int calc_exploit) {
+    return evaluate_impl((Builder *)builder, (EvalTables *)eval, updating_player, calc_exploit, nullptr,
+                         nullptr, nullptr, true);
+}
+
+int pr_evaluate_device(void *builder, void *eval, int updating_player, int calc_exploit,
+                       const float *d_ranges, float *d_results, void *stream) {
+    if (!d_ranges || !d_results) return fail(kErrArg, "pr_evaluate_device: null buffer");
+    return evaluate_impl((Builder *)builder, (EvalTables *)eval, updating_player, calc_exploit, d_ranges,
+                         d_results, (cudaStream_t)stream, false);
+}
+
+int pr_upload_batch(void *builder, int first, int count, const float *v) {
+    Builder *b = (Builder *)builder;
+    if (!b || !v || first < 0 || count < 0 || first + count > (int)b->desc.size())
+        return fail(kErrArg, "pr_upload_batch: bad builder or range");
+    for (int i = 0; i < count; i++)
+        memcpy(b->comm + (size_t)(first + i) * kRangeStride, v + (size_t)i * kHands, kHands * sizeof(float));
+    return kOk;
+}
+
+int pr_download_batch(void *builder, int first, int count, float *v) {
+    Builder *b = (Builder *)builder;
+    if (!b || !v || first < 0 || count < 0 || first + count > (int)b->desc.size())
+        return fail(kErrArg, "pr_download_batch: bad builder or range");
+    for (int i = 0; i < count; i++)
+        memcpy(v + (size_t)i * kHands, b->comm + (size_t)(first + i) * kRangeStride, kHands * sizeof(float));
+    return kOk;
+}
+
+int pr_builder_count(void *builder) { return builder ? (int)((Builder *)builder)->desc.size() : 0; }
+
+int pr_range_stride(void) { return kRangeStride; }
+
+int pr_get_regrets(void *builder, float *out) {
+    Builder *b = (Builder *)builder;
+    if (!b || !out) return fail(kErrArg, "pr_get_regrets: null argument");
+    int st = sync_device(b);
+    if (st) return st;
+    cudaError_t e = cudaMemcpyAsync(out, b->d_regrets, (size_t)b->dev_count * kEdges * kBuckets * sizeof(float),
+                                    cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return fail(kErrCuda, "regret download", e);
+    return kOk;
+}
+
+int pr_set_regrets(void *builder, const float *in) {
+    Builder *b = (Builder *)builder;
+    if (!b || !in) return fail(kErrArg, "pr_set_regrets: null argument");
+    int st = sync_device(b);
+    if (st) return st;
+    cudaError_t e = cudaMemcpyAsync(b->d_regrets, in, (size_t)b->dev_count * kEdges * kBuckets * sizeof(float),
+                                    cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return fail(kErrCuda, "regret upload", e);
+    return kOk;
+}
+
+void pr_free_builder(void *builder) {
+    Builder *b = (Builder *)builder;
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    cudaFree(b->d_desc);
+    cudaFree(b->d_ranges);
+    cudaFree(b->d_results);
+    cudaFree(b->d_regrets);
+    if (b->comm) cudaFreeHost(b->comm);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int pr_eval_status(void *eval) { return eval ? ((EvalTables *)eval)->status : -1; }
+
+size_t pr_river_smem_bytes(void) { return river_smem_bytes(); }
+
+}  // extern "C"

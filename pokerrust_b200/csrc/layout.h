@@ -1,0 +1,54 @@
+// Device data layout of the river solver.
+//
+// Board tables. The reference hands the GPU, per {turn, river} slot, the rank-sorted hand
+// order as an inverse permutation with group-start flags, per-card collision lists and
+// the bucket of every hand (src/cuda_interface.rs:48-102, src/cuda/evaluator.cuh:8-15).
+// transfer_flop_eval_cuda keeps that interface and re-packs the tables once on the device
+// into BoardPack, a layout built for the river kernel:
+//   - only the 1081 hands that share no card with the five board cards ("live" hands)
+//     appear; blocked hands have zero reach in every reference code path;
+//   - the live hands in rank order ("global list"), each with its bucket;
+//   - for each of the 47 cards not on the board, the 46 live hands holding it, in rank
+//     order ("card lists"); these give the blocker corrections of a showdown;
+//   - for each live hand the slots of its tie group in the global list and in its two
+//     card lists, so that a showdown value is a handful of prefix-sum lookups.
+#pragma once
+#include <stdint.h>
+
+namespace prb {
+
+constexpr int kHands = 1326;
+constexpr int kRangeStride = 1328;  // floats per range / result row (16-byte rows)
+constexpr int kBlocked = 245;       // hands sharing a card with a 5-card board
+constexpr int kLive = 1081;         // C(47, 2)
+constexpr int kGSlots = 1088;       // global list slots: 1081 hands, end sentinel, padding
+constexpr int kNumLists = 47;       // cards not on the board
+constexpr int kLSlots = 48;         // card list slots: 46 hands, end sentinel, padding
+constexpr int kListLen = 46;
+constexpr int kSlotsPerBoard = 1326;  // colex index of the {turn, river} pair
+
+// Element word of a list slot: hand | bucket << 11 | valid << 19.
+constexpr uint32_t kElemValid = 1u << 19;
+
+struct BoardPack {
+    // Per live hand in rank order (index l = sorted position - 245):
+    //  x: hand | bucket << 11 | low card << 19 | high card << 25
+    //  y: tie-group start slot | group end slot << 16      (global list, end = 1081)
+    //  z: same for the low card's list, slots counted from the start of the card lists
+    //  w: same for the high card's list
+    uint4 meta[kGSlots];
+    uint32_t gelem[kGSlots];               // global list elements
+    uint32_t celem[kNumLists * kLSlots];   // card list elements
+    uint8_t list_card[64];                 // card of each card list
+};
+
+static_assert(sizeof(BoardPack) % 16 == 0, "BoardPack rows must stay 16-byte aligned");
+
+// Per-subgame descriptor (one river root built by build_river_cuda).
+struct SubgameDesc {
+    unsigned long long board4;  // flop + turn
+    float bet;                  // equal bets at the river root
+    int pad;
+};
+
+}  // namespace prb

@@ -1,0 +1,198 @@
+"""Host-side mirror of the reference's Rust FFI wrapper (src/cuda_interface.rs:8-123),
+over the C ABI of include/pokerrust_b200.h.
+
+Function names, argument meaning and call order follow cuda_interface.rs:
+initialize_builder / build_river at game construction, transfer_flop_eval + free_eval
+around every iteration, upload_gpu / download_gpu per river root and evaluate_gpu per
+half-iteration. There is no CPU fallback: loading fails loudly when the CUDA library has
+not been built.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .build import SO_PATH
+
+HANDS = 1326
+RANGE_STRIDE = 1328
+EDGES = 26
+BUCKETS = 256
+
+_lib = None
+
+
+class PokerLibError(RuntimeError):
+    pass
+
+
+def lib():
+    """The loaded CUDA library (pokerrust_b200/_lib/libpokerrust_b200.so)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO_PATH):
+            raise PokerLibError(
+                f"{SO_PATH} is missing: build it with `python -m pokerrust_b200.build` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(SO_PATH)
+        vp, u64, u16, f32, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint16, ctypes.c_float, ctypes.c_int
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.init_builder.restype = vp
+        L.init_builder.argtypes = []
+        L.upload_c.argtypes = [vp, i32, fp]
+        L.download_c.argtypes = [vp, i32, fp]
+        L.build_river_cuda.restype = i32
+        L.build_river_cuda.argtypes = [u64, f32, vp]
+        L.transfer_flop_eval_cuda.restype = vp
+        L.transfer_flop_eval_cuda.argtypes = [u64, vp, vp, vp, vp, vp]
+        L.free_eval_cuda.argtypes = [vp]
+        L.evaluate_cuda.argtypes = [vp, vp, u16, ctypes.c_bool]
+        L.pr_last_error.restype = i32
+        L.pr_error_string.restype = ctypes.c_char_p
+        L.pr_error_string.argtypes = [i32]
+        L.pr_evaluate.restype = i32
+        L.pr_evaluate.argtypes = [vp, vp, i32, i32]
+        L.pr_evaluate_device.restype = i32
+        L.pr_evaluate_device.argtypes = [vp, vp, i32, i32, vp, vp, vp]
+        L.pr_upload_batch.restype = i32
+        L.pr_upload_batch.argtypes = [vp, i32, i32, vp]
+        L.pr_download_batch.restype = i32
+        L.pr_download_batch.argtypes = [vp, i32, i32, vp]
+        L.pr_builder_count.restype = i32
+        L.pr_builder_count.argtypes = [vp]
+        L.pr_range_stride.restype = i32
+        L.pr_get_regrets.restype = i32
+        L.pr_get_regrets.argtypes = [vp, vp]
+        L.pr_set_regrets.restype = i32
+        L.pr_set_regrets.argtypes = [vp, vp]
+        L.pr_free_builder.argtypes = [vp]
+        L.pr_eval_status.restype = i32
+        L.pr_eval_status.argtypes = [vp]
+        L.pr_river_smem_bytes.restype = ctypes.c_size_t
+        _lib = L
+    return _lib
+
+
+def _check(status, what):
+    if status != 0:
+        raise PokerLibError(f"{what}: {lib().pr_error_string(status).decode()} (status {status})")
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def initialize_builder():
+    """cuda_interface.rs:432-434."""
+    p = lib().init_builder()
+    if not p:
+        _check(lib().pr_last_error() or 1, "init_builder")
+    return p
+
+
+def build_river(cards, bet, builder):
+    """cuda_interface.rs:435-437: adds a river root, returns its index."""
+    idx = lib().build_river_cuda(int(cards), float(bet), builder)
+    if idx < 0:
+        _check(lib().pr_last_error() or 2, "build_river_cuda")
+    return idx
+
+
+def upload_gpu(builder, index, v):
+    """cuda_interface.rs:423-425."""
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    assert v.shape == (HANDS,)
+    lib().upload_c(builder, int(index), v.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+
+
+def download_gpu(builder, index):
+    """cuda_interface.rs:427-431."""
+    out = np.zeros(HANDS, dtype=np.float32)
+    lib().download_c(builder, int(index), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+    return out
+
+
+def transfer_flop_eval(flop, card_order, card_indexes, eval_tables, coll_vec, abstractions):
+    """cuda_interface.rs:438-492 after packing: the packed tables of all 1326 {turn, river}
+    slots for `flop` (1326*1838, 1326*2652 and 1326*1326 u16) go to the device."""
+    card_order = np.ascontiguousarray(card_order, dtype=np.uint64)
+    card_indexes = np.ascontiguousarray(card_indexes, dtype=np.uint16)
+    eval_tables = np.ascontiguousarray(eval_tables, dtype=np.uint16)
+    coll_vec = np.ascontiguousarray(coll_vec, dtype=np.uint16)
+    abstractions = np.ascontiguousarray(abstractions, dtype=np.uint16)
+    assert card_order.size == HANDS and card_indexes.size == 52 * 51
+    assert eval_tables.size == HANDS * (HANDS + 512)
+    assert coll_vec.size == HANDS * 52 * 51 and abstractions.size == HANDS * HANDS
+    p = lib().transfer_flop_eval_cuda(int(flop), _ptr(card_order), _ptr(card_indexes), _ptr(eval_tables),
+                                      _ptr(coll_vec), _ptr(abstractions))
+    st = lib().pr_eval_status(p)
+    if st != 0:
+        lib().free_eval_cuda(p)
+        raise PokerLibError(f"transfer_flop_eval_cuda rejected the tables (bits {st})")
+    return p
+
+
+def free_eval(ptr):
+    """cuda_interface.rs:494-498."""
+    lib().free_eval_cuda(ptr)
+
+
+def evaluate_gpu(builder, evaluator, updating_player, calc_exploit):
+    """cuda_interface.rs:500-513; updating_player is 0 (small) or 1 (big)."""
+    lib().pr_clear_error()
+    lib().evaluate_cuda(builder, evaluator, int(updating_player), bool(calc_exploit))
+    _check(lib().pr_last_error(), "evaluate_cuda")
+
+
+class Builder:
+    """Owning wrapper with batch access, for drivers and tests."""
+
+    def __init__(self):
+        self.ptr = initialize_builder()
+
+    def add(self, cards, bet):
+        return build_river(cards, bet, self.ptr)
+
+    @property
+    def count(self):
+        return lib().pr_builder_count(self.ptr)
+
+    def upload_all(self, ranges):
+        ranges = np.ascontiguousarray(ranges, dtype=np.float32)
+        assert ranges.shape == (self.count, HANDS)
+        _check(lib().pr_upload_batch(self.ptr, 0, self.count, _ptr(ranges)), "pr_upload_batch")
+
+    def download_all(self):
+        out = np.zeros((self.count, HANDS), dtype=np.float32)
+        _check(lib().pr_download_batch(self.ptr, 0, self.count, _ptr(out)), "pr_download_batch")
+        return out
+
+    def regrets(self):
+        out = np.zeros((self.count, EDGES, BUCKETS), dtype=np.float32)
+        _check(lib().pr_get_regrets(self.ptr, _ptr(out)), "pr_get_regrets")
+        return out
+
+    def set_regrets(self, regrets):
+        regrets = np.ascontiguousarray(regrets, dtype=np.float32)
+        assert regrets.shape == (self.count, EDGES, BUCKETS)
+        _check(lib().pr_set_regrets(self.ptr, _ptr(regrets)), "pr_set_regrets")
+
+    def evaluate(self, tables, updating_player, calc_exploit=False):
+        _check(lib().pr_evaluate(self.ptr, tables, int(updating_player), int(bool(calc_exploit))), "pr_evaluate")
+
+    def evaluate_device(self, tables, updating_player, calc_exploit, d_ranges, d_results, stream=None):
+        _check(lib().pr_evaluate_device(self.ptr, tables, int(updating_player), int(bool(calc_exploit)),
+                                        ctypes.c_void_p(d_ranges), ctypes.c_void_p(d_results),
+                                        ctypes.c_void_p(stream) if stream else None),
+               "pr_evaluate_device")
+
+    def close(self):
+        if self.ptr:
+            lib().pr_free_builder(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

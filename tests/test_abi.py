@@ -1,0 +1,62 @@
+"""The C-ABI library loads and exports every symbol include/pokerrust_b200.h declares
+(no GPU calls)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "pokerrust_b200.h")
+
+REFERENCE_SYMBOLS = ["init_builder", "upload_c", "download_c", "build_river_cuda",
+                     "transfer_flop_eval_cuda", "free_eval_cuda", "evaluate_cuda"]
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{]*\)\s*;", text)
+
+
+@pytest.fixture(scope="module")
+def so_path():
+    from pokerrust_b200.build import SO_PATH, build
+    build()
+    return SO_PATH
+
+
+def test_header_declares_reference_boundary():
+    fns = declared_functions()
+    for s in REFERENCE_SYMBOLS:
+        assert s in fns
+
+
+def test_library_exports_every_declared_symbol(so_path):
+    lib = ctypes.CDLL(so_path)
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_exports_are_unmangled_c_symbols(so_path):
+    out = subprocess.run(["nm", "-D", "--defined-only", so_path], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    for name in declared_functions():
+        assert name in exported, name
+
+
+def test_static_archive_for_rust_build(so_path):
+    from pokerrust_b200.build import A_PATH
+    out = subprocess.run(["nm", "--defined-only", A_PATH], capture_output=True, text=True,
+                         check=True).stdout
+    for s in REFERENCE_SYMBOLS:
+        assert re.search(rf" T {s}$", out, re.M), s
+
+
+def test_error_strings_without_gpu(so_path):
+    from pokerrust_b200 import lib
+    assert lib().pr_error_string(0) == b"ok"
+    assert lib().pr_range_stride() == 1328
+    assert lib().pr_river_smem_bytes() <= 227 * 1024

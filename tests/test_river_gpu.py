@@ -1,0 +1,185 @@
+"""Parity of the CUDA river solver with the oracle (CPU restatement of state.rs:377-433),
+through the C ABI.
+
+Tolerance: results and regrets are f32 sums of up to ~10^5 terms computed in a different
+order from the reference; per subgame we require
+    max |gpu - oracle| <= 1e-4 * max |oracle|
+(the north-star bound of 1e-4 relative), measured against the largest value of that
+subgame's vector so that entries that cancel to ~0 do not turn rounding into a false
+failure.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def P():
+    import pokerrust_b200 as P
+    P.lib()
+    return P
+
+
+@pytest.fixture(scope="module")
+def gpu_tables(P, flop_tables):
+    e, c, a = flop_tables
+    h = P.transfer_flop_eval(O.REFERENCE_FLOP, O.card_order(), O.card_indexes(), e, c, a)
+    yield h
+    P.free_eval(h)
+
+
+def subgames(rng, n, turns=None):
+    order = O.card_order()
+    flop = O.REFERENCE_FLOP
+    free = [c for c in range(52) if not (flop >> c) & 1]
+    if turns is None:
+        turns = rng.choice(free, n)
+    board4 = np.array([flop | (1 << int(t)) for t in turns], np.uint64)
+    bet = rng.choice(np.arange(1, 17), len(board4)).astype(np.float32)
+    opp = rng.random((len(board4), 1326)).astype(np.float32)
+    opp[rng.random(opp.shape) < 0.2] = 0.0
+    for i in range(len(board4)):
+        opp[i][(order & board4[i]) != 0] = 0
+    return board4, bet, opp
+
+
+def random_regrets(rng, n):
+    reg = (rng.random((n, 26, 256)) * 50).astype(np.float32)
+    reg[rng.random(reg.shape) < 0.3] = 0.0
+    reg[:, :, :8] = 0.0                         # all-zero buckets: the 1e-4 cutoff path
+    return reg
+
+
+def assert_close(got, want, what):
+    for i in range(len(want)):
+        scale = float(np.abs(want[i]).max())
+        err = float(np.abs(got[i] - want[i]).max())
+        assert err <= TOL * max(scale, 1e-30), f"{what}[{i}]: max err {err:.3e} vs scale {scale:.3e}"
+
+
+def run_both(P, gpu_tables, flop_tables, board4, bet, opp, reg, player, exploit):
+    e, _, a = flop_tables
+    b = P.Builder()
+    for cards, bt in zip(board4, bet):
+        b.add(int(cards), float(bt))
+    b.set_regrets(reg)
+    b.upload_all(opp)
+    P.evaluate_gpu(b.ptr, gpu_tables, player, exploit)
+    got = b.download_all()
+    got_reg = b.regrets()
+    ref_reg = reg.copy()
+    want = O.river_batch(O.REFERENCE_FLOP, e, a, board4, bet, opp, ref_reg, player, exploit)
+    b.close()
+    return got, want, got_reg, ref_reg
+
+
+@pytest.mark.parametrize("player", [0, 1])
+@pytest.mark.parametrize("exploit", [False, True])
+def test_one_pass_random_regrets(P, gpu_tables, flop_tables, player, exploit):
+    rng = np.random.default_rng(10 + player + 2 * exploit)
+    board4, bet, opp = subgames(rng, 12)
+    reg = random_regrets(rng, 12)
+    got, want, got_reg, ref_reg = run_both(P, gpu_tables, flop_tables, board4, bet, opp, reg, player, exploit)
+    assert_close(got, want, "values")
+    if exploit:
+        assert np.array_equal(got_reg, reg)
+    else:
+        assert_close(got_reg.reshape(12, -1), ref_reg.reshape(12, -1), "regrets")
+
+
+def test_one_pass_from_zero_regrets(P, gpu_tables, flop_tables):
+    # the reference's starting point: all regrets zero, uniform strategies everywhere
+    rng = np.random.default_rng(7)
+    board4, bet, opp = subgames(rng, 8)
+    reg = np.zeros((8, 26, 256), np.float32)
+    got, want, got_reg, ref_reg = run_both(P, gpu_tables, flop_tables, board4, bet, opp, reg, 0, False)
+    assert_close(got, want, "values")
+    assert_close(got_reg.reshape(8, -1), ref_reg.reshape(8, -1), "regrets")
+
+
+def test_blocked_and_masked_hands(P, gpu_tables, flop_tables):
+    # hands sharing a card with the turn board get exactly zero, whatever range they carry
+    rng = np.random.default_rng(8)
+    order = O.card_order()
+    board4, bet, opp = subgames(rng, 4)
+    opp_dirty = opp.copy()
+    opp_dirty[:, :] += 1.0                       # nonzero range on blocked hands too
+    got, want, _, _ = run_both(P, gpu_tables, flop_tables, board4, bet, opp_dirty,
+                               random_regrets(rng, 4), 1, False)
+    for i in range(4):
+        blocked = (order & board4[i]) != 0
+        assert np.all(got[i][blocked] == 0.0)
+    assert_close(got, want, "values")
+
+
+def test_iterations_alternating_players(P, gpu_tables, flop_tables):
+    # 100 CFR iterations (SB update then BB update, game.rs:68-119) on fixed ranges
+    rng = np.random.default_rng(11)
+    n = 6
+    board4, bet, opp_bb = subgames(rng, n)
+    _, _, opp_sb = subgames(rng, n, turns=[(int(b) ^ O.REFERENCE_FLOP).bit_length() - 1 for b in board4])
+    e, _, a = flop_tables
+    b = P.Builder()
+    for cards, bt in zip(board4, bet):
+        b.add(int(cards), float(bt))
+    ref_reg = np.zeros((n, 26, 256), np.float32)
+    for it in range(100):
+        for player, opp in ((0, opp_bb), (1, opp_sb)):
+            b.upload_all(opp)
+            P.evaluate_gpu(b.ptr, gpu_tables, player, False)
+            got = b.download_all()
+            want = O.river_batch(O.REFERENCE_FLOP, e, a, board4, bet, opp, ref_reg, player, False)
+    assert_close(got, want, "values after 100 iterations")
+    assert_close(b.regrets().reshape(n, -1), ref_reg.reshape(n, -1), "regrets after 100 iterations")
+    b.close()
+
+
+def test_one_turn_card_all_river_roots(P, gpu_tables, flop_tables):
+    # the reduced case: every river root of one turn card (63 * 9 = 567 subgames)
+    g = O.Game(O.REFERENCE_FLOP)
+    boards, bets = g.river_roots()
+    turn = boards[0]
+    sel = np.nonzero(boards == turn)[0]
+    assert len(sel) == 567
+    rng = np.random.default_rng(12)
+    _, _, opp = subgames(rng, len(sel), turns=[(int(turn) ^ O.REFERENCE_FLOP).bit_length() - 1] * len(sel))
+    reg = random_regrets(rng, len(sel))
+    got, want, got_reg, ref_reg = run_both(P, gpu_tables, flop_tables, boards[sel], bets[sel], opp, reg, 0, False)
+    assert_close(got, want, "values")
+    assert_close(got_reg.reshape(len(sel), -1), ref_reg.reshape(len(sel), -1), "regrets")
+
+
+def test_full_fixed_flop_pass_sampled(P, gpu_tables, flop_tables):
+    # all 27,783 river roots of the fixed-flop game in one launch; 48 of them re-checked
+    g = O.Game(O.REFERENCE_FLOP)
+    boards, bets = g.river_roots()
+    n = len(boards)
+    rng = np.random.default_rng(13)
+    order = O.card_order()
+    opp = rng.random((n, 1326)).astype(np.float32)
+    opp[(order[None, :] & boards[:, None]) != 0] = 0
+    reg = random_regrets(rng, n)
+    e, _, a = flop_tables
+    b = P.Builder()
+    for cards, bt in zip(boards, bets):
+        b.add(int(cards), float(bt))
+    b.set_regrets(reg)
+    b.upload_all(opp)
+    P.evaluate_gpu(b.ptr, gpu_tables, 1, False)
+    got = b.download_all()
+    got_reg = b.regrets()
+    b.close()
+    sample = rng.choice(n, 48, replace=False)
+    ref_reg = reg[sample].copy()
+    want = O.river_batch(O.REFERENCE_FLOP, e, a, boards[sample], bets[sample], opp[sample], ref_reg, 1, False)
+    assert_close(got[sample], want, "values")
+    assert_close(got_reg[sample].reshape(48, -1), ref_reg.reshape(48, -1), "regrets")
+    # size-independent properties on all roots: finite, blocked hands zero, regrets >= 0
+    assert np.all(np.isfinite(got))
+    assert np.all(got[(order[None, :] & boards[:, None]) != 0] == 0)
+    assert np.all(got_reg >= 0)
