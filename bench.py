@@ -193,7 +193,8 @@ def run_gpu(args):
     d_ranges = torch.zeros((n, stride), dtype=torch.float32, device=dev)
     d_ranges[:, :1326] = torch.from_numpy(ranges).to(dev)
     d_results = torch.zeros((n, stride), dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # a real stream handle: the library launches on it
+    torch.cuda.set_stream(stream)
 
     def step(i):
         builder.evaluate_device(tables, i % 2, False, d_ranges.data_ptr(), d_results.data_ptr(),

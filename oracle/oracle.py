@@ -23,9 +23,16 @@ REFERENCE_FLOP = 0b111  # cards {0, 1, 2}: the reference's fixed flop (game.rs:7
 _lib = None
 
 
+REF_SO = os.path.join(HERE, "_ref", "libpoker_ref.so")
+REFERENCE_TREE = "/root/reference"
+
+
 def build():
-    """Compiles the oracle with its Makefile (g++)."""
+    """Compiles the oracle with its Makefile (g++) and, where the reference sources are
+    present, the reference's own CUDA library into oracle/_ref (nvcc)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if os.path.isdir(os.path.join(REFERENCE_TREE, "src", "cuda")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={REFERENCE_TREE}"], check=True)
     return SO_PATH
 
 

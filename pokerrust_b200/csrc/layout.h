@@ -27,6 +27,8 @@ constexpr int kLSlots = 48;         // card list slots: 46 hands, end sentinel, 
 constexpr int kListLen = 46;
 constexpr int kSlotsPerBoard = 1326;  // colex index of the {turn, river} pair
 
+constexpr uint32_t kNoBucket = 0xFFFF;
+
 // Element word of a list slot: hand | bucket << 11 | valid << 19.
 constexpr uint32_t kElemValid = 1u << 19;
 
@@ -37,6 +39,9 @@ struct BoardPack {
     //  z: same for the low card's list, slots counted from the start of the card lists
     //  w: same for the high card's list
     uint4 meta[kGSlots];
+    // Live hands in bucket order (then rank order): l | bucket << 16; padding entries carry
+    // bucket kNoBucket. Bucket sums become segmented reductions over this order.
+    uint32_t border[kGSlots];
     uint32_t gelem[kGSlots];               // global list elements
     uint32_t celem[kNumLists * kLSlots];   // card list elements
     uint8_t list_card[64];                 // card of each card list

@@ -138,6 +138,18 @@ __global__ void __launch_bounds__(256) pack_boards_kernel(unsigned long long flo
         }
     }
     if (tid < 64) out->list_card[tid] = list_card[tid];
+    if (tid == 64) {
+        // counting sort of the live hands by bucket (stable in rank order)
+        uint16_t start[257];
+        for (int b = 0; b <= 256; b++) start[b] = 0;
+        for (int l = 0; l < kLive; l++) start[a[sorted[kBlocked + l]] + 1]++;
+        for (int b = 0; b < 256; b++) start[b + 1] += start[b];
+        for (int l = 0; l < kLive; l++) {
+            const int b = a[sorted[kBlocked + l]];
+            out->border[start[b]++] = (uint32_t)l | ((uint32_t)b << 16);
+        }
+        for (int l = kLive; l < kGSlots; l++) out->border[l] = kNoBucket << 16;
+    }
 }
 
 void launch_pack_boards(unsigned long long flop, const uint16_t *eval, const uint16_t *abstr,

@@ -42,6 +42,8 @@ constexpr int kGPer = 9;               // warps 0-3: global list slots per lane 
 constexpr int kCPer = 6;               // card list slots per lane (8 lanes * 6 = 48)
 constexpr int kPioW = 20;              // bucket row: SD channels 0-8, pad, fold channels 12-19
 constexpr int kFoldCol = 12;
+constexpr int kOutPer = 3;             // output phase: hands per lane, in bucket order
+constexpr int kOutWarps = 12;          // 12 * 32 * 3 >= 1081
 
 struct __align__(16) Smem {
     float pio[kBuckets][kPioW];    // opponent reach per bucket and leaf
@@ -55,6 +57,8 @@ struct __align__(16) Smem {
     float Tf[kNumFold];            // totals, fold channels
     float gwarp[4][kNumLeaves];    // global list warp totals
     float scale[kNumLeaves];
+    float stage[kOutWarps][2][kNumLeaves];  // bucket runs touching an output warp's ends
+    int stage_key[kOutWarps][2];
 };
 
 __device__ __forceinline__ void bar_global_list() {
@@ -87,6 +91,54 @@ __device__ __forceinline__ void elem_x_sd(const Smem &S, uint32_t e, float x[kNu
     x[8] = rh * q8;
 }
 
+// Leaf values (before the leaf's bet/sign scale) of live hand l for all 17 channels:
+// showdowns from the prefix sums at tie-group bounds, folds from totals and card sums.
+__device__ __forceinline__ int hand_values(const Smem &S, const BoardPack *__restrict__ pk, int l,
+                                           float v[kNumLeaves]) {
+    const uint4 m = __ldg(&pk->meta[l]);
+    const int h = m.x & 2047;
+    const int b = (m.x >> 11) & 255;
+    const int c1 = (m.x >> 19) & 63;
+    const int c2 = (m.x >> 25) & 63;
+    const int gs = m.y & 0xffff, ge = m.y >> 16;
+    const int s1 = m.z & 0xffff, e1 = m.z >> 16;
+    const int s2 = m.w & 0xffff, e2 = m.w >> 16;
+    const int t1 = (s1 / kLSlots) * kLSlots + kListLen;
+    const int t2 = (s2 / kLSlots) * kLSlots + kListLen;
+#pragma unroll
+    for (int c = 0; c < kNumSD; c++) {
+        const float wb = S.P[gs][c] + S.P[ge][c] - S.P[kLive][c];
+        const float wb1 = S.CP[s1][c] + S.CP[e1][c] - S.CP[t1][c];
+        const float wb2 = S.CP[s2][c] + S.CP[e2][c] - S.CP[t2][c];
+        v[c] = wb - wb1 - wb2;
+    }
+    const float rh = S.r[h];
+    const float4 *prow = reinterpret_cast<const float4 *>(S.pio[b]);
+    const float4 f0 = prow[3], f1 = prow[4];
+    const float xf[8] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};
+    const float4 *cf1 = reinterpret_cast<const float4 *>(S.Cf[c1]);
+    const float4 *cf2 = reinterpret_cast<const float4 *>(S.Cf[c2]);
+    const float4 a0 = cf1[0], a1 = cf1[1], b0 = cf2[0], b1 = cf2[1];
+    const float ca[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    const float cb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+    for (int f = 0; f < kNumFold; f++) v[kNumSD + f] = S.Tf[f] - ca[f] - cb[f] + rh * xf[f];
+    return h;
+}
+
+// Adds the staged warp-boundary bucket runs of the last output phase into abar, in a fixed
+// order (one thread per leaf channel), so that bucket sums do not depend on scheduling.
+__device__ __forceinline__ void resolve_stage(Smem &S, int c) {
+#pragma unroll 1
+    for (int w = 0; w < kOutWarps; w++) {
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            const int key = S.stage_key[w][side];
+            if (key >= 0) S.abar[key][c] += S.stage[w][side][c];
+        }
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(NT, 1)
     river_kernel(const SubgameDesc *__restrict__ desc, const float *__restrict__ ranges,
@@ -113,9 +165,9 @@ __global__ void __launch_bounds__(NT, 1)
         }
     }
     if (tid < kNumLeaves) S.scale[tid] = leaf_scale(kLeaf(tid), updater, bet);
-    float reg[kEdges];
     if (tid < kBuckets) {
         const int b = tid;
+        float reg[kEdges];
 #pragma unroll
         for (int e = 0; e < kEdges; e++) reg[e] = greg[e * kBuckets + b];
         float psb[kStates], pbb[kStates];
@@ -170,12 +222,15 @@ __global__ void __launch_bounds__(NT, 1)
     __syncthreads();
 
     // ---- the 48 river cards ----
+    int rc_done = 0;
     for (int rc = 0; rc < 52; rc++) {
         const unsigned long long rb = 1ull << rc;
         if (rb & d.board4) continue;
         const int slot = pair_index((d.board4 | rb) ^ flop);
         const BoardPack *__restrict__ pk = packs + slot;
         __syncthreads();  // previous river's readers are done with P, CP, Cf, Tf
+        if (MODE == kModeCFR && warp == NT / 32 - 1 && lane < kNumLeaves && rc_done > 0) resolve_stage(S, lane);
+        rc_done++;
 
         if (warp < 4) {
             // global list: lane g holds slots [9g, 9g + 9)
@@ -303,75 +358,156 @@ __global__ void __launch_bounds__(NT, 1)
         }
         __syncthreads();
 
-        // ---- per live hand: leaf values, bucket sums, root value ----
-        for (int l = tid; l < kLive; l += NT) {
-            const uint4 m = __ldg(&pk->meta[l]);
-            const int h = m.x & 2047;
-            const int b = (m.x >> 11) & 255;
-            const int c1 = (m.x >> 19) & 63;
-            const int c2 = (m.x >> 25) & 63;
-            const int gs = m.y & 0xffff, ge = m.y >> 16;
-            const int s1 = m.z & 0xffff, e1 = m.z >> 16;
-            const int s2 = m.w & 0xffff, e2 = m.w >> 16;
-            const int t1 = (s1 / kLSlots) * kLSlots + kListLen;
-            const int t2 = (s2 / kLSlots) * kLSlots + kListLen;
-            float v[kNumLeaves];
+        // ---- per live hand, in bucket order: root value and per-bucket leaf sums ----
+        if (warp < kOutWarps) {
+            const unsigned FULL = 0xffffffffu;
+            float F[kNumLeaves], L[kNumLeaves];  // first run / last run of this lane's hands
+            int nr = 0, kf = -1, kl = -1;
 #pragma unroll
-            for (int c = 0; c < kNumSD; c++) {
-                const float wb = S.P[gs][c] + S.P[ge][c] - S.P[kLive][c];
-                const float wb1 = S.CP[s1][c] + S.CP[e1][c] - S.CP[t1][c];
-                const float wb2 = S.CP[s2][c] + S.CP[e2][c] - S.CP[t2][c];
-                v[c] = wb - wb1 - wb2;
-            }
-            const float rh = S.r[h];
-            const float4 *prow = reinterpret_cast<const float4 *>(S.pio[b]);
-            const float4 f0 = prow[3], f1 = prow[4];
-            const float xf[8] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};
-            const float4 *cf1 = reinterpret_cast<const float4 *>(S.Cf[c1]);
-            const float4 *cf2 = reinterpret_cast<const float4 *>(S.Cf[c2]);
-            const float4 a0 = cf1[0], a1 = cf1[1], b0 = cf2[0], b1 = cf2[1];
-            const float ca[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float cb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            for (int c = 0; c < kNumLeaves; c++) F[c] = L[c] = 0.0f;
 #pragma unroll
-            for (int f = 0; f < kNumFold; f++) v[kNumSD + f] = S.Tf[f] - ca[f] - cb[f] + rh * xf[f];
-
-            if (MODE == kModeCFR) {
-                const float4 *wrow = reinterpret_cast<const float4 *>(S.wown[b]);
-                const float4 w0 = wrow[0], w1 = wrow[1], w2 = wrow[2], w3 = wrow[3], w4 = wrow[4];
-                float acc = v[0] * w0.x + v[1] * w0.y + v[2] * w0.z + v[3] * w0.w + v[4] * w1.x +
-                            v[5] * w1.y + v[6] * w1.z + v[7] * w1.w + v[8] * w2.x;
-                acc += v[9] * w3.x + v[10] * w3.y + v[11] * w3.z + v[12] * w3.w + v[13] * w4.x +
-                       v[14] * w4.y + v[15] * w4.z + v[16] * w4.w;
-                S.out[h] += acc;
+            for (int i = 0; i < kOutPer; i++) {
+                const int j = tid * kOutPer + i;
+                const uint32_t be = j < kLive ? __ldg(&pk->border[j]) : (kNoBucket << 16);
+                const int key = be >> 16;
+                if (key == (int)kNoBucket) continue;
+                float v[kNumLeaves];
+                const int h = hand_values(S, pk, be & 0xffff, v);
+                if (MODE == kModeCFR) {
+                    const float4 *wrow = reinterpret_cast<const float4 *>(S.wown[key]);
+                    const float4 w0 = wrow[0], w1 = wrow[1], w2 = wrow[2], w3 = wrow[3], w4 = wrow[4];
+                    float acc = v[0] * w0.x + v[1] * w0.y + v[2] * w0.z + v[3] * w0.w + v[4] * w1.x +
+                                v[5] * w1.y + v[6] * w1.z + v[7] * w1.w + v[8] * w2.x;
+                    acc += v[9] * w3.x + v[10] * w3.y + v[11] * w3.z + v[12] * w3.w + v[13] * w4.x +
+                           v[14] * w4.y + v[15] * w4.z + v[16] * w4.w;
+                    S.out[h] += acc;
+                    // runs of equal buckets; a run strictly inside the lane is a whole bucket
+                    if (nr == 0) {
+                        kf = kl = key;
+                        nr = 1;
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) atomicAdd(&S.abar[b][c], v[c]);
-            } else {
-                // best response: max over the updater's actions, sum over the opponent's
-                // (state.rs:273-284, poker.cu:437-471)
-                float A[kStates];
+                        for (int c = 0; c < kNumLeaves; c++) F[c] = v[c];
+                    } else if (key == kl) {
+                        if (nr == 1) {
 #pragma unroll
-                for (int L = 0; L < kNumLeaves; L++) A[kLeaf(L)] = v[L] * S.scale[L];
+                            for (int c = 0; c < kNumLeaves; c++) F[c] += v[c];
+                        } else {
 #pragma unroll
-                for (int di = kNumDecision - 1; di >= 0; di--) {
-                    const int s = kDecision(di);
-                    const int nk = kNChild(s);
-                    float acc = A[kChild(s, 0)];
-                    if (kActor(s) == updater) {
-#pragma unroll
-                        for (int k = 1; k < 3; k++)
-                            if (k < nk) acc = fmaxf(acc, A[kChild(s, k)]);
+                            for (int c = 0; c < kNumLeaves; c++) L[c] += v[c];
+                        }
                     } else {
+                        if (nr >= 2) {
 #pragma unroll
-                        for (int k = 1; k < 3; k++)
-                            if (k < nk) acc += A[kChild(s, k)];
+                            for (int c = 0; c < kNumLeaves; c++) S.abar[kl][c] += L[c];
+                        }
+#pragma unroll
+                        for (int c = 0; c < kNumLeaves; c++) L[c] = v[c];
+                        kl = key;
+                        nr = nr + 1;
                     }
-                    A[s] = acc;
+                } else {
+                    // best response: max over the updater's actions, sum over the opponent's
+                    // (state.rs:273-284, poker.cu:437-471)
+                    float A[kStates];
+#pragma unroll
+                    for (int Lf = 0; Lf < kNumLeaves; Lf++) A[kLeaf(Lf)] = v[Lf] * S.scale[Lf];
+#pragma unroll
+                    for (int di = kNumDecision - 1; di >= 0; di--) {
+                        const int s = kDecision(di);
+                        const int nk = kNChild(s);
+                        float acc = A[kChild(s, 0)];
+                        if (kActor(s) == updater) {
+#pragma unroll
+                            for (int k = 1; k < 3; k++)
+                                if (k < nk) acc = fmaxf(acc, A[kChild(s, k)]);
+                        } else {
+#pragma unroll
+                            for (int k = 1; k < 3; k++)
+                                if (k < nk) acc += A[kChild(s, k)];
+                        }
+                        A[s] = acc;
+                    }
+                    S.out[h] += A[1];
                 }
-                S.out[h] += A[1];
+            }
+            if (MODE == kModeCFR) {
+                // segmented reduction of bucket runs across the lanes of the warp; runs that
+                // touch the warp's first or last hand are staged for resolve_stage
+                const bool single = nr <= 1;
+                const int kfirst = nr > 0 ? kf : -1 - lane;  // unique keys for empty lanes
+                const int klast = nr > 0 ? kl : -1 - lane;
+                const int prev_kl = __shfl_up_sync(FULL, klast, 1);
+                const bool join = lane > 0 && kfirst == prev_kl;
+                const bool link = single && join;
+                const unsigned starts = __ballot_sync(FULL, !link);
+                const int seg_start = 31 - __clz(starts & (FULL >> (31 - lane)));
+                float R[kNumLeaves];
+#pragma unroll
+                for (int c = 0; c < kNumLeaves; c++) R[c] = single ? F[c] : L[c];
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+                    for (int c = 0; c < kNumLeaves; c++) {
+                        const float t = __shfl_up_sync(FULL, R[c], off);
+                        if (lane - off >= seg_start) R[c] += t;
+                    }
+                }
+                float Cin[kNumLeaves];
+#pragma unroll
+                for (int c = 0; c < kNumLeaves; c++) {
+                    const float t = __shfl_up_sync(FULL, R[c], 1);
+                    Cin[c] = join ? t : 0.0f;
+                }
+                const bool next_join = __shfl_down_sync(FULL, (int)join, 1) && lane < 31;
+                const unsigned ends = __ballot_sync(FULL, !single || !next_join);
+                const int hend = __ffs(ends) - 1;
+                if (lane == 31) S.stage_key[warp][1] = -1;
+                if (lane == hend) S.stage_key[warp][0] = -1;
+                __syncwarp();
+                if (nr > 0) {
+                    if (!single) {
+                        // first run ends in this lane
+                        if (lane == hend) {
+                            S.stage_key[warp][0] = kfirst;
+#pragma unroll
+                            for (int c = 0; c < kNumLeaves; c++) S.stage[warp][0][c] = Cin[c] + F[c];
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < kNumLeaves; c++) S.abar[kfirst][c] += Cin[c] + F[c];
+                        }
+                        // last run (R == L here) ends here unless the next lane joins it
+                        if (lane == 31) {
+                            S.stage_key[warp][1] = klast;
+#pragma unroll
+                            for (int c = 0; c < kNumLeaves; c++) S.stage[warp][1][c] = R[c];
+                        } else if (!next_join) {
+#pragma unroll
+                            for (int c = 0; c < kNumLeaves; c++) S.abar[klast][c] += R[c];
+                        }
+                    } else if (!next_join) {
+                        // the lane's only run ends here, total R
+                        if (lane == hend) {
+                            S.stage_key[warp][0] = klast;
+#pragma unroll
+                            for (int c = 0; c < kNumLeaves; c++) S.stage[warp][0][c] = R[c];
+                        } else if (lane == 31) {
+                            S.stage_key[warp][1] = klast;
+#pragma unroll
+                            for (int c = 0; c < kNumLeaves; c++) S.stage[warp][1][c] = R[c];
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < kNumLeaves; c++) S.abar[klast][c] += R[c];
+                        }
+                    }
+                }
             }
         }
     }
     __syncthreads();
+    if (MODE == kModeCFR) {
+        if (warp == NT / 32 - 1 && lane < kNumLeaves) resolve_stage(S, lane);
+        __syncthreads();
+    }
 
     // ---- results (state.rs:431 / poker.cu:603: mean over the 48 rivers) ----
     {
@@ -383,6 +519,9 @@ __global__ void __launch_bounds__(NT, 1)
     // ---- regret update, once per subgame (poker.cu:450-487,524-574) ----
     if (MODE == kModeCFR && tid < kBuckets) {
         const int b = tid;
+        float reg[kEdges];
+#pragma unroll
+        for (int e = 0; e < kEdges; e++) reg[e] = greg[e * kBuckets + b];
         float A[kStates];
 #pragma unroll
         for (int L = 0; L < kNumLeaves; L++) A[kLeaf(L)] = S.abar[b][L] * S.scale[L];
