@@ -1,6 +1,7 @@
 """Runs the reference's own CUDA library (oracle/_ref/libpoker_ref.so, built from
 src/cuda/interface.cu) through its C ABI on the fixed-flop game's 27,783 river roots and
-saves what it returns. Test infrastructure: tests/test_reference_kernel.py starts it in a
+records, for a sample of roots, the regret state before and after every pass together
+with the pass's ranges and returned values. Test infrastructure: tests/test_reference_kernel.py starts it in a
 fresh process, because the reference never zeroes its `updates` arrays
 (src/cuda/interface.cu:75-81) and relies on freshly mapped device memory being zero.
 
@@ -55,38 +56,43 @@ def main():
         assert L.build_river_cuda(int(boards[i]), float(bets[i]), b) == i
     ev = L.transfer_flop_eval_cuda(O.REFERENCE_FLOP, p(co), p(ci), p(e.view(np.int16)),
                                    p(c.view(np.int16)), p(a.view(np.int16)))
-    rng = np.random.default_rng(seed)
-    res = np.zeros((n, 1326), np.float32)
-    saved = {}
-    times = []
-    for it in range(iters):
-        for player in (0, 1):
-            r = ranges_for(order, boards, rng)
-            for i in range(n):
-                L.upload_c(b, i, p(r[i]))
-            t0 = time.perf_counter()
-            L.evaluate_cuda(b, ev, player, False)
-            times.append(time.perf_counter() - t0)
-            for i in range(n):
-                L.download_c(b, i, p(res[i]))
-            if it == iters - 1:
-                saved[f"cfv_p{player}"] = res.copy()
-    for player in (0, 1):
-        r = ranges_for(order, boards, rng)
-        for i in range(n):
-            L.upload_c(b, i, p(r[i]))
-        L.evaluate_cuda(b, ev, player, True)
-        for i in range(n):
-            L.download_c(b, i, p(res[i]))
-        saved[f"br_p{player}"] = res.copy()
     # Builder { int current_index; State *states; AbstractVector *abstract_vectors; ... }
-    # (src/cuda/structs.h:59-67): read the regrets straight from the device.
+    # (src/cuda/structs.h:59-67): the regrets are read straight from the device.
     fields = (ctypes.c_void_p * 7).from_address(b)
     abstract_vectors = fields[2]
     reg = np.zeros((n, 26, 256), np.float32)
-    assert cudart.cudaMemcpy(p(reg), abstract_vectors, reg.nbytes, 2) == 0
+
+    def regrets():
+        assert cudart.cudaMemcpy(p(reg), abstract_vectors, reg.nbytes, 2) == 0
+        return reg[sample].copy()
+
+    # every pass is recorded for a sample of river roots: the state before it, its input
+    # ranges, and what it returned and left behind
+    srng = np.random.default_rng(seed + 1)
+    sample = np.unique(np.concatenate([[0, 27, 45, 324], srng.choice(n, 252, replace=False)]))
+    rng = np.random.default_rng(seed)
+    res = np.zeros((n, 1326), np.float32)
+    rec = {"before": [], "after": [], "ranges": [], "values": [], "player": [], "exploit": []}
+    times = []
+    passes = [(player, False) for _ in range(iters) for player in (0, 1)] + [(0, True), (1, True)]
+    for player, exploit in passes:
+        r = ranges_for(order, boards, rng)
+        rec["before"].append(regrets())
+        for i in range(n):
+            L.upload_c(b, i, p(r[i]))
+        t0 = time.perf_counter()
+        L.evaluate_cuda(b, ev, player, exploit)
+        times.append(time.perf_counter() - t0)
+        for i in range(n):
+            L.download_c(b, i, p(res[i]))
+        rec["after"].append(regrets())
+        rec["ranges"].append(r[sample])
+        rec["values"].append(res[sample].copy())
+        rec["player"].append(player)
+        rec["exploit"].append(exploit)
     L.free_eval_cuda(ev)
-    np.savez(out_path, regrets=reg, seconds=np.array(times), **saved)
+    np.savez(out_path, sample=sample, seconds=np.array(times),
+             **{k: np.array(v) for k, v in rec.items()})
 
 
 if __name__ == "__main__":
