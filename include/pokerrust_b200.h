@@ -97,6 +97,16 @@ int pr_set_regrets(void *builder, const float *in);
 /* Releases a builder (the reference never frees it). */
 void pr_free_builder(void *builder);
 
+/* Builds the hand-rank tables of every river board of `flop` on the device (the work the
+ * reference's host does in src/evaluator.rs:22-184 and packs in src/cuda_interface.rs:48-102)
+ * and returns a handle usable wherever transfer_flop_eval_cuda's is; release it with
+ * free_eval_cuda. Check pr_eval_status. */
+void *pr_tables_build(uint64_t flop);
+
+/* Copies a handle's tables out in the reference's packed layout (1326 slots of 1838 eval,
+ * 2652 collision and 1326 bucket u16 entries); null outputs are skipped. */
+int pr_tables_export(void *eval, uint16_t *eval_out, uint16_t *coll_out, uint16_t *abstr_out);
+
 /* Status of a table handle: 0, or the bit set of table inconsistencies found on upload. */
 int pr_eval_status(void *eval);
 

@@ -9,9 +9,11 @@ from .interface import (  # noqa: F401
     RANGE_STRIDE,
     Builder,
     PokerLibError,
+    build_flop_tables,
     build_river,
     download_gpu,
     evaluate_gpu,
+    export_tables,
     free_eval,
     initialize_builder,
     lib,

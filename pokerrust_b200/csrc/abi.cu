@@ -11,6 +11,7 @@
 
 #include "../../include/pokerrust_b200.h"
 #include "device_common.cuh"
+#include "gen_tables.h"
 #include "layout.h"
 #include "pack_boards.h"
 #include "river_cfr.h"
@@ -129,10 +130,15 @@ struct EvalTables {
     unsigned long long flop = 0;
     BoardPack *packs = nullptr;
     uint16_t *d_eval = nullptr;
+    uint16_t *d_coll = nullptr;
     uint16_t *d_abstr = nullptr;
     int *d_err = nullptr;
     int status = 0;
 };
+
+constexpr size_t kEvalBytes = (size_t)kSlotsPerBoard * (1326 + 512) * sizeof(uint16_t);
+constexpr size_t kCollBytes = (size_t)kSlotsPerBoard * 52 * 51 * sizeof(uint16_t);
+constexpr size_t kAbstrBytes = (size_t)kSlotsPerBoard * kHands * sizeof(uint16_t);
 
 // One table set kept for reuse: the reference transfers and frees the tables on every
 // iteration (game.rs:71,180), so allocations are recycled instead of repeated.
@@ -266,6 +272,59 @@ bool card_order_ok(const uint64_t *card_order, const uint16_t *card_indexes) {
     return true;
 }
 
+// A table set with device buffers, recycled from the last free_eval_cuda when possible.
+EvalTables *acquire_tables() {
+    EvalTables *t = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        t = g_cache;
+        g_cache = nullptr;
+    }
+    if (t) {
+        t->status = 0;
+        return t;
+    }
+    t = new EvalTables();
+    cudaError_t e;
+    if ((e = cudaMalloc(&t->packs, (size_t)kSlotsPerBoard * sizeof(BoardPack))) != cudaSuccess ||
+        (e = cudaMalloc(&t->d_eval, kEvalBytes)) != cudaSuccess ||
+        (e = cudaMalloc(&t->d_coll, kCollBytes)) != cudaSuccess ||
+        (e = cudaMalloc(&t->d_abstr, kAbstrBytes)) != cudaSuccess ||
+        (e = cudaMalloc(&t->d_err, sizeof(int))) != cudaSuccess) {
+        fail(kErrAlloc, "table allocation", e);
+        t->status = -1;
+        return t;
+    }
+    // slots the re-pack never writes (pairs that overlap the flop) stay all-zero
+    if ((e = cudaMemset(t->packs, 0, (size_t)kSlotsPerBoard * sizeof(BoardPack))) != cudaSuccess ||
+        (e = cudaMemset(t->d_coll, 0, kCollBytes)) != cudaSuccess) {
+        fail(kErrCuda, "table initialisation", e);
+        t->status = -1;
+    }
+    return t;
+}
+
+// Validates the reference-layout tables in d_eval / d_abstr and re-packs them into BoardPack.
+void repack_tables(EvalTables *t) {
+    cudaError_t e;
+    if ((e = cudaMemset(t->d_err, 0, sizeof(int))) != cudaSuccess) {
+        fail(kErrCuda, "table re-pack", e);
+        t->status = -1;
+        return;
+    }
+    launch_pack_boards(t->flop, t->d_eval, t->d_abstr, t->packs, t->d_err, 0);
+    int err = 0;
+    if ((e = cudaMemcpy(&err, t->d_err, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+        fail(kErrCuda, "table re-pack", e);
+        t->status = -1;
+        return;
+    }
+    if (err) {
+        fail(kErrTables, "hand-rank tables are not a consistent rank order");
+        t->status = err;
+    }
+}
+
 }  // namespace
 }  // namespace prb
 
@@ -327,32 +386,9 @@ int build_river_cuda(uint64_t cards, float bet, void *builder) {
 void *transfer_flop_eval_cuda(uint64_t flop, const uint64_t *card_order, const uint16_t *card_indexes,
                               const uint16_t *eval, const uint16_t *coll_vec, const uint16_t *abstractions) {
     (void)coll_vec;  // rebuilt on the device from the sort order
-    EvalTables *t = nullptr;
-    {
-        std::lock_guard<std::mutex> lk(g_cache_mu);
-        t = g_cache;
-        g_cache = nullptr;
-    }
+    EvalTables *t = acquire_tables();
+    if (t->status) return t;
     cudaError_t e;
-    if (!t) {
-        t = new EvalTables();
-        if ((e = cudaMalloc(&t->packs, (size_t)kSlotsPerBoard * sizeof(BoardPack))) != cudaSuccess ||
-            (e = cudaMalloc(&t->d_eval, (size_t)kSlotsPerBoard * (1326 + 512) * sizeof(uint16_t))) !=
-                cudaSuccess ||
-            (e = cudaMalloc(&t->d_abstr, (size_t)kSlotsPerBoard * kHands * sizeof(uint16_t))) !=
-                cudaSuccess ||
-            (e = cudaMalloc(&t->d_err, sizeof(int))) != cudaSuccess) {
-            fail(kErrAlloc, "table allocation", e);
-            t->status = -1;
-            return t;
-        }
-        // slots the re-pack never writes (pairs that overlap the flop) stay all-zero
-        if ((e = cudaMemset(t->packs, 0, (size_t)kSlotsPerBoard * sizeof(BoardPack))) != cudaSuccess) {
-            fail(kErrCuda, "table initialisation", e);
-            t->status = -1;
-            return t;
-        }
-    }
     t->flop = flop;
     t->status = 0;
     if (__builtin_popcountll(flop) != 3 || (flop >> 52) || !card_order || !card_indexes || !eval ||
@@ -366,26 +402,14 @@ void *transfer_flop_eval_cuda(uint64_t flop, const uint64_t *card_order, const u
         t->status = 64;
         return t;
     }
-    if ((e = cudaMemcpy(t->d_eval, eval, (size_t)kSlotsPerBoard * (1326 + 512) * sizeof(uint16_t),
-                        cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(t->d_abstr, abstractions, (size_t)kSlotsPerBoard * kHands * sizeof(uint16_t),
-                        cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemset(t->d_err, 0, sizeof(int))) != cudaSuccess) {
+    if ((e = cudaMemcpy(t->d_eval, eval, kEvalBytes, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (coll_vec && (e = cudaMemcpy(t->d_coll, coll_vec, kCollBytes, cudaMemcpyHostToDevice)) != cudaSuccess) ||
+        (e = cudaMemcpy(t->d_abstr, abstractions, kAbstrBytes, cudaMemcpyHostToDevice)) != cudaSuccess) {
         fail(kErrCuda, "table upload", e);
         t->status = -1;
         return t;
     }
-    launch_pack_boards(flop, t->d_eval, t->d_abstr, t->packs, t->d_err, 0);
-    int err = 0;
-    if ((e = cudaMemcpy(&err, t->d_err, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) {
-        fail(kErrCuda, "table re-pack", e);
-        t->status = -1;
-        return t;
-    }
-    if (err) {
-        fail(kErrTables, "transfer_flop_eval_cuda: tables are not a consistent rank order");
-        t->status = err;
-    }
+    repack_tables(t);
     return t;
 }
 
@@ -399,6 +423,7 @@ void free_eval_cuda(void *eval) {
     }
     cudaFree(t->packs);
     cudaFree(t->d_eval);
+    cudaFree(t->d_coll);
     cudaFree(t->d_abstr);
     cudaFree(t->d_err);
     delete t;
@@ -497,6 +522,36 @@ void pr_free_builder(void *builder) {
     if (b->comm) cudaFreeHost(b->comm);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
+}
+
+void *pr_tables_build(uint64_t flop) {
+    EvalTables *t = acquire_tables();
+    if (t->status) return t;
+    t->flop = flop;
+    if (__builtin_popcountll(flop) != 3 || (flop >> 52)) {
+        fail(kErrArg, "pr_tables_build: a flop is three cards");
+        t->status = 32;
+        return t;
+    }
+    cudaError_t e = launch_gen_tables(flop, t->d_eval, t->d_coll, t->d_abstr, 0);
+    if (e != cudaSuccess) {
+        fail(kErrCuda, "table generation", e);
+        t->status = -1;
+        return t;
+    }
+    repack_tables(t);
+    return t;
+}
+
+int pr_tables_export(void *eval, uint16_t *eval_out, uint16_t *coll_out, uint16_t *abstr_out) {
+    EvalTables *t = (EvalTables *)eval;
+    if (!t || t->status) return fail(kErrArg, "pr_tables_export: invalid table handle");
+    cudaError_t e;
+    if ((eval_out && (e = cudaMemcpy(eval_out, t->d_eval, kEvalBytes, cudaMemcpyDeviceToHost)) != cudaSuccess) ||
+        (coll_out && (e = cudaMemcpy(coll_out, t->d_coll, kCollBytes, cudaMemcpyDeviceToHost)) != cudaSuccess) ||
+        (abstr_out && (e = cudaMemcpy(abstr_out, t->d_abstr, kAbstrBytes, cudaMemcpyDeviceToHost)) != cudaSuccess))
+        return fail(kErrCuda, "table export", e);
+    return kOk;
 }
 
 int pr_eval_status(void *eval) { return eval ? ((EvalTables *)eval)->status : -1; }

@@ -28,23 +28,35 @@ constexpr int kListLen = 46;
 constexpr int kSlotsPerBoard = 1326;  // colex index of the {turn, river} pair
 
 constexpr uint32_t kNoBucket = 0xFFFF;
+// Element words of the lists. Rank list (gelem):
+//   hand (bits 0-10) | bucket (11-18) | starts a tie group (19) | tie group id (20-30)
+// Card lists (celem):
+//   hand (bits 0-10) | bucket (11-18) | starts a group within the list (19) | card group id (20-31)
+// Padding elements carry hand kNoHand.
+constexpr uint32_t kNoHand = 2047;
+constexpr uint32_t kGroupStart = 1u << 19;
 
-// Element word of a list slot: hand | bucket << 11 | valid << 19.
-constexpr uint32_t kElemValid = 1u << 19;
+// Largest tie-group counts any 5-card board can have: 1081 hands in the rank list, 47 * 46
+// hands in the card lists.
+constexpr int kMaxGroups = kLive;
+constexpr int kMaxCardGroups = kNumLists * kListLen;
 
 struct BoardPack {
     // Per live hand in rank order (index l = sorted position - 245):
     //  x: hand | bucket << 11 | low card << 19 | high card << 25
-    //  y: tie-group start slot | group end slot << 16      (global list, end = 1081)
-    //  z: same for the low card's list, slots counted from the start of the card lists
-    //  w: same for the high card's list
+    //  y: tie group id in the rank list
+    //  z: group id of the hand in its low card's list
+    //  w: group id of the hand in its high card's list
     uint4 meta[kGSlots];
     // Live hands in bucket order (then rank order): l | bucket << 16; padding entries carry
     // bucket kNoBucket. Bucket sums become segmented reductions over this order.
     uint32_t border[kGSlots];
-    uint32_t gelem[kGSlots];               // global list elements
-    uint32_t celem[kNumLists * kLSlots];   // card list elements
+    uint32_t gelem[kGSlots];               // rank list elements
+    uint32_t celem[kNumLists * kLSlots];   // card list elements, 48 slots per list
     uint8_t list_card[64];                 // card of each card list
+    int32_t num_groups;                    // tie groups in the rank list
+    int32_t num_card_groups;               // groups over all card lists
+    int32_t pad[2];
 };
 
 static_assert(sizeof(BoardPack) % 16 == 0, "BoardPack rows must stay 16-byte aligned");

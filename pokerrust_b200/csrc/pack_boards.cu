@@ -32,9 +32,9 @@ __global__ void __launch_bounds__(256) pack_boards_kernel(unsigned long long flo
     __shared__ unsigned int seen[kHands];
     __shared__ uint16_t gid[kLive];
     __shared__ uint16_t gstart[kLive];
-    __shared__ uint16_t gend[kLive];
-    __shared__ uint32_t lo[kLive];  // low card list: start slot | end slot << 16
-    __shared__ uint32_t hi[kLive];
+    __shared__ uint32_t lo[kLive];  // group id of the hand in its low card's list
+    __shared__ uint32_t hi[kLive];  // ... and in its high card's list
+    __shared__ int list_groups[kNumLists];
     __shared__ uint8_t list_card[64];
     __shared__ int bad;
 
@@ -80,11 +80,7 @@ __global__ void __launch_bounds__(256) pack_boards_kernel(unsigned long long flo
             gid[l] = (uint16_t)g;
             gstart[l] = (uint16_t)start;
         }
-        int end = kLive;
-        for (int l = kLive - 1; l >= 0; l--) {
-            gend[l] = (uint16_t)end;
-            if (gstart[l] == l) end = l;
-        }
+        out->num_groups = g + 1;
         int n = 0;
         for (int c = 0; c < 52; c++) {
             if (!(board >> c & 1)) list_card[n++] = (uint8_t)c;
@@ -93,7 +89,24 @@ __global__ void __launch_bounds__(256) pack_boards_kernel(unsigned long long flo
     }
     __syncthreads();
     if (tid < kNumLists) {
-        // card list of one live card, in rank order, with tie-group bounds inside the list
+        // groups inside one card list: hands of the list that share a tie group
+        const int li = tid;
+        const int card = list_card[li];
+        int k = 0, ng = 0, prev = -1;
+        for (int l = 0; l < kLive && k < kListLen; l++) {
+            int h = sorted[kBlocked + l];
+            int hc1 = cards_of[h] & 255, hc2 = cards_of[h] >> 8;
+            if (hc1 == card || hc2 == card) {
+                if (gid[l] != prev) ng++;
+                prev = gid[l];
+                k++;
+            }
+        }
+        list_groups[li] = ng;
+    }
+    __syncthreads();
+    if (tid < kNumLists) {
+        // card list of one live card, in rank order, with its group ids
         const int li = tid;
         const int card = list_card[li];
         uint16_t pos[kListLen];
@@ -103,25 +116,23 @@ __global__ void __launch_bounds__(256) pack_boards_kernel(unsigned long long flo
             int hc1 = cards_of[h] & 255, hc2 = cards_of[h] >> 8;
             if (hc1 == card || hc2 == card) pos[k++] = (uint16_t)l;
         }
-        if (k != kListLen) {
-            atomicOr(err, 16);
-            return;
-        }
+        if (k != kListLen) atomicOr(err, 16);  // cannot happen once the checks above passed
+        int base = 0;
+        for (int i = 0; i < li; i++) base += list_groups[i];
         uint32_t *ce = out->celem + li * kLSlots;
-        int s = 0;
-        for (int j = 0; j < kListLen; j++) {
-            if (j == 0 || gid[pos[j]] != gid[pos[j - 1]]) s = j;
-            int en = j + 1;
-            while (en < kListLen && gid[pos[en]] == gid[pos[j]]) en++;
+        int cg = base - 1;
+        for (int j = 0; j < k; j++) {
+            const bool start = j == 0 || gid[pos[j]] != gid[pos[j - 1]];
+            if (start) cg++;
             int l = pos[j];
             int h = sorted[kBlocked + l];
-            ce[j] = (uint32_t)h | ((uint32_t)a[h] << 11) | kElemValid;
-            uint32_t v = (uint32_t)(li * kLSlots + s) | ((uint32_t)(li * kLSlots + en) << 16);
-            if ((cards_of[h] & 255) == card) lo[l] = v;
-            else hi[l] = v;
+            ce[j] = (uint32_t)h | ((uint32_t)a[h] << 11) | (start ? kGroupStart : 0u) | ((uint32_t)cg << 20);
+            if ((cards_of[h] & 255) == card) lo[l] = (uint32_t)cg;
+            else hi[l] = (uint32_t)cg;
         }
-        ce[kListLen] = 0;
-        ce[kListLen + 1] = 0;
+        ce[kListLen] = kNoHand;
+        ce[kListLen + 1] = kNoHand;
+        if (li == kNumLists - 1) out->num_card_groups = cg + 1;
     }
     __syncthreads();
     for (int l = tid; l < kGSlots; l += blockDim.x) {
@@ -130,11 +141,12 @@ __global__ void __launch_bounds__(256) pack_boards_kernel(unsigned long long flo
             int hc1 = cards_of[h] & 255, hc2 = cards_of[h] >> 8;
             uint32_t x = (uint32_t)h | ((uint32_t)a[h] << 11) | ((uint32_t)hc1 << 19) |
                          ((uint32_t)hc2 << 25);
-            out->meta[l] = make_uint4(x, (uint32_t)gstart[l] | ((uint32_t)gend[l] << 16), lo[l], hi[l]);
-            out->gelem[l] = (uint32_t)h | ((uint32_t)a[h] << 11) | kElemValid;
+            out->meta[l] = make_uint4(x, gid[l], lo[l], hi[l]);
+            out->gelem[l] = (uint32_t)h | ((uint32_t)a[h] << 11) | (gstart[l] == l ? kGroupStart : 0u) |
+                            ((uint32_t)gid[l] << 20);
         } else {
             out->meta[l] = make_uint4(0, 0, 0, 0);
-            out->gelem[l] = 0;
+            out->gelem[l] = kNoHand;
         }
     }
     if (tid < 64) out->list_card[tid] = list_card[tid];

@@ -48,13 +48,14 @@ constexpr int kOutWarps = 12;          // 12 * 32 * 3 >= 1081
 struct __align__(16) Smem {
     float pio[kBuckets][kPioW];    // opponent reach per bucket and leaf
     float wown[kBuckets][kPioW];   // updater reach * leaf scale per bucket and leaf
-    float P[kGSlots][kNumSD];      // exclusive prefix sums, global list
-    float CP[kNumLists * kLSlots][kNumSD];  // exclusive prefix sums, card lists
+    float Pg[kMaxGroups + 1][kNumSD];      // rank-list prefix sum at each tie group's start; [G] = total
+    float VC[kMaxCardGroups][kNumSD];      // W - B of each group of each card list
     float abar[kBuckets][kNumLeaves];       // per-bucket leaf sums over rivers
     float r[kRangeStride];         // opponent range of the subgame
     float out[kRangeStride];       // updater's value, summed over rivers
     float Cf[52][kNumFold];        // card sums, fold channels
     float Tf[kNumFold];            // totals, fold channels
+    float Tsd[kNumSD];             // totals, showdown channels
     float gwarp[4][kNumLeaves];    // global list warp totals
     float scale[kNumLeaves];
     float stage[kOutWarps][2][kNumLeaves];  // bucket runs touching an output warp's ends
@@ -69,7 +70,7 @@ __device__ __forceinline__ void bar_global_list() {
 __device__ __forceinline__ void elem_x(const Smem &S, uint32_t e, float x[kNumLeaves]) {
     const int h = e & 2047;
     const int b = (e >> 11) & 255;
-    const float rh = (e & kElemValid) ? S.r[h] : 0.0f;
+    const float rh = h != (int)kNoHand ? S.r[h] : 0.0f;
     const float4 *row = reinterpret_cast<const float4 *>(S.pio[b]);
     float4 q0 = row[0], q1 = row[1], q2 = row[2], q3 = row[3], q4 = row[4];
     x[0] = rh * q0.x; x[1] = rh * q0.y; x[2] = rh * q0.z; x[3] = rh * q0.w;
@@ -79,20 +80,8 @@ __device__ __forceinline__ void elem_x(const Smem &S, uint32_t e, float x[kNumLe
     x[13] = rh * q4.x; x[14] = rh * q4.y; x[15] = rh * q4.z; x[16] = rh * q4.w;
 }
 
-__device__ __forceinline__ void elem_x_sd(const Smem &S, uint32_t e, float x[kNumSD]) {
-    const int h = e & 2047;
-    const int b = (e >> 11) & 255;
-    const float rh = (e & kElemValid) ? S.r[h] : 0.0f;
-    const float4 *row = reinterpret_cast<const float4 *>(S.pio[b]);
-    float4 q0 = row[0], q1 = row[1];
-    float q8 = S.pio[b][8];
-    x[0] = rh * q0.x; x[1] = rh * q0.y; x[2] = rh * q0.z; x[3] = rh * q0.w;
-    x[4] = rh * q1.x; x[5] = rh * q1.y; x[6] = rh * q1.z; x[7] = rh * q1.w;
-    x[8] = rh * q8;
-}
-
 // Leaf values (before the leaf's bet/sign scale) of live hand l for all 17 channels:
-// showdowns from the prefix sums at tie-group bounds, folds from totals and card sums.
+// showdowns from the group values of the scans, folds from totals and card sums.
 __device__ __forceinline__ int hand_values(const Smem &S, const BoardPack *__restrict__ pk, int l,
                                            float v[kNumLeaves]) {
     const uint4 m = __ldg(&pk->meta[l]);
@@ -100,17 +89,12 @@ __device__ __forceinline__ int hand_values(const Smem &S, const BoardPack *__res
     const int b = (m.x >> 11) & 255;
     const int c1 = (m.x >> 19) & 63;
     const int c2 = (m.x >> 25) & 63;
-    const int gs = m.y & 0xffff, ge = m.y >> 16;
-    const int s1 = m.z & 0xffff, e1 = m.z >> 16;
-    const int s2 = m.w & 0xffff, e2 = m.w >> 16;
-    const int t1 = (s1 / kLSlots) * kLSlots + kListLen;
-    const int t2 = (s2 / kLSlots) * kLSlots + kListLen;
+    const int gid = m.y, cg1 = m.z, cg2 = m.w;
 #pragma unroll
     for (int c = 0; c < kNumSD; c++) {
-        const float wb = S.P[gs][c] + S.P[ge][c] - S.P[kLive][c];
-        const float wb1 = S.CP[s1][c] + S.CP[e1][c] - S.CP[t1][c];
-        const float wb2 = S.CP[s2][c] + S.CP[e2][c] - S.CP[t2][c];
-        v[c] = wb - wb1 - wb2;
+        // (W - B) over the rank list minus (W - B) over the two card lists
+        const float wb = S.Pg[gid][c] + S.Pg[gid + 1][c] - S.Tsd[c];
+        v[c] = wb - S.VC[cg1][c] - S.VC[cg2][c];
     }
     const float rh = S.r[h];
     const float4 *prow = reinterpret_cast<const float4 *>(S.pio[b]);
@@ -233,20 +217,27 @@ __global__ void __launch_bounds__(NT, 1)
         rc_done++;
 
         if (warp < 4) {
-            // global list: lane g holds slots [9g, 9g + 9)
+            // rank list: lane g holds slots [9g, 9g + 9); writes the prefix sum at every
+            // tie-group start (and the total at [G])
             const int g = tid;
+            uint32_t ge[kGPer];
             float tot[kNumLeaves];
 #pragma unroll
             for (int c = 0; c < kNumLeaves; c++) tot[c] = 0.0f;
 #pragma unroll
             for (int i = 0; i < kGPer; i++) {
                 const int s = g * kGPer + i;
-                if (s < kLive) {
-                    float x[kNumLeaves];
-                    elem_x(S, __ldg(&pk->gelem[s]), x);
+                const uint32_t e = s < kLive ? __ldg(&pk->gelem[s]) : kNoHand;
+                ge[i] = e;
+                float x[kNumLeaves];
+                elem_x(S, e, x);
+                if ((e & 2047) != kNoHand && (e & kGroupStart)) {
+                    float *dst = S.Pg[e >> 20];
 #pragma unroll
-                    for (int c = 0; c < kNumLeaves; c++) tot[c] += x[c];
+                    for (int c = 0; c < kNumSD; c++) dst[c] = tot[c];  // lane-local part
                 }
+#pragma unroll
+                for (int c = 0; c < kNumLeaves; c++) tot[c] += x[c];
             }
             float inc[kNumLeaves];
 #pragma unroll
@@ -264,7 +255,7 @@ __global__ void __launch_bounds__(NT, 1)
                 for (int c = 0; c < kNumLeaves; c++) S.gwarp[warp][c] = inc[c];
             }
             bar_global_list();
-            float run[kNumSD];
+            float offs[kNumSD];
             float total[kNumLeaves];
 #pragma unroll
             for (int c = 0; c < kNumLeaves; c++) {
@@ -276,9 +267,24 @@ __global__ void __launch_bounds__(NT, 1)
                     all += v;
                 }
                 total[c] = all;
-                if (c < kNumSD) run[c] = before + inc[c] - tot[c];
+                if (c < kNumSD) offs[c] = before + inc[c] - tot[c];
+            }
+#pragma unroll
+            for (int i = 0; i < kGPer; i++) {
+                const uint32_t e = ge[i];
+                if ((e & 2047) != kNoHand && (e & kGroupStart)) {
+                    float *dst = S.Pg[e >> 20];
+#pragma unroll
+                    for (int c = 0; c < kNumSD; c++) dst[c] += offs[c];
+                }
             }
             if (tid == 0) {
+                const int G = pk->num_groups;
+#pragma unroll
+                for (int c = 0; c < kNumSD; c++) {
+                    S.Pg[G][c] = total[c];
+                    S.Tsd[c] = total[c];
+                }
 #pragma unroll
                 for (int f = 0; f < kNumFold; f++) S.Tf[f] = total[kNumSD + f];
                 if (MODE == kModeCFR) {
@@ -288,27 +294,16 @@ __global__ void __launch_bounds__(NT, 1)
                         S.abar[0][c] += (c < kNumSD ? -235.0f : 235.0f) * total[c];
                 }
             }
-#pragma unroll
-            for (int i = 0; i < kGPer; i++) {
-                const int s = g * kGPer + i;
-                if (s < kGSlots) {
-#pragma unroll
-                    for (int c = 0; c < kNumSD; c++) S.P[s][c] = run[c];
-                    if (s < kLive) {
-                        float x[kNumSD];
-                        elem_x_sd(S, __ldg(&pk->gelem[s]), x);
-#pragma unroll
-                        for (int c = 0; c < kNumSD; c++) run[c] += x[c];
-                    }
-                }
-            }
         } else {
-            // card lists: 8 lanes per list, 6 slots per lane, 4 lists per warp
+            // card lists: 8 lanes per list, 6 slots per lane, 4 lists per warp. Each group of
+            // a list gets VC = W - B = prefix(start) + prefix(end) - list total.
+            const unsigned FULL = 0xffffffffu;
             const int cw = warp - 4;
             const int sub = lane >> 3;       // list within the warp
             const int sl = lane & 7;         // lane within the list
             const int li = cw * 4 + sub;     // card list index (48 >= 47)
             const bool active = li < kNumLists;
+            uint32_t ce[kCPer];
             float xs[kCPer][kNumSD];
             float tot[kNumLeaves];
 #pragma unroll
@@ -316,8 +311,9 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
             for (int i = 0; i < kCPer; i++) {
                 const int j = sl * kCPer + i;
+                const uint32_t e = (active && j < kListLen) ? __ldg(&pk->celem[li * kLSlots + j]) : kNoHand;
+                ce[i] = e;
                 float x[kNumLeaves];
-                const uint32_t e = (active && j < kListLen) ? __ldg(&pk->celem[li * kLSlots + j]) : 0u;
                 elem_x(S, e, x);
 #pragma unroll
                 for (int c = 0; c < kNumLeaves; c++) tot[c] += x[c];
@@ -331,29 +327,57 @@ __global__ void __launch_bounds__(NT, 1)
             for (int off = 1; off < 8; off <<= 1) {
 #pragma unroll
                 for (int c = 0; c < kNumLeaves; c++) {
-                    const float t = __shfl_up_sync(0xffffffffu, inc[c], off);
+                    const float t = __shfl_up_sync(FULL, inc[c], off);
                     if (sl >= off) inc[c] += t;
                 }
             }
-            if (active) {
-                float run[kNumSD];
+            if (active && sl == 7) {
+                const int card = pk->list_card[li];
 #pragma unroll
-                for (int c = 0; c < kNumSD; c++) run[c] = inc[c] - tot[c];
+                for (int f = 0; f < kNumFold; f++) S.Cf[card][f] = inc[kNumSD + f];
+            }
+            float run[kNumSD], Tc[kNumSD];
 #pragma unroll
-                for (int i = 0; i < kCPer; i++) {
-                    const int j = sl * kCPer + i;
-                    float *dst = S.CP[li * kLSlots + j];
+            for (int c = 0; c < kNumSD; c++) {
+                run[c] = inc[c] - tot[c];
+                Tc[c] = __shfl_sync(FULL, inc[c], lane | 7);
+            }
+            bool open = false, any = false;
+            int cgo = 0;
+            float Wo[kNumSD], Ff[kNumSD];
 #pragma unroll
-                    for (int c = 0; c < kNumSD; c++) {
-                        dst[c] = run[c];
-                        run[c] += xs[i][c];
+            for (int c = 0; c < kNumSD; c++) Wo[c] = Ff[c] = 0.0f;
+#pragma unroll
+            for (int i = 0; i < kCPer; i++) {
+                const uint32_t e = ce[i];
+                if ((e & 2047) != kNoHand && (e & kGroupStart)) {
+                    if (open) {
+                        float *dst = S.VC[cgo];
+#pragma unroll
+                        for (int c = 0; c < kNumSD; c++) dst[c] = Wo[c] + run[c] - Tc[c];
                     }
-                }
-                if (sl == 7) {
-                    const int card = pk->list_card[li];
+                    if (!any) {
 #pragma unroll
-                    for (int f = 0; f < kNumFold; f++) S.Cf[card][f] = inc[kNumSD + f];
+                        for (int c = 0; c < kNumSD; c++) Ff[c] = run[c];
+                        any = true;
+                    }
+                    open = true;
+                    cgo = e >> 20;
+#pragma unroll
+                    for (int c = 0; c < kNumSD; c++) Wo[c] = run[c];
                 }
+#pragma unroll
+                for (int c = 0; c < kNumSD; c++) run[c] += xs[i][c];
+            }
+            // the group still open at this lane's end closes at the next lane of the list that
+            // starts a group, or at the end of the list
+            const unsigned m = __ballot_sync(FULL, any);
+            const unsigned later = (m >> (lane & ~7)) & 0xffu & ~((2u << sl) - 1u);
+            const int nxt = later ? (lane & ~7) + __ffs(later) - 1 : lane;
+#pragma unroll
+            for (int c = 0; c < kNumSD; c++) {
+                const float f = __shfl_sync(FULL, Ff[c], nxt);
+                if (open) S.VC[cgo][c] = Wo[c] + (later ? f : Tc[c]) - Tc[c];
             }
         }
         __syncthreads();

@@ -69,6 +69,10 @@ def lib():
         L.pr_eval_status.restype = i32
         L.pr_eval_status.argtypes = [vp]
         L.pr_river_smem_bytes.restype = ctypes.c_size_t
+        L.pr_tables_build.restype = vp
+        L.pr_tables_build.argtypes = [u64]
+        L.pr_tables_export.restype = i32
+        L.pr_tables_export.argtypes = [vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -130,6 +134,26 @@ def transfer_flop_eval(flop, card_order, card_indexes, eval_tables, coll_vec, ab
         lib().free_eval_cuda(p)
         raise PokerLibError(f"transfer_flop_eval_cuda rejected the tables (bits {st})")
     return p
+
+
+def build_flop_tables(flop):
+    """Hand-rank tables of every river board of `flop`, generated on the device (no host
+    tables needed); usable wherever transfer_flop_eval's handle is."""
+    p = lib().pr_tables_build(int(flop))
+    st = lib().pr_eval_status(p)
+    if st != 0:
+        lib().free_eval_cuda(p)
+        raise PokerLibError(f"pr_tables_build failed (status {st})")
+    return p
+
+
+def export_tables(ptr):
+    """The handle's tables in the reference's packed layout: (eval, coll, abstractions)."""
+    e = np.zeros(HANDS * (HANDS + 512), np.uint16)
+    c = np.zeros(HANDS * 52 * 51, np.uint16)
+    a = np.zeros(HANDS * HANDS, np.uint16)
+    _check(lib().pr_tables_export(ptr, _ptr(e), _ptr(c), _ptr(a)), "pr_tables_export")
+    return e, c, a
 
 
 def free_eval(ptr):
