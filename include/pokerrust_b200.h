@@ -110,8 +110,13 @@ int pr_tables_export(void *eval, uint16_t *eval_out, uint16_t *coll_out, uint16_
 /* Status of a table handle: 0, or the bit set of table inconsistencies found on upload. */
 int pr_eval_status(void *eval);
 
-/* Shared memory bytes the river kernel uses per CTA. */
-size_t pr_river_smem_bytes(void);
+/* Shared memory bytes the river kernel uses per CTA with these tables (0 if invalid). */
+size_t pr_river_smem_bytes(void *eval, int calc_exploit, int fp64);
+
+/* Best-response pass in double precision (the exploitability check): ranges / results are
+ * host arrays of count rows of 1326 doubles; regrets are read, not changed. Synchronous. */
+int pr_evaluate_br64(void *builder, void *eval, int updating_player, const double *ranges,
+                     double *results);
 
 #ifdef __cplusplus
 }

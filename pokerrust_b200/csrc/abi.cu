@@ -121,6 +121,9 @@ struct Builder {
     float *d_regrets = nullptr;
     float *d_ranges = nullptr;
     float *d_results = nullptr;
+    double *d_ranges64 = nullptr;   // double-precision best response (lazily allocated)
+    double *d_results64 = nullptr;
+    int cap64 = 0;
     cudaStream_t stream = nullptr;
     unsigned long long checked_flop = 0;  // boards validated against this flop
     int checked_count = -1;
@@ -132,8 +135,9 @@ struct EvalTables {
     uint16_t *d_eval = nullptr;
     uint16_t *d_coll = nullptr;
     uint16_t *d_abstr = nullptr;
-    int *d_err = nullptr;
+    int *d_err = nullptr;  // [0] error bits, [1] max tie groups, [2] max card-list groups
     int status = 0;
+    int max_groups = 0, max_card_groups = 0;
 };
 
 constexpr size_t kEvalBytes = (size_t)kSlotsPerBoard * (1326 + 512) * sizeof(uint16_t);
@@ -244,7 +248,7 @@ int evaluate_impl(Builder *b, EvalTables *t, int player, int exploit, const floa
         d_out = b->d_results;
     }
     e = launch_river(exploit ? kModeBR : kModeCFR, b->d_desc, n, d_in, d_out, b->d_regrets, t->packs,
-                     t->flop, player, s);
+                     t->flop, player, t->max_groups, t->max_card_groups, s);
     if (e != cudaSuccess) return fail(kErrCuda, "river kernel launch", e);
     if (staged) {
         e = cudaMemcpyAsync(b->comm, b->d_results, (size_t)n * kRangeStride * sizeof(float),
@@ -290,7 +294,7 @@ EvalTables *acquire_tables() {
         (e = cudaMalloc(&t->d_eval, kEvalBytes)) != cudaSuccess ||
         (e = cudaMalloc(&t->d_coll, kCollBytes)) != cudaSuccess ||
         (e = cudaMalloc(&t->d_abstr, kAbstrBytes)) != cudaSuccess ||
-        (e = cudaMalloc(&t->d_err, sizeof(int))) != cudaSuccess) {
+        (e = cudaMalloc(&t->d_err, 4 * sizeof(int))) != cudaSuccess) {
         fail(kErrAlloc, "table allocation", e);
         t->status = -1;
         return t;
@@ -307,21 +311,29 @@ EvalTables *acquire_tables() {
 // Validates the reference-layout tables in d_eval / d_abstr and re-packs them into BoardPack.
 void repack_tables(EvalTables *t) {
     cudaError_t e;
-    if ((e = cudaMemset(t->d_err, 0, sizeof(int))) != cudaSuccess) {
+    if ((e = cudaMemset(t->d_err, 0, 4 * sizeof(int))) != cudaSuccess) {
         fail(kErrCuda, "table re-pack", e);
         t->status = -1;
         return;
     }
     launch_pack_boards(t->flop, t->d_eval, t->d_abstr, t->packs, t->d_err, 0);
-    int err = 0;
-    if ((e = cudaMemcpy(&err, t->d_err, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+    int err[4] = {0, 0, 0, 0};
+    if ((e = cudaMemcpy(err, t->d_err, 4 * sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) {
         fail(kErrCuda, "table re-pack", e);
         t->status = -1;
         return;
     }
-    if (err) {
+    if (err[0]) {
         fail(kErrTables, "hand-rank tables are not a consistent rank order");
-        t->status = err;
+        t->status = err[0];
+        return;
+    }
+    t->max_groups = err[1];
+    t->max_card_groups = err[2];
+    if (river_smem_bytes(kModeCFR, 0, t->max_groups, t->max_card_groups) > 227 * 1024 ||
+        river_smem_bytes(kModeBR, 1, t->max_groups, t->max_card_groups) > 227 * 1024) {
+        fail(kErrTables, "a board of this flop has more tie groups than shared memory holds");
+        t->status = 128;
     }
 }
 
@@ -519,6 +531,8 @@ void pr_free_builder(void *builder) {
     cudaFree(b->d_ranges);
     cudaFree(b->d_results);
     cudaFree(b->d_regrets);
+    cudaFree(b->d_ranges64);
+    cudaFree(b->d_results64);
     if (b->comm) cudaFreeHost(b->comm);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -556,6 +570,50 @@ int pr_tables_export(void *eval, uint16_t *eval_out, uint16_t *coll_out, uint16_
 
 int pr_eval_status(void *eval) { return eval ? ((EvalTables *)eval)->status : -1; }
 
-size_t pr_river_smem_bytes(void) { return river_smem_bytes(); }
+size_t pr_river_smem_bytes(void *eval, int calc_exploit, int fp64) {
+    EvalTables *t = (EvalTables *)eval;
+    if (!t || t->status) return 0;
+    return river_smem_bytes(calc_exploit ? kModeBR : kModeCFR, fp64, t->max_groups, t->max_card_groups);
+}
+
+int pr_evaluate_br64(void *builder, void *eval, int updating_player, const double *ranges, double *results) {
+    Builder *b = (Builder *)builder;
+    EvalTables *t = (EvalTables *)eval;
+    if (!b || !t || !ranges || !results) return fail(kErrArg, "pr_evaluate_br64: null argument");
+    if (t->status) return fail(kErrTables, "pr_evaluate_br64: tables failed validation");
+    if (updating_player != 0 && updating_player != 1) return fail(kErrArg, "pr_evaluate_br64: bad player");
+    for (const SubgameDesc &d : b->desc)
+        if ((d.board4 & t->flop) != t->flop || __builtin_popcountll(d.board4) != 4)
+            return fail(kErrArg, "pr_evaluate_br64: a river root's board does not contain the flop");
+    int st = sync_device(b);
+    if (st) return st;
+    const int n = b->dev_count;
+    if (n == 0) return kOk;
+    cudaError_t e;
+    if (b->cap64 < b->dev_capacity) {
+        cudaFree(b->d_ranges64);
+        cudaFree(b->d_results64);
+        b->d_ranges64 = b->d_results64 = nullptr;
+        b->cap64 = 0;
+        const size_t bytes = (size_t)b->dev_capacity * kRangeStride * sizeof(double);
+        if ((e = cudaMalloc(&b->d_ranges64, bytes)) != cudaSuccess ||
+            (e = cudaMalloc(&b->d_results64, bytes)) != cudaSuccess)
+            return fail(kErrAlloc, "double-precision buffers", e);
+        cudaMemset(b->d_ranges64, 0, bytes);
+        b->cap64 = b->dev_capacity;
+    }
+    // host rows of 1326 -> device rows of kRangeStride
+    e = cudaMemcpy2DAsync(b->d_ranges64, kRangeStride * sizeof(double), ranges, kHands * sizeof(double),
+                          kHands * sizeof(double), n, cudaMemcpyHostToDevice, b->stream);
+    if (e != cudaSuccess) return fail(kErrCuda, "double range upload", e);
+    e = launch_river_br64(b->d_desc, n, b->d_ranges64, b->d_results64, b->d_regrets, t->packs, t->flop,
+                          updating_player, t->max_groups, t->max_card_groups, b->stream);
+    if (e != cudaSuccess) return fail(kErrCuda, "double best-response launch", e);
+    e = cudaMemcpy2DAsync(results, kHands * sizeof(double), b->d_results64, kRangeStride * sizeof(double),
+                          kHands * sizeof(double), n, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return fail(kErrCuda, "double best-response pass", e);
+    return kOk;
+}
 
 }  // extern "C"

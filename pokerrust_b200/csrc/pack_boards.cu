@@ -81,6 +81,7 @@ __global__ void __launch_bounds__(256) pack_boards_kernel(unsigned long long flo
             gstart[l] = (uint16_t)start;
         }
         out->num_groups = g + 1;
+        atomicMax(err + 1, g + 1);
         int n = 0;
         for (int c = 0; c < 52; c++) {
             if (!(board >> c & 1)) list_card[n++] = (uint8_t)c;
@@ -132,7 +133,10 @@ __global__ void __launch_bounds__(256) pack_boards_kernel(unsigned long long flo
         }
         ce[kListLen] = kNoHand;
         ce[kListLen + 1] = kNoHand;
-        if (li == kNumLists - 1) out->num_card_groups = cg + 1;
+        if (li == kNumLists - 1) {
+            out->num_card_groups = cg + 1;
+            atomicMax(err + 2, cg + 1);
+        }
     }
     __syncthreads();
     for (int l = tid; l < kGSlots; l += blockDim.x) {

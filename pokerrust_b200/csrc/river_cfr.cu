@@ -14,9 +14,10 @@
 //  * Showdown value of hand h at leaf L is
 //        sum_{o worse, o shares no card with h} x_L(o) - sum_{o better, ...} x_L(o)
 //    = [W(g) - B(g)] - [W_c1 - B_c1] - [W_c2 - B_c2]
-//    with W/B prefix sums over the rank-sorted live hands ("global list") and over the
-//    46 live hands holding each card ("card lists"), evaluated at tie-group bounds
-//    (inclusion-exclusion of blockers; state.rs:494-569, poker.cu:163-302).
+//    with W/B prefix sums over the rank-sorted live hands ("rank list") and over the 46
+//    live hands holding each card ("card lists"), evaluated at tie-group bounds
+//    (inclusion-exclusion of blockers; state.rs:494-569, poker.cu:163-302). The scans
+//    leave one value per tie group, so a hand needs five group lookups per channel.
 //  * Fold value is T - C[c1] - C[c2] + x(h) (state.rs:456-492, poker.cu:305-371).
 //  * Regret updates are linear in the leaf values, so the per-bucket leaf sums are
 //    accumulated over all 48 rivers and the tree is walked once per subgame at the end
@@ -26,6 +27,13 @@
 //    (poker.cu:281-288, strategy.rs:118-126 run over all 1326 hands and blocked hands have
 //    bucket 0). Over the 245 blocked hands that sum is -235 T at a showdown and +235 T at a
 //    fold, T the leaf's total opponent weight; it is added in closed form.
+//
+// Best response (MODE kModeBR) takes the per-hand maximum over the updater's actions
+// (state.rs:273-284, poker.cu:437-471) and can run in double precision (V = double), the
+// only double-precision step of the solver.
+//
+// Shared memory is laid out at launch: the group arrays are sized by the largest tie-group
+// counts of the flop's boards (BoardPack::num_groups / num_card_groups).
 #include <cuda_runtime.h>
 
 #include "device_common.cuh"
@@ -38,52 +46,122 @@ namespace prb {
 namespace {
 
 constexpr int NT = 512;                // threads per CTA
-constexpr int kGPer = 9;               // warps 0-3: global list slots per lane (128 * 9 >= 1082)
+constexpr int kGPer = 9;               // warps 0-3: rank list slots per lane (128 * 9 >= 1082)
 constexpr int kCPer = 6;               // card list slots per lane (8 lanes * 6 = 48)
 constexpr int kPioW = 20;              // bucket row: SD channels 0-8, pad, fold channels 12-19
 constexpr int kFoldCol = 12;
 constexpr int kOutPer = 3;             // output phase: hands per lane, in bucket order
 constexpr int kOutWarps = 12;          // 12 * 32 * 3 >= 1081
 
-struct __align__(16) Smem {
-    float pio[kBuckets][kPioW];    // opponent reach per bucket and leaf
-    float wown[kBuckets][kPioW];   // updater reach * leaf scale per bucket and leaf
-    float Pg[kMaxGroups + 1][kNumSD];      // rank-list prefix sum at each tie group's start; [G] = total
-    float VC[kMaxCardGroups][kNumSD];      // W - B of each group of each card list
-    float abar[kBuckets][kNumLeaves];       // per-bucket leaf sums over rivers
-    float r[kRangeStride];         // opponent range of the subgame
-    float out[kRangeStride];       // updater's value, summed over rivers
-    float Cf[52][kNumFold];        // card sums, fold channels
-    float Tf[kNumFold];            // totals, fold channels
-    float Tsd[kNumSD];             // totals, showdown channels
-    float gwarp[4][kNumLeaves];    // global list warp totals
-    float scale[kNumLeaves];
-    float stage[kOutWarps][2][kNumLeaves];  // bucket runs touching an output warp's ends
-    int stage_key[kOutWarps][2];
+// Byte offsets of the shared-memory arrays; computed the same way on host and device.
+struct Layout {
+    unsigned pio, wown, Pg, VC, abar, r, out, Cf, Tf, Tsd, gwarp, scale, stage, stage_key, total;
 };
 
-__device__ __forceinline__ void bar_global_list() {
-    asm volatile("bar.sync 1, 128;" ::: "memory");
+__host__ __device__ inline unsigned take(unsigned *o, unsigned bytes) {
+    const unsigned at = *o;
+    *o += (bytes + 15u) & ~15u;
+    return at;
 }
 
-// x for all 17 channels of one list element (bucket row load).
-__device__ __forceinline__ void elem_x(const Smem &S, uint32_t e, float x[kNumLeaves]) {
+__host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned groups, unsigned card_groups) {
+    Layout L;
+    unsigned o = 0;
+    L.pio = take(&o, kBuckets * kPioW * vb);
+    L.wown = cfr ? take(&o, kBuckets * kPioW * 4) : 0;
+    L.Pg = take(&o, (groups + 1) * kNumSD * vb);
+    L.VC = take(&o, card_groups * kNumSD * vb);
+    L.abar = cfr ? take(&o, kBuckets * kNumLeaves * 4) : 0;
+    L.r = take(&o, kRangeStride * vb);
+    L.out = take(&o, kRangeStride * vb);
+    L.Cf = take(&o, 52 * kNumFold * vb);
+    L.Tf = take(&o, kNumFold * vb);
+    L.Tsd = take(&o, kNumSD * vb);
+    L.gwarp = take(&o, 4 * kNumLeaves * vb);
+    L.scale = take(&o, kNumLeaves * 4);
+    L.stage = cfr ? take(&o, kOutWarps * 2 * kNumLeaves * 4) : 0;
+    L.stage_key = cfr ? take(&o, kOutWarps * 2 * 4) : 0;
+    L.total = o;
+    return L;
+}
+
+template <typename V>
+struct Smem {
+    V (*pio)[kPioW];             // opponent reach per bucket and leaf
+    float (*wown)[kPioW];        // updater reach * leaf scale per bucket and leaf (CFR)
+    V (*Pg)[kNumSD];             // rank-list prefix sum at each tie group's start; [G] = total
+    V (*VC)[kNumSD];             // W - B of each group of each card list
+    float (*abar)[kNumLeaves];   // per-bucket leaf sums over rivers (CFR)
+    V *r;                        // opponent range of the subgame
+    V *out;                      // updater's value, summed over rivers
+    V (*Cf)[kNumFold];           // card sums, fold channels
+    V *Tf;                       // totals, fold channels
+    V *Tsd;                      // totals, showdown channels
+    V (*gwarp)[kNumLeaves];      // rank-list warp totals
+    float *scale;                // leaf scales
+    float (*stage)[2][kNumLeaves];  // bucket runs touching an output warp's ends (CFR)
+    int (*stage_key)[2];
+
+    __device__ Smem(unsigned char *base, const Layout &L)
+        : pio(reinterpret_cast<V(*)[kPioW]>(base + L.pio)),
+          wown(reinterpret_cast<float(*)[kPioW]>(base + L.wown)),
+          Pg(reinterpret_cast<V(*)[kNumSD]>(base + L.Pg)),
+          VC(reinterpret_cast<V(*)[kNumSD]>(base + L.VC)),
+          abar(reinterpret_cast<float(*)[kNumLeaves]>(base + L.abar)),
+          r(reinterpret_cast<V *>(base + L.r)),
+          out(reinterpret_cast<V *>(base + L.out)),
+          Cf(reinterpret_cast<V(*)[kNumFold]>(base + L.Cf)),
+          Tf(reinterpret_cast<V *>(base + L.Tf)),
+          Tsd(reinterpret_cast<V *>(base + L.Tsd)),
+          gwarp(reinterpret_cast<V(*)[kNumLeaves]>(base + L.gwarp)),
+          scale(reinterpret_cast<float *>(base + L.scale)),
+          stage(reinterpret_cast<float(*)[2][kNumLeaves]>(base + L.stage)),
+          stage_key(reinterpret_cast<int(*)[2]>(base + L.stage_key)) {}
+};
+
+__device__ __forceinline__ void bar_rank_list() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Loads n consecutive values (n a multiple of 4 floats / 2 doubles) with 16-byte loads.
+__device__ __forceinline__ void load_row(const float *p, float *o, int n) {
+    const float4 *q = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+    for (int i = 0; i < n / 4; i++) {
+        const float4 t = q[i];
+        o[4 * i] = t.x;
+        o[4 * i + 1] = t.y;
+        o[4 * i + 2] = t.z;
+        o[4 * i + 3] = t.w;
+    }
+}
+__device__ __forceinline__ void load_row(const double *p, double *o, int n) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+    for (int i = 0; i < n / 2; i++) {
+        const double2 t = q[i];
+        o[2 * i] = t.x;
+        o[2 * i + 1] = t.y;
+    }
+}
+
+// x for all 17 channels of one list element (one bucket-row load).
+template <typename V>
+__device__ __forceinline__ void elem_x(const Smem<V> &S, uint32_t e, V x[kNumLeaves]) {
     const int h = e & 2047;
     const int b = (e >> 11) & 255;
-    const float rh = h != (int)kNoHand ? S.r[h] : 0.0f;
-    const float4 *row = reinterpret_cast<const float4 *>(S.pio[b]);
-    float4 q0 = row[0], q1 = row[1], q2 = row[2], q3 = row[3], q4 = row[4];
-    x[0] = rh * q0.x; x[1] = rh * q0.y; x[2] = rh * q0.z; x[3] = rh * q0.w;
-    x[4] = rh * q1.x; x[5] = rh * q1.y; x[6] = rh * q1.z; x[7] = rh * q1.w;
-    x[8] = rh * q2.x;
-    x[9] = rh * q3.x; x[10] = rh * q3.y; x[11] = rh * q3.z; x[12] = rh * q3.w;
-    x[13] = rh * q4.x; x[14] = rh * q4.y; x[15] = rh * q4.z; x[16] = rh * q4.w;
+    const V rh = h != (int)kNoHand ? S.r[h] : V(0);
+    V row[kPioW];
+    load_row(S.pio[b], row, kPioW);
+#pragma unroll
+    for (int c = 0; c < kNumSD; c++) x[c] = rh * row[c];
+#pragma unroll
+    for (int f = 0; f < kNumFold; f++) x[kNumSD + f] = rh * row[kFoldCol + f];
 }
 
 // Leaf values (before the leaf's bet/sign scale) of live hand l for all 17 channels:
 // showdowns from the group values of the scans, folds from totals and card sums.
-__device__ __forceinline__ int hand_values(const Smem &S, const BoardPack *__restrict__ pk, int l,
-                                           float v[kNumLeaves]) {
+template <typename V>
+__device__ __forceinline__ int hand_values(const Smem<V> &S, const BoardPack *__restrict__ pk, int l,
+                                           V v[kNumLeaves]) {
     const uint4 m = __ldg(&pk->meta[l]);
     const int h = m.x & 2047;
     const int b = (m.x >> 11) & 255;
@@ -93,18 +171,14 @@ __device__ __forceinline__ int hand_values(const Smem &S, const BoardPack *__res
 #pragma unroll
     for (int c = 0; c < kNumSD; c++) {
         // (W - B) over the rank list minus (W - B) over the two card lists
-        const float wb = S.Pg[gid][c] + S.Pg[gid + 1][c] - S.Tsd[c];
+        const V wb = S.Pg[gid][c] + S.Pg[gid + 1][c] - S.Tsd[c];
         v[c] = wb - S.VC[cg1][c] - S.VC[cg2][c];
     }
-    const float rh = S.r[h];
-    const float4 *prow = reinterpret_cast<const float4 *>(S.pio[b]);
-    const float4 f0 = prow[3], f1 = prow[4];
-    const float xf[8] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};
-    const float4 *cf1 = reinterpret_cast<const float4 *>(S.Cf[c1]);
-    const float4 *cf2 = reinterpret_cast<const float4 *>(S.Cf[c2]);
-    const float4 a0 = cf1[0], a1 = cf1[1], b0 = cf2[0], b1 = cf2[1];
-    const float ca[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-    const float cb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+    const V rh = S.r[h];
+    V xf[kNumFold], ca[kNumFold], cb[kNumFold];
+    load_row(S.pio[b] + kFoldCol, xf, kNumFold);
+    load_row(S.Cf[c1], ca, kNumFold);
+    load_row(S.Cf[c2], cb, kNumFold);
 #pragma unroll
     for (int f = 0; f < kNumFold; f++) v[kNumSD + f] = S.Tf[f] - ca[f] - cb[f] + rh * xf[f];
     return h;
@@ -112,7 +186,7 @@ __device__ __forceinline__ int hand_values(const Smem &S, const BoardPack *__res
 
 // Adds the staged warp-boundary bucket runs of the last output phase into abar, in a fixed
 // order (one thread per leaf channel), so that bucket sums do not depend on scheduling.
-__device__ __forceinline__ void resolve_stage(Smem &S, int c) {
+__device__ __forceinline__ void resolve_stage(Smem<float> &S, int c) {
 #pragma unroll 1
     for (int w = 0; w < kOutWarps; w++) {
 #pragma unroll
@@ -123,13 +197,20 @@ __device__ __forceinline__ void resolve_stage(Smem &S, int c) {
     }
 }
 
-template <int MODE>
+template <typename V>
+__device__ __forceinline__ V vmax(V a, V b) {
+    return a > b ? a : b;
+}
+
+template <int MODE, typename V>
 __global__ void __launch_bounds__(NT, 1)
-    river_kernel(const SubgameDesc *__restrict__ desc, const float *__restrict__ ranges,
-                 float *__restrict__ results, float *__restrict__ regrets,
-                 const BoardPack *__restrict__ packs, unsigned long long flop, int updater) {
+    river_kernel(const SubgameDesc *__restrict__ desc, const V *__restrict__ ranges, V *__restrict__ results,
+                 float *__restrict__ regrets, const BoardPack *__restrict__ packs, unsigned long long flop,
+                 int updater, int max_groups, int max_card_groups) {
+    static_assert(MODE == kModeBR || sizeof(V) == 4, "CFR runs in single precision");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+    const Layout L = make_layout(MODE == kModeCFR, sizeof(V), max_groups, max_card_groups);
+    Smem<V> S(smem_raw, L);
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -139,14 +220,9 @@ __global__ void __launch_bounds__(NT, 1)
     float *greg = regrets + (size_t)sg * kEdges * kBuckets;
 
     // ---- subgame setup: range, per-bucket reach tables ----
-    {
-        const float4 *src = reinterpret_cast<const float4 *>(ranges + (size_t)sg * kRangeStride);
-        float4 *dst = reinterpret_cast<float4 *>(S.r);
-        float4 *o = reinterpret_cast<float4 *>(S.out);
-        for (int i = tid; i < kRangeStride / 4; i += NT) {
-            dst[i] = src[i];
-            o[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+    for (int i = tid; i < kRangeStride; i += NT) {
+        S.r[i] = ranges[(size_t)sg * kRangeStride + i];
+        S.out[i] = V(0);
     }
     if (tid < kNumLeaves) S.scale[tid] = leaf_scale(kLeaf(tid), updater, bet);
     if (tid < kBuckets) {
@@ -154,23 +230,23 @@ __global__ void __launch_bounds__(NT, 1)
         float reg[kEdges];
 #pragma unroll
         for (int e = 0; e < kEdges; e++) reg[e] = greg[e * kBuckets + b];
-        float psb[kStates], pbb[kStates];
-        psb[1] = 1.0f;
-        pbb[1] = 1.0f;
+        V psb[kStates], pbb[kStates];
+        psb[1] = V(1);
+        pbb[1] = V(1);
 #pragma unroll
         for (int di = 0; di < kNumDecision; di++) {
             const int s = kDecision(di);
             const int nk = kNChild(s);
-            float sum = 0.0f;
+            V sum = V(0);
 #pragma unroll
             for (int k = 0; k < 3; k++)
-                if (k < nk) sum += reg[kEdge(s, k)];
+                if (k < nk) sum += V(reg[kEdge(s, k)]);
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 if (k < nk) {
                     // regret matching with the reference's cutoff (strategy.rs:138-146,
                     // poker.cu:492-510)
-                    const float sig = sum <= 1e-4f ? 1.0f / (float)nk : reg[kEdge(s, k)] / sum;
+                    const V sig = sum <= V(1e-4f) ? V(1) / V(nk) : V(reg[kEdge(s, k)]) / sum;
                     const int c = kChild(s, k);
                     if (kActor(s) == 0) {
                         psb[c] = psb[s] * sig;
@@ -182,25 +258,21 @@ __global__ void __launch_bounds__(NT, 1)
                 }
             }
         }
-        float pio_row[kPioW], wown_row[kPioW];
 #pragma unroll
-        for (int i = 0; i < kPioW; i++) pio_row[i] = wown_row[i] = 0.0f;
+        for (int i = 0; i < kPioW; i++) S.pio[b][i] = V(0);
 #pragma unroll
-        for (int L = 0; L < kNumLeaves; L++) {
-            const int s = kLeaf(L);
-            const int col = L < kNumSD ? L : kFoldCol + (L - kNumSD);
-            const float own = updater == 0 ? psb[s] : pbb[s];
-            const float opp = updater == 0 ? pbb[s] : psb[s];
-            pio_row[col] = opp;
-            wown_row[col] = own * leaf_scale(s, updater, bet);
-            S.abar[b][L] = 0.0f;
+        for (int Lf = 0; Lf < kNumLeaves; Lf++) {
+            const int s = kLeaf(Lf);
+            const int col = Lf < kNumSD ? Lf : kFoldCol + (Lf - kNumSD);
+            S.pio[b][col] = updater == 0 ? pbb[s] : psb[s];
+            if constexpr (MODE == kModeCFR) {
+                S.wown[b][col] = float(updater == 0 ? psb[s] : pbb[s]) * leaf_scale(s, updater, bet);
+                S.abar[b][Lf] = 0.0f;
+            }
         }
-        float4 *pr = reinterpret_cast<float4 *>(S.pio[b]);
-        float4 *wr = reinterpret_cast<float4 *>(S.wown[b]);
+        if constexpr (MODE == kModeCFR) {
 #pragma unroll
-        for (int i = 0; i < kPioW / 4; i++) {
-            pr[i] = make_float4(pio_row[4 * i], pio_row[4 * i + 1], pio_row[4 * i + 2], pio_row[4 * i + 3]);
-            wr[i] = make_float4(wown_row[4 * i], wown_row[4 * i + 1], wown_row[4 * i + 2], wown_row[4 * i + 3]);
+            for (int i = kNumSD; i < kFoldCol; i++) S.wown[b][i] = 0.0f;
         }
     }
     __syncthreads();
@@ -212,8 +284,10 @@ __global__ void __launch_bounds__(NT, 1)
         if (rb & d.board4) continue;
         const int slot = pair_index((d.board4 | rb) ^ flop);
         const BoardPack *__restrict__ pk = packs + slot;
-        __syncthreads();  // previous river's readers are done with P, CP, Cf, Tf
-        if (MODE == kModeCFR && warp == NT / 32 - 1 && lane < kNumLeaves && rc_done > 0) resolve_stage(S, lane);
+        __syncthreads();  // previous river's readers are done with Pg, VC, Cf, Tf
+        if constexpr (MODE == kModeCFR) {
+            if (warp == NT / 32 - 1 && lane < kNumLeaves && rc_done > 0) resolve_stage(S, lane);
+        }
         rc_done++;
 
         if (warp < 4) {
@@ -221,32 +295,32 @@ __global__ void __launch_bounds__(NT, 1)
             // tie-group start (and the total at [G])
             const int g = tid;
             uint32_t ge[kGPer];
-            float tot[kNumLeaves];
+            V tot[kNumLeaves];
 #pragma unroll
-            for (int c = 0; c < kNumLeaves; c++) tot[c] = 0.0f;
+            for (int c = 0; c < kNumLeaves; c++) tot[c] = V(0);
 #pragma unroll
             for (int i = 0; i < kGPer; i++) {
                 const int s = g * kGPer + i;
                 const uint32_t e = s < kLive ? __ldg(&pk->gelem[s]) : kNoHand;
                 ge[i] = e;
-                float x[kNumLeaves];
+                V x[kNumLeaves];
                 elem_x(S, e, x);
                 if ((e & 2047) != kNoHand && (e & kGroupStart)) {
-                    float *dst = S.Pg[e >> 20];
+                    V *dst = S.Pg[e >> 20];
 #pragma unroll
                     for (int c = 0; c < kNumSD; c++) dst[c] = tot[c];  // lane-local part
                 }
 #pragma unroll
                 for (int c = 0; c < kNumLeaves; c++) tot[c] += x[c];
             }
-            float inc[kNumLeaves];
+            V inc[kNumLeaves];
 #pragma unroll
             for (int c = 0; c < kNumLeaves; c++) inc[c] = tot[c];
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
                 for (int c = 0; c < kNumLeaves; c++) {
-                    const float t = __shfl_up_sync(0xffffffffu, inc[c], off);
+                    const V t = __shfl_up_sync(0xffffffffu, inc[c], off);
                     if (lane >= off) inc[c] += t;
                 }
             }
@@ -254,15 +328,15 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
                 for (int c = 0; c < kNumLeaves; c++) S.gwarp[warp][c] = inc[c];
             }
-            bar_global_list();
-            float offs[kNumSD];
-            float total[kNumLeaves];
+            bar_rank_list();
+            V offs[kNumSD];
+            V total[kNumLeaves];
 #pragma unroll
             for (int c = 0; c < kNumLeaves; c++) {
-                float before = 0.0f, all = 0.0f;
+                V before = V(0), all = V(0);
 #pragma unroll
                 for (int w = 0; w < 4; w++) {
-                    const float v = S.gwarp[w][c];
+                    const V v = S.gwarp[w][c];
                     if (w < warp) before += v;
                     all += v;
                 }
@@ -273,7 +347,7 @@ __global__ void __launch_bounds__(NT, 1)
             for (int i = 0; i < kGPer; i++) {
                 const uint32_t e = ge[i];
                 if ((e & 2047) != kNoHand && (e & kGroupStart)) {
-                    float *dst = S.Pg[e >> 20];
+                    V *dst = S.Pg[e >> 20];
 #pragma unroll
                     for (int c = 0; c < kNumSD; c++) dst[c] += offs[c];
                 }
@@ -287,7 +361,7 @@ __global__ void __launch_bounds__(NT, 1)
                 }
 #pragma unroll
                 for (int f = 0; f < kNumFold; f++) S.Tf[f] = total[kNumSD + f];
-                if (MODE == kModeCFR) {
+                if constexpr (MODE == kModeCFR) {
                     // blocked hands' contribution to bucket 0 (see the file comment)
 #pragma unroll
                     for (int c = 0; c < kNumLeaves; c++)
@@ -304,30 +378,30 @@ __global__ void __launch_bounds__(NT, 1)
             const int li = cw * 4 + sub;     // card list index (48 >= 47)
             const bool active = li < kNumLists;
             uint32_t ce[kCPer];
-            float xs[kCPer][kNumSD];
-            float tot[kNumLeaves];
+            V xs[kCPer][kNumSD];
+            V tot[kNumLeaves];
 #pragma unroll
-            for (int c = 0; c < kNumLeaves; c++) tot[c] = 0.0f;
+            for (int c = 0; c < kNumLeaves; c++) tot[c] = V(0);
 #pragma unroll
             for (int i = 0; i < kCPer; i++) {
                 const int j = sl * kCPer + i;
                 const uint32_t e = (active && j < kListLen) ? __ldg(&pk->celem[li * kLSlots + j]) : kNoHand;
                 ce[i] = e;
-                float x[kNumLeaves];
+                V x[kNumLeaves];
                 elem_x(S, e, x);
 #pragma unroll
                 for (int c = 0; c < kNumLeaves; c++) tot[c] += x[c];
 #pragma unroll
                 for (int c = 0; c < kNumSD; c++) xs[i][c] = x[c];
             }
-            float inc[kNumLeaves];
+            V inc[kNumLeaves];
 #pragma unroll
             for (int c = 0; c < kNumLeaves; c++) inc[c] = tot[c];
 #pragma unroll
             for (int off = 1; off < 8; off <<= 1) {
 #pragma unroll
                 for (int c = 0; c < kNumLeaves; c++) {
-                    const float t = __shfl_up_sync(FULL, inc[c], off);
+                    const V t = __shfl_up_sync(FULL, inc[c], off);
                     if (sl >= off) inc[c] += t;
                 }
             }
@@ -336,7 +410,7 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
                 for (int f = 0; f < kNumFold; f++) S.Cf[card][f] = inc[kNumSD + f];
             }
-            float run[kNumSD], Tc[kNumSD];
+            V run[kNumSD], Tc[kNumSD];
 #pragma unroll
             for (int c = 0; c < kNumSD; c++) {
                 run[c] = inc[c] - tot[c];
@@ -344,15 +418,15 @@ __global__ void __launch_bounds__(NT, 1)
             }
             bool open = false, any = false;
             int cgo = 0;
-            float Wo[kNumSD], Ff[kNumSD];
+            V Wo[kNumSD], Ff[kNumSD];
 #pragma unroll
-            for (int c = 0; c < kNumSD; c++) Wo[c] = Ff[c] = 0.0f;
+            for (int c = 0; c < kNumSD; c++) Wo[c] = Ff[c] = V(0);
 #pragma unroll
             for (int i = 0; i < kCPer; i++) {
                 const uint32_t e = ce[i];
                 if ((e & 2047) != kNoHand && (e & kGroupStart)) {
                     if (open) {
-                        float *dst = S.VC[cgo];
+                        V *dst = S.VC[cgo];
 #pragma unroll
                         for (int c = 0; c < kNumSD; c++) dst[c] = Wo[c] + run[c] - Tc[c];
                     }
@@ -376,7 +450,7 @@ __global__ void __launch_bounds__(NT, 1)
             const int nxt = later ? (lane & ~7) + __ffs(later) - 1 : lane;
 #pragma unroll
             for (int c = 0; c < kNumSD; c++) {
-                const float f = __shfl_sync(FULL, Ff[c], nxt);
+                const V f = __shfl_sync(FULL, Ff[c], nxt);
                 if (open) S.VC[cgo][c] = Wo[c] + (later ? f : Tc[c]) - Tc[c];
             }
         }
@@ -385,25 +459,28 @@ __global__ void __launch_bounds__(NT, 1)
         // ---- per live hand, in bucket order: root value and per-bucket leaf sums ----
         if (warp < kOutWarps) {
             const unsigned FULL = 0xffffffffu;
-            float F[kNumLeaves], L[kNumLeaves];  // first run / last run of this lane's hands
+            float F[kNumLeaves], Lr[kNumLeaves];  // first run / last run of this lane's hands
             int nr = 0, kf = -1, kl = -1;
+            if constexpr (MODE == kModeCFR) {
 #pragma unroll
-            for (int c = 0; c < kNumLeaves; c++) F[c] = L[c] = 0.0f;
+                for (int c = 0; c < kNumLeaves; c++) F[c] = Lr[c] = 0.0f;
+            }
 #pragma unroll
             for (int i = 0; i < kOutPer; i++) {
                 const int j = tid * kOutPer + i;
                 const uint32_t be = j < kLive ? __ldg(&pk->border[j]) : (kNoBucket << 16);
                 const int key = be >> 16;
                 if (key == (int)kNoBucket) continue;
-                float v[kNumLeaves];
+                V v[kNumLeaves];
                 const int h = hand_values(S, pk, be & 0xffff, v);
-                if (MODE == kModeCFR) {
-                    const float4 *wrow = reinterpret_cast<const float4 *>(S.wown[key]);
-                    const float4 w0 = wrow[0], w1 = wrow[1], w2 = wrow[2], w3 = wrow[3], w4 = wrow[4];
-                    float acc = v[0] * w0.x + v[1] * w0.y + v[2] * w0.z + v[3] * w0.w + v[4] * w1.x +
-                                v[5] * w1.y + v[6] * w1.z + v[7] * w1.w + v[8] * w2.x;
-                    acc += v[9] * w3.x + v[10] * w3.y + v[11] * w3.z + v[12] * w3.w + v[13] * w4.x +
-                           v[14] * w4.y + v[15] * w4.z + v[16] * w4.w;
+                if constexpr (MODE == kModeCFR) {
+                    float w[kPioW];
+                    load_row(S.wown[key], w, kPioW);
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int c = 0; c < kNumSD; c++) acc += v[c] * w[c];
+#pragma unroll
+                    for (int f = 0; f < kNumFold; f++) acc += v[kNumSD + f] * w[kFoldCol + f];
                     S.out[h] += acc;
                     // runs of equal buckets; a run strictly inside the lane is a whole bucket
                     if (nr == 0) {
@@ -417,33 +494,31 @@ __global__ void __launch_bounds__(NT, 1)
                             for (int c = 0; c < kNumLeaves; c++) F[c] += v[c];
                         } else {
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) L[c] += v[c];
+                            for (int c = 0; c < kNumLeaves; c++) Lr[c] += v[c];
                         }
                     } else {
                         if (nr >= 2) {
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) S.abar[kl][c] += L[c];
+                            for (int c = 0; c < kNumLeaves; c++) S.abar[kl][c] += Lr[c];
                         }
 #pragma unroll
-                        for (int c = 0; c < kNumLeaves; c++) L[c] = v[c];
+                        for (int c = 0; c < kNumLeaves; c++) Lr[c] = v[c];
                         kl = key;
                         nr = nr + 1;
                     }
                 } else {
-                    // best response: max over the updater's actions, sum over the opponent's
-                    // (state.rs:273-284, poker.cu:437-471)
-                    float A[kStates];
+                    V A[kStates];
 #pragma unroll
-                    for (int Lf = 0; Lf < kNumLeaves; Lf++) A[kLeaf(Lf)] = v[Lf] * S.scale[Lf];
+                    for (int Lf = 0; Lf < kNumLeaves; Lf++) A[kLeaf(Lf)] = v[Lf] * V(S.scale[Lf]);
 #pragma unroll
                     for (int di = kNumDecision - 1; di >= 0; di--) {
                         const int s = kDecision(di);
                         const int nk = kNChild(s);
-                        float acc = A[kChild(s, 0)];
+                        V acc = A[kChild(s, 0)];
                         if (kActor(s) == updater) {
 #pragma unroll
                             for (int k = 1; k < 3; k++)
-                                if (k < nk) acc = fmaxf(acc, A[kChild(s, k)]);
+                                if (k < nk) acc = vmax(acc, A[kChild(s, k)]);
                         } else {
 #pragma unroll
                             for (int k = 1; k < 3; k++)
@@ -454,7 +529,7 @@ __global__ void __launch_bounds__(NT, 1)
                     S.out[h] += A[1];
                 }
             }
-            if (MODE == kModeCFR) {
+            if constexpr (MODE == kModeCFR) {
                 // segmented reduction of bucket runs across the lanes of the warp; runs that
                 // touch the warp's first or last hand are staged for resolve_stage
                 const bool single = nr <= 1;
@@ -467,7 +542,7 @@ __global__ void __launch_bounds__(NT, 1)
                 const int seg_start = 31 - __clz(starts & (FULL >> (31 - lane)));
                 float R[kNumLeaves];
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) R[c] = single ? F[c] : L[c];
+                for (int c = 0; c < kNumLeaves; c++) R[c] = single ? F[c] : Lr[c];
 #pragma unroll
                 for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
@@ -499,7 +574,7 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
                             for (int c = 0; c < kNumLeaves; c++) S.abar[kfirst][c] += Cin[c] + F[c];
                         }
-                        // last run (R == L here) ends here unless the next lane joins it
+                        // last run (R == Lr here) ends here unless the next lane joins it
                         if (lane == 31) {
                             S.stage_key[warp][1] = klast;
 #pragma unroll
@@ -528,87 +603,101 @@ __global__ void __launch_bounds__(NT, 1)
         }
     }
     __syncthreads();
-    if (MODE == kModeCFR) {
+    if constexpr (MODE == kModeCFR) {
         if (warp == NT / 32 - 1 && lane < kNumLeaves) resolve_stage(S, lane);
         __syncthreads();
     }
 
     // ---- results (state.rs:431 / poker.cu:603: mean over the 48 rivers) ----
     {
-        float *dst = results + (size_t)sg * kRangeStride;
-        const float inv = 1.0f / 48.0f;
-        for (int i = tid; i < kRangeStride; i += NT) dst[i] = i < kHands ? S.out[i] * inv : 0.0f;
+        V *dst = results + (size_t)sg * kRangeStride;
+        const V inv = V(1) / V(48);
+        for (int i = tid; i < kRangeStride; i += NT) dst[i] = i < kHands ? S.out[i] * inv : V(0);
     }
 
     // ---- regret update, once per subgame (poker.cu:450-487,524-574) ----
-    if (MODE == kModeCFR && tid < kBuckets) {
-        const int b = tid;
-        float reg[kEdges];
+    if constexpr (MODE == kModeCFR) {
+        if (tid < kBuckets) {
+            const int b = tid;
+            float reg[kEdges];
 #pragma unroll
-        for (int e = 0; e < kEdges; e++) reg[e] = greg[e * kBuckets + b];
-        float A[kStates];
+            for (int e = 0; e < kEdges; e++) reg[e] = greg[e * kBuckets + b];
+            float A[kStates];
 #pragma unroll
-        for (int L = 0; L < kNumLeaves; L++) A[kLeaf(L)] = S.abar[b][L] * S.scale[L];
+            for (int Lf = 0; Lf < kNumLeaves; Lf++) A[kLeaf(Lf)] = S.abar[b][Lf] * S.scale[Lf];
 #pragma unroll
-        for (int di = kNumDecision - 1; di >= 0; di--) {
-            const int s = kDecision(di);
-            const int nk = kNChild(s);
-            if (kActor(s) == updater) {
-                float sum = 0.0f;
+            for (int di = kNumDecision - 1; di >= 0; di--) {
+                const int s = kDecision(di);
+                const int nk = kNChild(s);
+                if (kActor(s) == updater) {
+                    float sum = 0.0f;
 #pragma unroll
-                for (int k = 0; k < 3; k++)
-                    if (k < nk) sum += reg[kEdge(s, k)];
-                float node = 0.0f;
+                    for (int k = 0; k < 3; k++)
+                        if (k < nk) sum += reg[kEdge(s, k)];
+                    float node = 0.0f;
 #pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    if (k < nk) {
-                        const float sig = sum <= 1e-4f ? 1.0f / (float)nk : reg[kEdge(s, k)] / sum;
-                        node += sig * A[kChild(s, k)];
+                    for (int k = 0; k < 3; k++) {
+                        if (k < nk) {
+                            const float sig = sum <= 1e-4f ? 1.0f / (float)nk : reg[kEdge(s, k)] / sum;
+                            node += sig * A[kChild(s, k)];
+                        }
                     }
-                }
-                A[s] = node;
+                    A[s] = node;
 #pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    if (k < nk) {
-                        const int e = kEdge(s, k);
-                        reg[e] = fmaxf(reg[e] + (A[kChild(s, k)] - node), 0.0f);
-                        greg[e * kBuckets + b] = reg[e];
+                    for (int k = 0; k < 3; k++) {
+                        if (k < nk) {
+                            const int e = kEdge(s, k);
+                            reg[e] = fmaxf(reg[e] + (A[kChild(s, k)] - node), 0.0f);
+                            greg[e * kBuckets + b] = reg[e];
+                        }
                     }
-                }
-            } else {
-                float node = 0.0f;
+                } else {
+                    float node = 0.0f;
 #pragma unroll
-                for (int k = 0; k < 3; k++)
-                    if (k < nk) node += A[kChild(s, k)];
-                A[s] = node;
+                    for (int k = 0; k < 3; k++)
+                        if (k < nk) node += A[kChild(s, k)];
+                    A[s] = node;
+                }
             }
         }
     }
 }
 
+template <int MODE, typename V>
+cudaError_t launch_one(const SubgameDesc *desc, int n, const V *ranges, V *results, float *regrets,
+                       const BoardPack *packs, unsigned long long flop, int updater, int max_groups,
+                       int max_card_groups, cudaStream_t stream) {
+    const Layout L = make_layout(MODE == kModeCFR, sizeof(V), max_groups, max_card_groups);
+    if (L.total > 227u * 1024u) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(river_kernel<MODE, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)L.total);
+    if (e != cudaSuccess) return e;
+    river_kernel<MODE, V><<<n, NT, L.total, stream>>>(desc, ranges, results, regrets, packs, flop, updater,
+                                                      max_groups, max_card_groups);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
-size_t river_smem_bytes() { return sizeof(Smem); }
+size_t river_smem_bytes(int mode, int fp64, int max_groups, int max_card_groups) {
+    return make_layout(mode == kModeCFR, fp64 ? 8 : 4, max_groups, max_card_groups).total;
+}
 
-cudaError_t launch_river(int mode, const SubgameDesc *desc, int n, const float *ranges,
-                         float *results, float *regrets, const BoardPack *packs,
-                         unsigned long long flop, int updater, cudaStream_t stream) {
-    const size_t smem = sizeof(Smem);
-    cudaError_t e;
-    if (mode == kModeCFR) {
-        e = cudaFuncSetAttribute(river_kernel<kModeCFR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        river_kernel<kModeCFR><<<n, NT, smem, stream>>>(desc, ranges, results, regrets, packs, flop,
-                                                        updater);
-    } else {
-        e = cudaFuncSetAttribute(river_kernel<kModeBR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        river_kernel<kModeBR><<<n, NT, smem, stream>>>(desc, ranges, results, regrets, packs, flop,
-                                                       updater);
-    }
-    return cudaGetLastError();
+cudaError_t launch_river(int mode, const SubgameDesc *desc, int n, const float *ranges, float *results,
+                         float *regrets, const BoardPack *packs, unsigned long long flop, int updater,
+                         int max_groups, int max_card_groups, cudaStream_t stream) {
+    if (mode == kModeCFR)
+        return launch_one<kModeCFR, float>(desc, n, ranges, results, regrets, packs, flop, updater, max_groups,
+                                           max_card_groups, stream);
+    return launch_one<kModeBR, float>(desc, n, ranges, results, regrets, packs, flop, updater, max_groups,
+                                      max_card_groups, stream);
+}
+
+cudaError_t launch_river_br64(const SubgameDesc *desc, int n, const double *ranges, double *results,
+                              float *regrets, const BoardPack *packs, unsigned long long flop, int updater,
+                              int max_groups, int max_card_groups, cudaStream_t stream) {
+    return launch_one<kModeBR, double>(desc, n, ranges, results, regrets, packs, flop, updater, max_groups,
+                                       max_card_groups, stream);
 }
 
 }  // namespace prb

@@ -8,13 +8,20 @@ namespace prb {
 
 enum { kModeCFR = 0, kModeBR = 1 };
 
-size_t river_smem_bytes();
+// Shared memory per CTA for a pass; max_groups / max_card_groups are the largest tie-group
+// counts over the flop's boards.
+size_t river_smem_bytes(int mode, int fp64, int max_groups, int max_card_groups);
 
 // One pass over n river subgames: CFR (regret update of `updater`'s edges, results are
 // counterfactual values) or best response (results are best-response values, regrets
-// read only). ranges / results: n rows of kRangeStride floats; regrets: n * 26 * 256.
-cudaError_t launch_river(int mode, const SubgameDesc *desc, int n, const float *ranges,
-                         float *results, float *regrets, const BoardPack *packs,
-                         unsigned long long flop, int updater, cudaStream_t stream);
+// read only). ranges / results: n rows of kRangeStride values; regrets: n * 26 * 256.
+cudaError_t launch_river(int mode, const SubgameDesc *desc, int n, const float *ranges, float *results,
+                         float *regrets, const BoardPack *packs, unsigned long long flop, int updater,
+                         int max_groups, int max_card_groups, cudaStream_t stream);
+
+// Best response in double precision.
+cudaError_t launch_river_br64(const SubgameDesc *desc, int n, const double *ranges, double *results,
+                              float *regrets, const BoardPack *packs, unsigned long long flop, int updater,
+                              int max_groups, int max_card_groups, cudaStream_t stream);
 
 }  // namespace prb

@@ -69,6 +69,9 @@ def lib():
         L.pr_eval_status.restype = i32
         L.pr_eval_status.argtypes = [vp]
         L.pr_river_smem_bytes.restype = ctypes.c_size_t
+        L.pr_river_smem_bytes.argtypes = [vp, i32, i32]
+        L.pr_evaluate_br64.restype = i32
+        L.pr_evaluate_br64.argtypes = [vp, vp, i32, vp, vp]
         L.pr_tables_build.restype = vp
         L.pr_tables_build.argtypes = [u64]
         L.pr_tables_export.restype = i32
@@ -203,6 +206,15 @@ class Builder:
 
     def evaluate(self, tables, updating_player, calc_exploit=False):
         _check(lib().pr_evaluate(self.ptr, tables, int(updating_player), int(bool(calc_exploit))), "pr_evaluate")
+
+    def best_response_f64(self, tables, updating_player, ranges):
+        """Double-precision best-response values for every subgame (count x 1326)."""
+        ranges = np.ascontiguousarray(ranges, dtype=np.float64)
+        assert ranges.shape == (self.count, HANDS)
+        out = np.zeros((self.count, HANDS), np.float64)
+        _check(lib().pr_evaluate_br64(self.ptr, tables, int(updating_player), _ptr(ranges), _ptr(out)),
+               "pr_evaluate_br64")
+        return out
 
     def evaluate_device(self, tables, updating_player, calc_exploit, d_ranges, d_results, stream=None):
         _check(lib().pr_evaluate_device(self.ptr, tables, int(updating_player), int(bool(calc_exploit)),

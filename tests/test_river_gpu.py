@@ -237,3 +237,32 @@ def test_full_fixed_flop_pass_sampled(P, gpu_tables, flop_tables):
     assert np.all(np.isfinite(got))
     assert np.all(got[(order[None, :] & boards[:, None]) != 0] == 0)
     assert np.all(got_reg >= 0)
+
+
+@pytest.mark.parametrize("player", [0, 1])
+def test_best_response_double_precision(P, gpu_tables, flop_tables, player):
+    # the double-precision best response against the oracle's double traversal; the only
+    # differences are summation orders, so the bound is far tighter than in single precision
+    rng = np.random.default_rng(40 + player)
+    board4, bet, opp = subgames(rng, 10)
+    reg = random_regrets(rng, 10)
+    e, _, a = flop_tables
+    b = P.Builder()
+    for cards, bt in zip(board4, bet):
+        b.add(int(cards), float(bt))
+    b.set_regrets(reg)
+    got = b.best_response_f64(gpu_tables, player, opp.astype(np.float64))
+    assert np.array_equal(b.regrets(), reg)
+    b.close()
+    want = O.river_br_f64(O.REFERENCE_FLOP, e, a, board4, bet.astype(np.float64), opp.astype(np.float64),
+                          reg, player)
+    for i in range(10):
+        scale = np.abs(want[i]).max()
+        assert np.abs(got[i] - want[i]).max() <= 1e-9 * scale
+
+
+def test_shared_memory_sized_by_flop(P, gpu_tables):
+    # group arrays are sized by the flop's largest tie-group counts and fit one CTA per SM
+    for exploit, fp64 in ((0, 0), (1, 0), (1, 1)):
+        smem = P.lib().pr_river_smem_bytes(gpu_tables, exploit, fp64)
+        assert 0 < smem <= 227 * 1024
