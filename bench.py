@@ -31,6 +31,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SUBGAMES = 27783                 # 63 * 49 * 9 river roots (interface.cu:17)
+REFERENCE_FLOP = 0b111           # cards {0, 1, 2} = 2c 3c 4c, the reference's fixed flop
 NODES_PER_SUBGAME = 48 * 27      # 48 river cards x 27 states below the river root
 METRIC = "river-subtree CFR throughput, fixed-flop game (river node visits/s)"
 UNIT = "nodes/s"
@@ -98,17 +99,9 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def game_roots():
-    """River roots (4-card board, bet) of the fixed-flop game in builder order."""
-    from oracle import oracle as O  # the game's river roots only; the pass never runs on it
-    g = O.Game(O.REFERENCE_FLOP)
-    return g.river_roots()
-
-
-def synthetic_ranges(boards, seed=1234):
-    from oracle import oracle as O
+def synthetic_ranges(order, boards, seed=1234):
+    """Seeded opponent ranges: U(0,1) per hand, zero on hands that hit the 4-card board."""
     rng = np.random.default_rng(seed)
-    order = O.card_order()
     r = rng.random((len(boards), 1326), dtype=np.float32)
     r[(order[None, :] & boards[:, None]) != 0] = 0.0
     return r
@@ -137,10 +130,11 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    from oracle import oracle as O
+    from oracle import oracle as O  # the reference's CPU path (restated), timed here
     nthreads = os.cpu_count() or 1
-    boards, bets = game_roots()
-    ranges = synthetic_ranges(boards)
+    game = O.Game(O.REFERENCE_FLOP, nthreads)
+    boards, bets = game.river_roots()
+    ranges = synthetic_ranges(O.card_order(), boards)
     tables = O.pack_flop_tables(O.REFERENCE_FLOP, nthreads)
     sample = max(8 * nthreads, 64)
     for _ in range(args.warmup):
@@ -176,19 +170,20 @@ def run_gpu(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     import pokerrust_b200 as P
-    from oracle import oracle as O  # table generation and the CPU baseline only
 
-    boards, bets = game_roots()
+    # the game, its river roots and its hand-rank tables, all built by the library
+    game = P.Game(REFERENCE_FLOP)
+    boards, bets = game.river_roots()
+    tables = game.tables
     if args.subgames:
         boards, bets = boards[:args.subgames], bets[:args.subgames]
+        builder = P.Builder()
+        for cards, bt in zip(boards, bets):
+            builder.add(int(cards), float(bt))
+    else:
+        builder = P.Builder.wrap(game.builder)   # owned by the game
     n = len(boards)
-    ranges = synthetic_ranges(boards, seed=1234 + rank)
-    tables_host = O.pack_flop_tables(O.REFERENCE_FLOP)
-    e, c, a = tables_host
-    tables = P.transfer_flop_eval(O.REFERENCE_FLOP, O.card_order(), O.card_indexes(), e, c, a)
-    builder = P.Builder()
-    for cards, bt in zip(boards, bets):
-        builder.add(int(cards), float(bt))
+    ranges = synthetic_ranges(P.card_order(), boards, seed=1234 + rank)
     stride = P.RANGE_STRIDE
     d_ranges = torch.zeros((n, stride), dtype=torch.float32, device=dev)
     d_ranges[:, :1326] = torch.from_numpy(ranges).to(dev)
@@ -229,8 +224,9 @@ def run_gpu(args):
         if rank == 0:
             print(json.dumps({"profile": True, "subgames": n, "kernel_ms": kernel_ms,
                               "value": value, "unit": UNIT}), flush=True)
-        builder.close()
-        P.free_eval(tables)
+        if args.subgames:
+            builder.close()
+        game.close()
         if world > 1:
             torch.distributed.destroy_process_group()
         return 0
@@ -255,12 +251,24 @@ def run_gpu(args):
     e2e_s = float(t.item())
     assert np.all(np.isfinite(out))
 
+    # whole-game CFR iterations through the library's game driver (game.rs:68-119):
+    # host traversal of the upper tree + one device pass per player
+    torch.cuda.synchronize(dev)
+    game.iterate(1)
+    h0, d0 = game.timings()
+    t0 = time.perf_counter()
+    game.iterate(2)
+    iter_s = (time.perf_counter() - t0) / 2
+    h1, d1 = game.timings()
+
     line = None
     if rank == 0:
+        from oracle import oracle as O  # CPU baseline only
         peak, peak_kind = measured_peaks()
         ab = algorithmic_bytes(n)
         achieved = ab / (kernel_ms / 1e3) / 1e9
         cpu_threads = os.cpu_count() or 1
+        tables_host = O.pack_flop_tables(O.REFERENCE_FLOP, cpu_threads)
         cpu_rate, cpu_dt = cpu_sample(boards, bets, ranges, tables_host, cpu_threads, max(8 * cpu_threads, 64))
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -283,10 +291,15 @@ def run_gpu(args):
                                        f"{cpu_dt:.2f} s, scaled to nodes/s"},
             "gpu_launches": args.steps,
             "clocks": clk,
+            "game_iteration": {"ms": iter_s * 1e3, "host_ms": (h1 - h0) / 2 * 1e3,
+                               "device_ms": (d1 - d0) / 2 * 1e3,
+                               "note": "one full CFR iteration of the fixed-flop game (both players), "
+                                       "upper tree on the host, river passes through evaluate_cuda"},
         }
         print(json.dumps(line), flush=True)
-    builder.close()
-    P.free_eval(tables)
+    if args.subgames:
+        builder.close()
+    game.close()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

@@ -118,6 +118,31 @@ size_t pr_river_smem_bytes(void *eval, int calc_exploit, int fp64);
 int pr_evaluate_br64(void *builder, void *eval, int updating_player, const double *ranges,
                      double *results);
 
+/* ---- whole-game driver (extension): the host side of the reference's GPU build ----
+ * (src/builder.rs, src/state.rs, src/strategy.rs:37-82, src/permutation_handler.rs,
+ * src/game.rs) over the functions above. Tables are built on the device. */
+
+/* Builds the fixed-flop game (preflop, the given flop, turn, river roots); nthreads <= 0
+ * uses every core for the turn cards. Null on failure (see pr_last_error). */
+void *pr_game_new(uint64_t flop, int nthreads);
+void pr_game_free(void *game);
+int pr_game_num_rivers(void *game);
+/* River roots (4-card board, equal bet) in the order the game registers them. */
+int pr_game_river_roots(void *game, uint64_t *boards, float *bets);
+/* The game's river builder and table handle, for the functions above. */
+void *pr_game_builder(void *game);
+void *pr_game_tables(void *game);
+/* CFR iterations (game.rs:68-119): small blind update, then big blind update. */
+int pr_game_iterate(void *game, int iterations);
+/* Best-response sums of both players and the reference's mb/h figure (game.rs:120-178);
+ * fp64 = 1 runs the whole best response in double precision. */
+int pr_game_exploitability(void *game, int fp64, double *sum_sb, double *sum_bb, double *mbh);
+/* Seconds spent so far in host traversal and in device passes. */
+int pr_game_timings(void *game, double *host_seconds, double *device_seconds);
+/* Upper-tree regrets (pr_game_upper_regret_count floats, node order) and river regrets. */
+size_t pr_game_upper_regret_count(void *game);
+int pr_game_get_regrets(void *game, float *upper, float *river);
+
 #ifdef __cplusplus
 }
 #endif

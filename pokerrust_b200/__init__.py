@@ -8,9 +8,11 @@ from .interface import (  # noqa: F401
     HANDS,
     RANGE_STRIDE,
     Builder,
+    Game,
     PokerLibError,
     build_flop_tables,
     build_river,
+    card_order,
     download_gpu,
     evaluate_gpu,
     export_tables,

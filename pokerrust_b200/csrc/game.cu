@@ -1,0 +1,608 @@
+// Host driver of the whole fixed-flop game over the C ABI: the part of the reference's
+// `--features GPU` program above the river solver (src/builder.rs, src/state.rs,
+// src/strategy.rs:37-82, src/permutation_handler.rs, src/game.rs), as a C++ library.
+//
+// The preflop, flop and turn tree is built from the reference's rules (builder.rs:13-79,
+// state.rs:66-217) into flat node arrays; the river roots it reaches are registered with
+// build_river_cuda in the same order the reference registers them. A half-iteration is the
+// reference's GPU protocol (game.rs:68-119): an upload pass that stores every river root's
+// opponent range in the staging (state.rs:379-387), one evaluate_cuda, and a download pass
+// that reads the river values back and updates the upper-tree regrets (state.rs:219-296,
+// strategy.rs:57-66). Turn children run on a thread pool (state.rs:340-341 uses rayon).
+// The upload pass only propagates ranges: in the reference its utilities are discarded.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <functional>
+#include <limits>
+#include <mutex>
+#include <set>
+#include <thread>
+#include <vector>
+
+#include "../../include/pokerrust_b200.h"
+
+namespace prb {
+namespace {
+
+constexpr int H = 1326;
+enum Kind : int8_t { kDecide = 0, kSBWins = 1, kBBWins = 2, kFlop = 4, kTurn = 5, kRiverRoot = 6 };
+enum Act : int8_t { Fold, Check, Call, Raise, DealHole, DealFlop, DealTurn, DealRiver };
+
+struct UNode {
+    int8_t kind, actor, action, nchild;
+    int32_t first;       // first child in `kids`
+    uint64_t cards;
+    float sb, bb;
+    int64_t regret;      // offset of nchild * H regrets (decision nodes)
+    int32_t river;       // river root index (kRiverRoot)
+    int32_t perm_first;  // flop nodes: suit permutations [perm_first, perm_first + nperm)
+    int32_t nperm;
+};
+
+// Thread pool with a blocking parallel-for; the caller works too.
+class Pool {
+  public:
+    explicit Pool(int n) {
+        for (int i = 0; i < n; i++) workers_.emplace_back([this] { loop(); });
+    }
+    ~Pool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : workers_) t.join();
+    }
+    void run(int n, const std::function<void(int)> &f) {
+        if (workers_.empty() || n <= 1) {
+            for (int i = 0; i < n; i++) f(i);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job_ = &f;
+            n_ = n;
+            next_.store(0);
+            active_ = (int)workers_.size();
+            gen_++;
+        }
+        cv_.notify_all();
+        for (int i; (i = next_.fetch_add(1)) < n;) f(i);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [this] { return active_ == 0; });
+        job_ = nullptr;
+    }
+    int size() const { return (int)workers_.size() + 1; }
+
+  private:
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            const std::function<void(int)> *job;
+            int n;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                job = job_;
+                n = n_;
+            }
+            for (int i; (i = next_.fetch_add(1)) < n;) (*job)(i);
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--active_ == 0) done_cv_.notify_all();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(int)> *job_ = nullptr;
+    int n_ = 0, active_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+    std::atomic<int> next_{0};
+};
+
+// Per-thread scratch: vectors of H values per recursion depth.
+template <typename T>
+struct Scratch {
+    static constexpr int kSlots = 9;  // avg, 3 strategies, child range, 3 results, misc
+    std::vector<T> buf;
+    explicit Scratch(int depth) : buf((size_t)depth * kSlots * H) {}
+    T *at(int depth, int slot) { return buf.data() + ((size_t)depth * kSlots + slot) * H; }
+};
+
+enum Pass { kUpload = 0, kDownload = 1 };
+
+struct Game {
+    uint64_t flop = 0;
+    void *tables = nullptr;
+    void *builder = nullptr;
+    std::vector<UNode> nodes;
+    std::vector<int32_t> kids;
+    std::vector<float> regrets;
+    std::vector<std::array<int, 4>> perms;
+    std::vector<std::vector<int32_t>> perm_maps;  // hand index -> permuted hand index
+    std::vector<uint64_t> card_order;
+    std::vector<uint64_t> river_board;
+    std::vector<float> river_bet;
+    std::vector<double> ranges64, results64;      // double-precision best-response staging
+    Pool *pool = nullptr;
+    int max_depth = 0;
+    double t_host = 0, t_gpu = 0;
+    int status = 0;
+
+    // ---- tree construction (builder.rs:34-79, state.rs:66-217) ----
+    static int popc(uint64_t x) { return __builtin_popcountll(x); }
+
+    void possible(const UNode &s, int raises, std::vector<int> &out) const {
+        out.clear();
+        switch (s.action) {
+            case Fold: break;
+            case Check: out = {Call, Raise}; break;
+            case Call:
+                if (popc(s.cards) == 0) out = {DealFlop};
+                else if (popc(s.cards) == 3) out = {DealTurn};
+                break;  // 4 cards: a river root, solved on the device
+            case Raise:
+                out = {Fold, Call};
+                if (raises < 4) out.push_back(Raise);
+                break;
+            case DealHole: out = {Fold, Check, Raise}; break;
+            default: out = {Check, Raise}; break;
+        }
+    }
+
+    static uint64_t permute_cards(uint64_t cards, const std::array<int, 4> &p) {
+        uint64_t o = 0;
+        while (cards) {
+            const int c = __builtin_ctzll(cards);
+            cards &= cards - 1;
+            o |= 1ull << (13 * p[c / 13] + c % 13);
+        }
+        return o;
+    }
+
+    static int colex2(uint64_t set) {
+        const int a = __builtin_ctzll(set);
+        set &= set - 1;
+        const int b = __builtin_ctzll(set);
+        return a + b * (b - 1) / 2;
+    }
+
+    // children states of `s` for `action` (state.rs:66-217)
+    void children_of(const UNode &s, int action, std::vector<UNode> &out) {
+        out.clear();
+        UNode t{};
+        t.kind = s.kind;
+        t.action = (int8_t)action;
+        t.cards = s.cards;
+        t.sb = s.sb;
+        t.bb = s.bb;
+        t.actor = s.actor == 0 ? 1 : 0;
+        t.river = -1;
+        const float other = s.actor == 0 ? s.bb : s.sb;
+        switch (action) {
+            case Fold: t.kind = s.actor == 0 ? kBBWins : kSBWins; break;
+            case Check:
+                t.kind = kDecide;
+                t.sb = s.bb;
+                break;
+            case Call:
+                t.sb = t.bb = other;
+                if (popc(s.cards) == 0) {
+                    t.kind = kFlop;
+                } else if (popc(s.cards) == 3) {
+                    t.kind = kTurn;
+                } else {
+                    t.kind = kRiverRoot;
+                    t.river = (int)river_board.size();
+                    river_board.push_back(s.cards);
+                    river_bet.push_back(other);
+                }
+                break;
+            case Raise: {
+                const float amount = popc(s.cards) < 4 ? 1.0f : 2.0f;
+                t.kind = kDecide;
+                if (s.actor == 0) t.sb = s.bb + amount;
+                else t.bb = s.sb + amount;
+                break;
+            }
+            case DealFlop: {
+                // the one fixed flop and the suit permutations of [C, H, S, D], in
+                // lexicographic order, that reach a flop not seen before (state.rs:146-172)
+                std::set<uint64_t> seen;
+                std::array<int, 4> p = {0, 1, 2, 3};
+                t.perm_first = (int)perms.size();
+                t.nperm = 0;
+                do {
+                    if (seen.insert(permute_cards(flop, p)).second) {
+                        perms.push_back(p);
+                        t.nperm++;
+                    }
+                } while (std::next_permutation(p.begin(), p.end()));
+                t.kind = kDecide;
+                t.cards = flop;
+                t.actor = 0;
+                break;
+            }
+            case DealTurn:
+                for (int c = 0; c < 52; c++) {
+                    if ((s.cards >> c) & 1) continue;
+                    UNode n = t;
+                    n.kind = kDecide;
+                    n.cards = s.cards | (1ull << c);
+                    n.actor = 0;
+                    out.push_back(n);
+                }
+                return;
+        }
+        out.push_back(t);
+    }
+
+    int build(int si, int raises, int depth) {
+        max_depth = std::max(max_depth, depth + 1);
+        std::vector<int> acts;
+        possible(nodes[si], raises, acts);
+        std::vector<int> kids_here;
+        std::vector<UNode> ch;
+        for (int a : acts) {
+            const int nr = a == Raise ? raises + 1 : (a == DealFlop || a == DealTurn) ? 0 : raises;
+            children_of(nodes[si], a, ch);
+            for (UNode &c : ch) {
+                const int ci = (int)nodes.size();
+                nodes.push_back(c);
+                build(ci, nr, depth + 1);
+                kids_here.push_back(ci);
+            }
+        }
+        UNode &s = nodes[si];
+        s.first = (int)kids.size();
+        s.nchild = (int8_t)kids_here.size();
+        kids.insert(kids.end(), kids_here.begin(), kids_here.end());
+        if (s.kind == kDecide && s.nchild > 0) {
+            s.regret = (int64_t)regrets.size();
+            regrets.resize(regrets.size() + (size_t)s.nchild * H, 0.0f);
+        }
+        return si;
+    }
+
+    bool init(uint64_t f, int nthreads) {
+        flop = f;
+        card_order.resize(H);
+        for (int hi = 1, n = 0; hi < 52; hi++)
+            for (int lo = 0; lo < hi; lo++) card_order[n++] = (1ull << lo) | (1ull << hi);
+        UNode root{};
+        root.kind = kDecide;
+        root.action = DealHole;
+        root.sb = 0.5f;
+        root.bb = 1.0f;
+        root.actor = 0;
+        root.river = -1;
+        nodes.reserve(1 << 18);
+        nodes.push_back(root);
+        build(0, 1, 0);
+        perm_maps.resize(perms.size());
+        for (size_t i = 0; i < perms.size(); i++) {
+            perm_maps[i].resize(H);
+            for (int h = 0; h < H; h++) perm_maps[i][h] = colex2(permute_cards(card_order[h], perms[i]));
+        }
+        tables = pr_tables_build(flop);
+        if (!tables || pr_eval_status(tables) != 0) return false;
+        builder = init_builder();
+        if (!builder) return false;
+        for (size_t i = 0; i < river_board.size(); i++)
+            if (build_river_cuda(river_board[i], river_bet[i], builder) != (int)i) return false;
+        if (nthreads <= 0) nthreads = (int)std::thread::hardware_concurrency();
+        pool = new Pool(std::max(0, nthreads - 1));
+        return true;
+    }
+
+    ~Game() {
+        delete pool;
+        if (builder) pr_free_builder(builder);
+        if (tables) free_eval_cuda(tables);
+    }
+
+    // ---- traversal (state.rs:219-376) ----
+    template <typename T>
+    void strategy(const UNode &s, T *probs) const {
+        // RegularStrategy::get_strategy (strategy.rs:68-81)
+        const float *r = regrets.data() + s.regret;
+        const int n = s.nchild;
+        for (int i = 0; i < H; i++) {
+            T sum = T(0);
+            for (int k = 0; k < n; k++) sum += T(r[(size_t)k * H + i]);
+            for (int k = 0; k < n; k++)
+                probs[(size_t)k * H + i] = sum <= T(1e-4f) ? T(1) / T(n) : T(r[(size_t)k * H + i]) / sum;
+        }
+    }
+
+    template <typename T>
+    void fold(const UNode &s, const T *opp, int upd, int folding, T *out) const {
+        // evaluate_fold (state.rs:456-492)
+        T total = T(0);
+        T coll[52] = {};
+        for (int i = 0; i < H; i++) {
+            total += opp[i];
+            coll[__builtin_ctzll(card_order[i])] += opp[i];
+            coll[63 - __builtin_clzll(card_order[i])] += opp[i];
+        }
+        const T b = T(folding == 0 ? s.sb : s.bb);
+        const T m = b * (upd == folding ? T(-1) : T(1));
+        for (int i = 0; i < H; i++) {
+            T v = total + opp[i];
+            v -= coll[__builtin_ctzll(card_order[i])];
+            v -= coll[63 - __builtin_clzll(card_order[i])];
+            out[i] = v * m;
+        }
+    }
+
+    template <typename T>
+    void river(const UNode &s, const T *opp, int pass, T *out);
+
+    template <typename T>
+    void eval(int si, const T *sb, const T *bb, int upd, bool br, int pass, T *out, int depth,
+              Scratch<T> &sc) {
+        const UNode &s = nodes[si];
+        const T *opp = upd == 0 ? bb : sb;
+        switch (s.kind) {
+            case kDecide: {
+                T *avg = sc.at(depth, 0);
+                T *probs = sc.at(depth, 1);  // slots 1..3
+                T *child = sc.at(depth, 4);
+                T *res = sc.at(depth, 5);    // slots 5..7
+                T *u = sc.at(depth, 8);
+                strategy(s, probs);
+                const bool mine = upd == s.actor;
+                const T init = (mine && br) ? -std::numeric_limits<T>::infinity() : T(0);
+                for (int i = 0; i < H; i++) avg[i] = init;
+                for (int k = 0; k < s.nchild; k++) {
+                    const T *p = probs + (size_t)k * H;
+                    const T *own = s.actor == 0 ? sb : bb;
+                    for (int i = 0; i < H; i++) child[i] = own[i] * p[i];
+                    T *uk = (mine && !br) ? res + (size_t)k * H : u;
+                    if (s.actor == 0) eval(kids[s.first + k], child, bb, upd, br, pass, uk, depth + 1, sc);
+                    else eval(kids[s.first + k], sb, child, upd, br, pass, uk, depth + 1, sc);
+                    if (pass == kUpload) continue;  // no utilities in the upload pass
+                    if (mine) {
+                        if (!br) for (int i = 0; i < H; i++) avg[i] += uk[i] * p[i];
+                        else for (int i = 0; i < H; i++) avg[i] = std::fmax(avg[i], uk[i]);
+                    } else {
+                        for (int i = 0; i < H; i++) avg[i] += uk[i];
+                    }
+                }
+                if (pass == kDownload && mine && !br) {
+                    // RegularStrategy::update_add (strategy.rs:57-66)
+                    float *r = regrets.data() + s.regret;
+                    for (int k = 0; k < s.nchild; k++)
+                        for (int i = 0; i < H; i++) {
+                            float &x = r[(size_t)k * H + i];
+                            x = std::fmax(x + float(res[(size_t)k * H + i] - avg[i]), 0.0f);
+                        }
+                }
+                memcpy(out, avg, sizeof(T) * H);
+                return;
+            }
+            case kSBWins:
+                if (pass == kDownload) fold(s, opp, upd, 1, out);
+                return;
+            case kBBWins:
+                if (pass == kDownload) fold(s, opp, upd, 0, out);
+                return;
+            case kFlop: {
+                // state.rs:301-336: mask, evaluate, mask, average over suit permutations
+                T *nsb = sc.at(depth, 0), *nbb = sc.at(depth, 1), *r = sc.at(depth, 2);
+                T *tot = sc.at(depth, 3);
+                for (int i = 0; i < H; i++) tot[i] = T(0);
+                T count = T(0);
+                for (int k = 0; k < s.nchild; k++) {
+                    const UNode &c = nodes[kids[s.first + k]];
+                    for (int i = 0; i < H; i++) {
+                        const bool blocked = card_order[i] & c.cards;
+                        nsb[i] = blocked ? T(0) : sb[i];
+                        nbb[i] = blocked ? T(0) : bb[i];
+                    }
+                    eval(kids[s.first + k], nsb, nbb, upd, br, pass, r, depth + 1, sc);
+                    if (pass == kUpload) continue;
+                    for (int i = 0; i < H; i++)
+                        if (card_order[i] & c.cards) r[i] = T(0);
+                    for (int p = 0; p < c.nperm; p++) {
+                        count += T(1);
+                        const int32_t *map = perm_maps[c.perm_first + p].data();
+                        for (int i = 0; i < H; i++) tot[map[i]] += r[i];
+                    }
+                }
+                if (pass == kDownload) {
+                    const T scale = T(1) / count;
+                    for (int i = 0; i < H; i++) out[i] = tot[i] * scale;
+                }
+                return;
+            }
+            case kTurn: {
+                // state.rs:337-376: the 49 turn cards in parallel, then their mean
+                const int n = s.nchild;
+                std::vector<T> res((size_t)n * H);
+                pool->run(n, [&](int k) {
+                    thread_local Scratch<T> *tsc = nullptr;
+                    thread_local int tsc_depth = 0;
+                    if (!tsc || tsc_depth < max_depth + 2) {
+                        delete tsc;
+                        tsc = new Scratch<T>(max_depth + 2);
+                        tsc_depth = max_depth + 2;
+                    }
+                    const UNode &c = nodes[kids[s.first + k]];
+                    T *nsb = tsc->at(depth, 0), *nbb = tsc->at(depth, 1);
+                    for (int i = 0; i < H; i++) {
+                        const bool blocked = card_order[i] & c.cards;
+                        nsb[i] = blocked ? T(0) : sb[i];
+                        nbb[i] = blocked ? T(0) : bb[i];
+                    }
+                    T *r = res.data() + (size_t)k * H;
+                    eval(kids[s.first + k], nsb, nbb, upd, br, pass, r, depth + 1, *tsc);
+                    if (pass == kDownload)
+                        for (int i = 0; i < H; i++)
+                            if (card_order[i] & c.cards) r[i] = T(0);
+                });
+                if (pass == kDownload) {
+                    for (int i = 0; i < H; i++) out[i] = T(0);
+                    for (int k = 0; k < n; k++)
+                        for (int i = 0; i < H; i++) out[i] += res[(size_t)k * H + i];
+                    const T scale = T(1) / T(n);
+                    for (int i = 0; i < H; i++) out[i] *= scale;
+                }
+                return;
+            }
+            case kRiverRoot:
+                river(s, opp, pass, out);
+                return;
+        }
+    }
+
+    // One half-iteration or best-response pass of `upd` (game.rs:73-96 / 122-168).
+    template <typename T>
+    int half(int upd, bool br, T *out) {
+        using clk = std::chrono::steady_clock;
+        Scratch<T> sc(max_depth + 2);
+        std::vector<T> ones(H, T(1));
+        auto t0 = clk::now();
+        eval<T>(0, ones.data(), ones.data(), upd, br, kUpload, out, 0, sc);
+        auto t1 = clk::now();
+        int st;
+        if (sizeof(T) == 8) {
+            st = pr_evaluate_br64(builder, tables, upd, ranges64.data(), results64.data());
+        } else {
+            st = pr_evaluate(builder, tables, upd, br ? 1 : 0);
+        }
+        auto t2 = clk::now();
+        if (st) return st;
+        eval<T>(0, ones.data(), ones.data(), upd, br, kDownload, out, 0, sc);
+        auto t3 = clk::now();
+        t_host += std::chrono::duration<double>((t1 - t0) + (t3 - t2)).count();
+        t_gpu += std::chrono::duration<double>(t2 - t1).count();
+        return 0;
+    }
+};
+
+template <>
+void Game::river<float>(const UNode &s, const float *opp, int pass, float *out) {
+    // state.rs:378-389: stage the opponent range, or read the device's values back
+    if (pass == kUpload) upload_c(builder, s.river, opp);
+    else download_c(builder, s.river, out);
+}
+
+template <>
+void Game::river<double>(const UNode &s, const double *opp, int pass, double *out) {
+    if (pass == kUpload) memcpy(ranges64.data() + (size_t)s.river * H, opp, sizeof(double) * H);
+    else memcpy(out, results64.data() + (size_t)s.river * H, sizeof(double) * H);
+}
+
+}  // namespace
+}  // namespace prb
+
+using prb::Game;
+
+extern "C" {
+
+void *pr_game_new(uint64_t flop, int nthreads) {
+    Game *g = new Game();
+    if (!g->init(flop, nthreads)) {
+        delete g;
+        return nullptr;
+    }
+    return g;
+}
+
+void pr_game_free(void *game) { delete (Game *)game; }
+
+int pr_game_num_rivers(void *game) { return game ? (int)((Game *)game)->river_board.size() : 0; }
+
+int pr_game_river_roots(void *game, uint64_t *boards, float *bets) {
+    Game *g = (Game *)game;
+    if (!g || !boards || !bets) return 2;
+    for (size_t i = 0; i < g->river_board.size(); i++) {
+        boards[i] = g->river_board[i];
+        bets[i] = g->river_bet[i];
+    }
+    return 0;
+}
+
+void *pr_game_builder(void *game) { return game ? ((Game *)game)->builder : nullptr; }
+void *pr_game_tables(void *game) { return game ? ((Game *)game)->tables : nullptr; }
+
+int pr_game_iterate(void *game, int iterations) {
+    Game *g = (Game *)game;
+    if (!g) return 2;
+    std::vector<float> out(prb::H);
+    for (int it = 0; it < iterations; it++) {
+        for (int upd = 0; upd < 2; upd++) {
+            const int st = g->half<float>(upd, false, out.data());
+            if (st) return st;
+        }
+    }
+    return 0;
+}
+
+int pr_game_exploitability(void *game, int fp64, double *sum_sb, double *sum_bb, double *mbh) {
+    Game *g = (Game *)game;
+    if (!g) return 2;
+    if (fp64) {
+        const size_t n = g->river_board.size() * prb::H;
+        g->ranges64.assign(n, 0.0);
+        g->results64.assign(n, 0.0);
+        std::vector<double> sb(prb::H), bb(prb::H);
+        int st = g->half<double>(0, true, sb.data());
+        if (!st) st = g->half<double>(1, true, bb.data());
+        if (st) return st;
+        double s1 = 0, s2 = 0;
+        for (int i = 0; i < prb::H; i++) {
+            s1 += sb[i];
+            s2 += bb[i];
+        }
+        *sum_sb = s1;
+        *sum_bb = s2;
+        *mbh = (s1 + s2) * 1000.0 / 1326.0 / 1255.0 / 2.0;
+        return 0;
+    }
+    std::vector<float> sb(prb::H), bb(prb::H);
+    int st = g->half<float>(0, true, sb.data());
+    if (!st) st = g->half<float>(1, true, bb.data());
+    if (st) return st;
+    float s1 = 0, s2 = 0;
+    for (int i = 0; i < prb::H; i++) {
+        s1 += sb[i];
+        s2 += bb[i];
+    }
+    *sum_sb = s1;
+    *sum_bb = s2;
+    *mbh = (double)((s1 + s2) * 1000.0f / 1326.0f / 1255.0f / 2.0f);  // game.rs:175
+    return 0;
+}
+
+int pr_game_timings(void *game, double *host_seconds, double *device_seconds) {
+    Game *g = (Game *)game;
+    if (!g) return 2;
+    *host_seconds = g->t_host;
+    *device_seconds = g->t_gpu;
+    return 0;
+}
+
+int pr_game_get_regrets(void *game, float *upper, float *river) {
+    Game *g = (Game *)game;
+    if (!g) return 2;
+    if (upper) memcpy(upper, g->regrets.data(), g->regrets.size() * sizeof(float));
+    if (river) return pr_get_regrets(g->builder, river);
+    return 0;
+}
+
+size_t pr_game_upper_regret_count(void *game) { return game ? ((Game *)game)->regrets.size() : 0; }
+
+}  // extern "C"

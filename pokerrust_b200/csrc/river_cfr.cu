@@ -52,10 +52,11 @@ constexpr int kPioW = 20;              // bucket row: SD channels 0-8, pad, fold
 constexpr int kFoldCol = 12;
 constexpr int kOutPer = 3;             // output phase: hands per lane, in bucket order
 constexpr int kOutWarps = 12;          // 12 * 32 * 3 >= 1081
+constexpr int kRowW = 12;              // group rows: 9 showdown channels padded to 16-byte loads
 
 // Byte offsets of the shared-memory arrays; computed the same way on host and device.
 struct Layout {
-    unsigned pio, wown, Pg, VC, abar, r, out, Cf, Tf, Tsd, gwarp, scale, stage, stage_key, total;
+    unsigned pio, wown, Pg, VG, VC, abar, r, out, Cf, Tf, Tsd, gwarp, scale, stage, stage_key, total;
 };
 
 __host__ __device__ inline unsigned take(unsigned *o, unsigned bytes) {
@@ -70,7 +71,8 @@ __host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned gr
     L.pio = take(&o, kBuckets * kPioW * vb);
     L.wown = cfr ? take(&o, kBuckets * kPioW * 4) : 0;
     L.Pg = take(&o, (groups + 1) * kNumSD * vb);
-    L.VC = take(&o, card_groups * kNumSD * vb);
+    L.VG = take(&o, groups * kRowW * vb);
+    L.VC = take(&o, card_groups * kRowW * vb);
     L.abar = cfr ? take(&o, kBuckets * kNumLeaves * 4) : 0;
     L.r = take(&o, kRangeStride * vb);
     L.out = take(&o, kRangeStride * vb);
@@ -90,7 +92,8 @@ struct Smem {
     V (*pio)[kPioW];             // opponent reach per bucket and leaf
     float (*wown)[kPioW];        // updater reach * leaf scale per bucket and leaf (CFR)
     V (*Pg)[kNumSD];             // rank-list prefix sum at each tie group's start; [G] = total
-    V (*VC)[kNumSD];             // W - B of each group of each card list
+    V (*VG)[kRowW];              // W - B of each rank-list tie group
+    V (*VC)[kRowW];              // W - B of each group of each card list
     float (*abar)[kNumLeaves];   // per-bucket leaf sums over rivers (CFR)
     V *r;                        // opponent range of the subgame
     V *out;                      // updater's value, summed over rivers
@@ -106,7 +109,8 @@ struct Smem {
         : pio(reinterpret_cast<V(*)[kPioW]>(base + L.pio)),
           wown(reinterpret_cast<float(*)[kPioW]>(base + L.wown)),
           Pg(reinterpret_cast<V(*)[kNumSD]>(base + L.Pg)),
-          VC(reinterpret_cast<V(*)[kNumSD]>(base + L.VC)),
+          VG(reinterpret_cast<V(*)[kRowW]>(base + L.VG)),
+          VC(reinterpret_cast<V(*)[kRowW]>(base + L.VC)),
           abar(reinterpret_cast<float(*)[kNumLeaves]>(base + L.abar)),
           r(reinterpret_cast<V *>(base + L.r)),
           out(reinterpret_cast<V *>(base + L.out)),
@@ -168,12 +172,12 @@ __device__ __forceinline__ int hand_values(const Smem<V> &S, const BoardPack *__
     const int c1 = (m.x >> 19) & 63;
     const int c2 = (m.x >> 25) & 63;
     const int gid = m.y, cg1 = m.z, cg2 = m.w;
+    V g[kRowW], a1[kRowW], a2[kRowW];
+    load_row(S.VG[gid], g, kRowW);
+    load_row(S.VC[cg1], a1, kRowW);
+    load_row(S.VC[cg2], a2, kRowW);
 #pragma unroll
-    for (int c = 0; c < kNumSD; c++) {
-        // (W - B) over the rank list minus (W - B) over the two card lists
-        const V wb = S.Pg[gid][c] + S.Pg[gid + 1][c] - S.Tsd[c];
-        v[c] = wb - S.VC[cg1][c] - S.VC[cg2][c];
-    }
+    for (int c = 0; c < kNumSD; c++) v[c] = g[c] - a1[c] - a2[c];  // (W - B): rank list minus card lists
     const V rh = S.r[h];
     V xf[kNumFold], ca[kNumFold], cb[kNumFold];
     load_row(S.pio[b] + kFoldCol, xf, kNumFold);
@@ -352,8 +356,8 @@ __global__ void __launch_bounds__(NT, 1)
                     for (int c = 0; c < kNumSD; c++) dst[c] += offs[c];
                 }
             }
+            const int G = pk->num_groups;
             if (tid == 0) {
-                const int G = pk->num_groups;
 #pragma unroll
                 for (int c = 0; c < kNumSD; c++) {
                     S.Pg[G][c] = total[c];
@@ -367,6 +371,12 @@ __global__ void __launch_bounds__(NT, 1)
                     for (int c = 0; c < kNumLeaves; c++)
                         S.abar[0][c] += (c < kNumSD ? -235.0f : 235.0f) * total[c];
                 }
+            }
+            // W - B of every tie group: prefix at its start + prefix at its end - total
+            bar_rank_list();
+            for (int gg = g; gg < G; gg += 128) {
+#pragma unroll
+                for (int c = 0; c < kNumSD; c++) S.VG[gg][c] = S.Pg[gg][c] + S.Pg[gg + 1][c] - total[c];
             }
         } else {
             // card lists: 8 lanes per list, 6 slots per lane, 4 lists per warp. Each group of

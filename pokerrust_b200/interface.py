@@ -70,6 +70,27 @@ def lib():
         L.pr_eval_status.argtypes = [vp]
         L.pr_river_smem_bytes.restype = ctypes.c_size_t
         L.pr_river_smem_bytes.argtypes = [vp, i32, i32]
+        L.pr_game_new.restype = vp
+        L.pr_game_new.argtypes = [u64, i32]
+        L.pr_game_free.argtypes = [vp]
+        L.pr_game_num_rivers.restype = i32
+        L.pr_game_num_rivers.argtypes = [vp]
+        L.pr_game_river_roots.restype = i32
+        L.pr_game_river_roots.argtypes = [vp, vp, vp]
+        L.pr_game_builder.restype = vp
+        L.pr_game_builder.argtypes = [vp]
+        L.pr_game_tables.restype = vp
+        L.pr_game_tables.argtypes = [vp]
+        L.pr_game_iterate.restype = i32
+        L.pr_game_iterate.argtypes = [vp, i32]
+        L.pr_game_exploitability.restype = i32
+        L.pr_game_exploitability.argtypes = [vp, i32, vp, vp, vp]
+        L.pr_game_timings.restype = i32
+        L.pr_game_timings.argtypes = [vp, vp, vp]
+        L.pr_game_upper_regret_count.restype = ctypes.c_size_t
+        L.pr_game_upper_regret_count.argtypes = [vp]
+        L.pr_game_get_regrets.restype = i32
+        L.pr_game_get_regrets.argtypes = [vp, vp, vp]
         L.pr_evaluate_br64.restype = i32
         L.pr_evaluate_br64.argtypes = [vp, vp, i32, vp, vp]
         L.pr_tables_build.restype = vp
@@ -83,6 +104,17 @@ def lib():
 def _check(status, what):
     if status != 0:
         raise PokerLibError(f"{what}: {lib().pr_error_string(status).decode()} (status {status})")
+
+
+def card_order():
+    """The 1326 two-card hands as 52-bit masks in colex order (src/evaluator.rs:29-40)."""
+    out = np.zeros(HANDS, np.uint64)
+    n = 0
+    for hi in range(1, 52):
+        for lo in range(hi):
+            out[n] = (1 << lo) | (1 << hi)
+            n += 1
+    return out
 
 
 def _ptr(a):
@@ -176,6 +208,15 @@ class Builder:
 
     def __init__(self):
         self.ptr = initialize_builder()
+        self.owner = True
+
+    @classmethod
+    def wrap(cls, ptr):
+        """A non-owning view of a builder owned elsewhere (e.g. by a Game)."""
+        b = cls.__new__(cls)
+        b.ptr = ptr
+        b.owner = False
+        return b
 
     def add(self, cards, bet):
         return build_river(cards, bet, self.ptr)
@@ -223,8 +264,68 @@ class Builder:
                "pr_evaluate_device")
 
     def close(self):
-        if self.ptr:
+        if self.ptr and self.owner:
             lib().pr_free_builder(self.ptr)
+        self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Game:
+    """The whole fixed-flop game (src/game.rs) driven on the device: upper tree on the host,
+    river subgames on the GPU, tables generated on the GPU."""
+
+    def __init__(self, flop, nthreads=0):
+        self.ptr = lib().pr_game_new(int(flop), int(nthreads))
+        if not self.ptr:
+            raise PokerLibError(f"pr_game_new failed (status {lib().pr_last_error()})")
+
+    @property
+    def num_rivers(self):
+        return lib().pr_game_num_rivers(self.ptr)
+
+    def river_roots(self):
+        n = self.num_rivers
+        boards = np.zeros(n, np.uint64)
+        bets = np.zeros(n, np.float32)
+        _check(lib().pr_game_river_roots(self.ptr, _ptr(boards), _ptr(bets)), "pr_game_river_roots")
+        return boards, bets
+
+    @property
+    def builder(self):
+        return lib().pr_game_builder(self.ptr)
+
+    @property
+    def tables(self):
+        return lib().pr_game_tables(self.ptr)
+
+    def iterate(self, iterations=1):
+        _check(lib().pr_game_iterate(self.ptr, int(iterations)), "pr_game_iterate")
+
+    def exploitability(self, fp64=False):
+        a, b, m = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(lib().pr_game_exploitability(self.ptr, int(bool(fp64)), ctypes.byref(a), ctypes.byref(b),
+                                            ctypes.byref(m)), "pr_game_exploitability")
+        return a.value, b.value, m.value
+
+    def timings(self):
+        h, d = ctypes.c_double(), ctypes.c_double()
+        _check(lib().pr_game_timings(self.ptr, ctypes.byref(h), ctypes.byref(d)), "pr_game_timings")
+        return h.value, d.value
+
+    def regrets(self):
+        up = np.zeros(lib().pr_game_upper_regret_count(self.ptr), np.float32)
+        riv = np.zeros((self.num_rivers, EDGES, BUCKETS), np.float32)
+        _check(lib().pr_game_get_regrets(self.ptr, _ptr(up), _ptr(riv)), "pr_game_get_regrets")
+        return up, riv
+
+    def close(self):
+        if self.ptr:
+            lib().pr_game_free(self.ptr)
             self.ptr = None
 
     def __del__(self):
