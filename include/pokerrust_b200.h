@@ -85,6 +85,15 @@ int pr_evaluate_device(void *builder, void *eval, int updating_player, int calc_
 int pr_upload_batch(void *builder, int first, int count, const float *v);
 int pr_download_batch(void *builder, int first, int count, float *v);
 
+/* Average strategies (an addition: the reference keeps none). After pr_enable_average, every
+ * CFR pass of evaluate_cuda / pr_evaluate also accumulates, per river root, edge and bucket,
+ * the sum over rivers and hands of the updater's reach into the state times the action's
+ * probability. The updater's own range at each root is staged with pr_upload_own (same
+ * contract as upload_c). pr_get_average copies the sums (count * 26 * 256 floats). */
+int pr_enable_average(void *builder);
+void pr_upload_own(void *builder, int index, const float *v);
+int pr_get_average(void *builder, float *out);
+
 /* Number of river subgames in the builder, and the row stride (floats) of pr_* buffers. */
 int pr_builder_count(void *builder);
 int pr_range_stride(void);
@@ -142,6 +151,10 @@ int pr_game_timings(void *game, double *host_seconds, double *device_seconds);
 /* Upper-tree regrets (pr_game_upper_regret_count floats, node order) and river regrets. */
 size_t pr_game_upper_regret_count(void *game);
 int pr_game_get_regrets(void *game, float *upper, float *river);
+/* Average strategies for the whole game: upper-tree sums (per hand, regret layout) and
+ * river sums (per bucket, pr_get_average layout) from the next iteration on. */
+int pr_game_enable_average(void *game);
+int pr_game_get_average(void *game, float *upper, float *river);
 
 #ifdef __cplusplus
 }

@@ -85,6 +85,15 @@ int or_river_batch(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, i
                    const uint64_t *board4, const float *bet, const float *opp_range,
                    float *regrets, int player, int calc_exploit, float *result, int nthreads);
 
+/* A CFR pass that also accumulates average-strategy sums (an addition: the reference keeps
+ * none): own_range[n*1326] is the updating player's range at the river root; for each of
+ * its decision states avg[edge][bucket] += sum over hands of reach into the state times
+ * the action probability. */
+int or_river_batch_avg(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, int n,
+                       const uint64_t *board4, const float *bet, const float *opp_range,
+                       const float *own_range, float *regrets, float *avg, int player,
+                       float *result, int nthreads);
+
 /* Same traversal in double precision, best response only (calc_exploit semantics). */
 int or_river_br_f64(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, int n,
                     const uint64_t *board4, const double *bet, const double *opp_range,

@@ -59,6 +59,8 @@ def load():
         L.or_river_tree.argtypes = [vp] * 8
         L.or_river_batch.restype = i32
         L.or_river_batch.argtypes = [u64, vp, vp, i32, vp, vp, vp, vp, i32, i32, vp, i32]
+        L.or_river_batch_avg.restype = i32
+        L.or_river_batch_avg.argtypes = [u64, vp, vp, i32, vp, vp, vp, vp, vp, vp, i32, vp, i32]
         L.or_river_br_f64.restype = i32
         L.or_river_br_f64.argtypes = [u64, vp, vp, i32, vp, vp, vp, vp, i32, vp, i32]
         L.or_game_new.restype = vp
@@ -139,6 +141,24 @@ def river_batch(flop, eval_tables, abstr, board4, bet, opp_range, regrets, playe
     out = np.zeros((n, HANDS), np.float32)
     err = load().or_river_batch(int(flop), _p(eval_tables), _p(abstr), n, _p(board4), _p(bet), _p(opp),
                                 _p(regrets), int(player), int(bool(calc_exploit)), _p(out), nthreads)
+    if err:
+        raise AssertionError(f"oracle river pass hit a reference assertion (code {err})")
+    return out
+
+
+def river_batch_avg(flop, eval_tables, abstr, board4, bet, opp_range, own_range, regrets, avg, player,
+                    nthreads=0):
+    """A CFR pass that also accumulates average-strategy sums into `avg` (in place)."""
+    board4 = np.ascontiguousarray(board4, np.uint64)
+    bet = np.ascontiguousarray(bet, np.float32)
+    opp = np.ascontiguousarray(opp_range, np.float32)
+    own = np.ascontiguousarray(own_range, np.float32)
+    assert regrets.dtype == np.float32 and regrets.flags.c_contiguous
+    assert avg.dtype == np.float32 and avg.flags.c_contiguous
+    n = board4.size
+    out = np.zeros((n, HANDS), np.float32)
+    err = load().or_river_batch_avg(int(flop), _p(eval_tables), _p(abstr), n, _p(board4), _p(bet), _p(opp),
+                                    _p(own), _p(regrets), _p(avg), int(player), _p(out), nthreads)
     if err:
         raise AssertionError(f"oracle river pass hit a reference assertion (code {err})")
     return out

@@ -129,6 +129,7 @@ struct RiverEval {
     float *updates;        // [26][256] or null
     int upd;
     bool exploit;
+    float *avg = nullptr;  // [26][256] average-strategy sums or null
 
     // strategy.rs:129-150 (get_strategy of AbstractStrategy)
     void strategy(const RNode &s, const Board &b, Vec<T> *out) {
@@ -237,6 +238,16 @@ struct RiverEval {
                 Vec<T> avg(OR_HANDS, br_here ? -std::numeric_limits<T>::infinity() : T(0));
                 Vec<T> strat[3];
                 strategy(s, bd, strat);
+                if (this->avg && s.actor == upd && !exploit) {
+                    // average-strategy sums: the updater's reach into the node times the
+                    // action probability, summed into the hand's bucket (not in the reference)
+                    const Vec<T> &mine = upd == Small ? sb : bbr;
+                    for (int i = 0; i < OR_HANDS; i++) {
+                        int a = bd.abstr[i];
+                        for (int k = 0; k < s.nchild; k++)
+                            this->avg[s.edge[k] * OR_BUCKETS + a] += float(mine[i] * strat[k][i]);
+                    }
+                }
                 Vec<T> results[3];
                 for (int k = 0; k < s.nchild; k++) {
                     const Vec<T> &prob = strat[k];
@@ -284,14 +295,14 @@ struct RiverEval {
 template <typename T>
 int river_one(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, uint64_t board4,
               float bet, const T *opp_in, float *regrets, const float *regrets_ro, int player,
-              bool exploit, T *out) {
+              bool exploit, T *out, const T *own_in = nullptr, float *avg = nullptr) {
     static thread_local uint64_t card_order[OR_HANDS];
     static thread_local bool init = false;
     if (!init) { or_card_order(card_order); init = true; }
     const RTree &tr = tree();
     std::vector<float> updates(OR_RIVER_EDGES * OR_BUCKETS, 0.0f);
     RiverEval<T> ev{card_order, tr, bet, regrets ? regrets : regrets_ro,
-                    (regrets && !exploit) ? updates.data() : nullptr, player, exploit};
+                    (regrets && !exploit) ? updates.data() : nullptr, player, exploit, avg};
     Vec<T> total(OR_HANDS, T(0));
     Vec<T> own(OR_HANDS, T(1));
     int count = 0, err = 0;
@@ -313,7 +324,7 @@ int river_one(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, uint64
         for (int i = 0; i < OR_HANDS; i++) {
             bool blocked = (card_order[i] & cards) != 0;
             opp[i] = blocked ? T(0) : opp_in[i];
-            mine[i] = blocked ? T(0) : own[i];
+            mine[i] = blocked ? T(0) : (own_in ? own_in[i] : own[i]);
         }
         // node 1 is the DealRiver child of the River root
         Vec<T> res = player == Small ? ev.eval(1, mine, opp, bd, &err) : ev.eval(1, opp, mine, bd, &err);
@@ -383,6 +394,21 @@ extern "C" int or_river_batch(uint64_t flop, const uint16_t *eval, const uint16_
         int e = river_one<float>(flop, eval, abstr, board4[i], bet[i], opp_range + (size_t)i * OR_HANDS,
                                  regrets + (size_t)i * OR_RIVER_EDGES * OR_BUCKETS, nullptr, player,
                                  calc_exploit != 0, result + (size_t)i * OR_HANDS);
+        if (e) err = e;
+    });
+    return err;
+}
+
+extern "C" int or_river_batch_avg(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, int n,
+                                  const uint64_t *board4, const float *bet, const float *opp_range,
+                                  const float *own_range, float *regrets, float *avg, int player,
+                                  float *result, int nthreads) {
+    std::atomic_int err(0);
+    or_parallel_for(n, nthreads, [&](int i) {
+        int e = river_one<float>(flop, eval, abstr, board4[i], bet[i], opp_range + (size_t)i * OR_HANDS,
+                                 regrets + (size_t)i * OR_RIVER_EDGES * OR_BUCKETS, nullptr, player, false,
+                                 result + (size_t)i * OR_HANDS, own_range + (size_t)i * OR_HANDS,
+                                 avg + (size_t)i * OR_RIVER_EDGES * OR_BUCKETS);
         if (e) err = e;
     });
     return err;

@@ -121,6 +121,12 @@ struct Builder {
     float *d_regrets = nullptr;
     float *d_ranges = nullptr;
     float *d_results = nullptr;
+    // average strategies (pr_enable_average): own-range staging and the sums
+    bool avg_on = false;
+    float *comm_own = nullptr;      // pinned, capacity rows
+    float *d_own = nullptr;
+    float *d_avg = nullptr;
+    int avg_capacity = 0;
     double *d_ranges64 = nullptr;   // double-precision best response (lazily allocated)
     double *d_results64 = nullptr;
     int cap64 = 0;
@@ -166,8 +172,46 @@ bool grow_staging(Builder *b, int need) {
         cudaFreeHost(b->comm);
     }
     b->comm = fresh;
+    if (b->avg_on) {
+        float *own = nullptr;
+        e = cudaHostAlloc((void **)&own, (size_t)cap * kRangeStride * sizeof(float), cudaHostAllocPortable);
+        if (e != cudaSuccess) {
+            fail(kErrAlloc, "pinned staging allocation", e);
+            return false;
+        }
+        memset(own, 0, (size_t)cap * kRangeStride * sizeof(float));
+        if (b->comm_own) {
+            memcpy(own, b->comm_own, (size_t)b->capacity * kRangeStride * sizeof(float));
+            cudaFreeHost(b->comm_own);
+        }
+        b->comm_own = own;
+    }
     b->capacity = cap;
     return true;
+}
+
+// Device arrays of the average-strategy sums, grown with the subgames (new rows zero).
+int sync_average(Builder *b) {
+    if (b->avg_capacity >= b->dev_capacity) return kOk;
+    cudaError_t e;
+    float *own = nullptr, *avg = nullptr;
+    const size_t rows = (size_t)b->dev_capacity * kRangeStride * sizeof(float);
+    const size_t sums = (size_t)b->dev_capacity * kEdges * kBuckets * sizeof(float);
+    if ((e = cudaMalloc(&own, rows)) != cudaSuccess || (e = cudaMalloc(&avg, sums)) != cudaSuccess) {
+        cudaFree(own);
+        return fail(kErrAlloc, "average-strategy allocation", e);
+    }
+    cudaMemsetAsync(avg, 0, sums, b->stream);
+    if (b->d_avg)
+        cudaMemcpyAsync(avg, b->d_avg, (size_t)b->avg_capacity * kEdges * kBuckets * sizeof(float),
+                        cudaMemcpyDeviceToDevice, b->stream);
+    e = cudaStreamSynchronize(b->stream);
+    cudaFree(b->d_own);
+    cudaFree(b->d_avg);
+    b->d_own = own;
+    b->d_avg = avg;
+    b->avg_capacity = b->dev_capacity;
+    return e == cudaSuccess ? kOk : fail(kErrCuda, "average-strategy allocation", e);
 }
 
 // Brings the device arrays up to the host's subgame count; new regrets start at zero
@@ -240,6 +284,13 @@ int evaluate_impl(Builder *b, EvalTables *t, int player, int exploit, const floa
     if (n == 0) return kOk;
     cudaStream_t s = stream ? stream : b->stream;
     cudaError_t e;
+    const bool avg = staged && b->avg_on && !exploit;
+    if (avg) {
+        if ((st = sync_average(b))) return st;
+        e = cudaMemcpyAsync(b->d_own, b->comm_own, (size_t)n * kRangeStride * sizeof(float),
+                            cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return fail(kErrCuda, "own range upload", e);
+    }
     if (staged) {
         e = cudaMemcpyAsync(b->d_ranges, b->comm, (size_t)n * kRangeStride * sizeof(float),
                             cudaMemcpyHostToDevice, s);
@@ -248,7 +299,8 @@ int evaluate_impl(Builder *b, EvalTables *t, int player, int exploit, const floa
         d_out = b->d_results;
     }
     e = launch_river(exploit ? kModeBR : kModeCFR, b->d_desc, n, d_in, d_out, b->d_regrets, t->packs,
-                     t->flop, player, t->max_groups, t->max_card_groups, s);
+                     t->flop, player, t->max_groups, t->max_card_groups, avg ? b->d_own : nullptr,
+                     avg ? b->d_avg : nullptr, s);
     if (e != cudaSuccess) return fail(kErrCuda, "river kernel launch", e);
     if (staged) {
         e = cudaMemcpyAsync(b->comm, b->d_results, (size_t)n * kRangeStride * sizeof(float),
@@ -495,6 +547,42 @@ int pr_download_batch(void *builder, int first, int count, float *v) {
     return kOk;
 }
 
+int pr_enable_average(void *builder) {
+    Builder *b = (Builder *)builder;
+    if (!b) return fail(kErrArg, "pr_enable_average: null builder");
+    if (b->avg_on) return kOk;
+    b->avg_on = true;
+    const int cap = b->capacity;
+    b->capacity = 0;  // re-allocate both staging areas at the current capacity
+    float *old = b->comm;
+    b->comm = nullptr;
+    if (!grow_staging(b, cap)) return kErrAlloc;
+    memcpy(b->comm, old, (size_t)cap * kRangeStride * sizeof(float));
+    cudaFreeHost(old);
+    return kOk;
+}
+
+void pr_upload_own(void *builder, int index, const float *v) {
+    Builder *b = (Builder *)builder;
+    if (!b || !b->avg_on || index < 0 || index >= (int)b->desc.size() || !v) {
+        fail(kErrArg, "pr_upload_own: bad builder or index, or averages not enabled");
+        return;
+    }
+    memcpy(b->comm_own + (size_t)index * kRangeStride, v, kHands * sizeof(float));
+}
+
+int pr_get_average(void *builder, float *out) {
+    Builder *b = (Builder *)builder;
+    if (!b || !out || !b->avg_on) return fail(kErrArg, "pr_get_average: averages not enabled");
+    int st = sync_device(b);
+    if (st) return st;
+    if ((st = sync_average(b))) return st;
+    cudaError_t e = cudaMemcpyAsync(out, b->d_avg, (size_t)b->dev_count * kEdges * kBuckets * sizeof(float),
+                                    cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? kOk : fail(kErrCuda, "average download", e);
+}
+
 int pr_builder_count(void *builder) { return builder ? (int)((Builder *)builder)->desc.size() : 0; }
 
 int pr_range_stride(void) { return kRangeStride; }
@@ -533,6 +621,9 @@ void pr_free_builder(void *builder) {
     cudaFree(b->d_regrets);
     cudaFree(b->d_ranges64);
     cudaFree(b->d_results64);
+    cudaFree(b->d_own);
+    cudaFree(b->d_avg);
+    if (b->comm_own) cudaFreeHost(b->comm_own);
     if (b->comm) cudaFreeHost(b->comm);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;

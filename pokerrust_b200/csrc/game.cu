@@ -129,6 +129,8 @@ struct Game {
     std::vector<UNode> nodes;
     std::vector<int32_t> kids;
     std::vector<float> regrets;
+    std::vector<float> avg_upper;                 // average-strategy sums, same layout as regrets
+    bool avg_on = false;
     std::vector<std::array<int, 4>> perms;
     std::vector<std::vector<int32_t>> perm_maps;  // hand index -> permuted hand index
     std::vector<uint64_t> card_order;
@@ -347,7 +349,7 @@ struct Game {
     }
 
     template <typename T>
-    void river(const UNode &s, const T *opp, int pass, T *out);
+    void river(const UNode &s, const T *opp, const T *own, int pass, T *out);
 
     template <typename T>
     void eval(int si, const T *sb, const T *bb, int upd, bool br, int pass, T *out, int depth,
@@ -379,6 +381,13 @@ struct Game {
                     } else {
                         for (int i = 0; i < H; i++) avg[i] += uk[i];
                     }
+                }
+                if (pass == kDownload && mine && !br && avg_on) {
+                    // average-strategy sums: own reach into the node times the action probability
+                    const T *own = s.actor == 0 ? sb : bb;
+                    float *a = avg_upper.data() + s.regret;
+                    for (int k = 0; k < s.nchild; k++)
+                        for (int i = 0; i < H; i++) a[(size_t)k * H + i] += float(own[i] * probs[(size_t)k * H + i]);
                 }
                 if (pass == kDownload && mine && !br) {
                     // RegularStrategy::update_add (strategy.rs:57-66)
@@ -462,7 +471,7 @@ struct Game {
                 return;
             }
             case kRiverRoot:
-                river(s, opp, pass, out);
+                river(s, opp, upd == 0 ? sb : bb, pass, out);
                 return;
         }
     }
@@ -493,14 +502,18 @@ struct Game {
 };
 
 template <>
-void Game::river<float>(const UNode &s, const float *opp, int pass, float *out) {
+void Game::river<float>(const UNode &s, const float *opp, const float *own, int pass, float *out) {
     // state.rs:378-389: stage the opponent range, or read the device's values back
-    if (pass == kUpload) upload_c(builder, s.river, opp);
-    else download_c(builder, s.river, out);
+    if (pass == kUpload) {
+        upload_c(builder, s.river, opp);
+        if (avg_on) pr_upload_own(builder, s.river, own);
+    } else {
+        download_c(builder, s.river, out);
+    }
 }
 
 template <>
-void Game::river<double>(const UNode &s, const double *opp, int pass, double *out) {
+void Game::river<double>(const UNode &s, const double *opp, const double *, int pass, double *out) {
     if (pass == kUpload) memcpy(ranges64.data() + (size_t)s.river * H, opp, sizeof(double) * H);
     else memcpy(out, results64.data() + (size_t)s.river * H, sizeof(double) * H);
 }
@@ -604,5 +617,24 @@ int pr_game_get_regrets(void *game, float *upper, float *river) {
 }
 
 size_t pr_game_upper_regret_count(void *game) { return game ? ((Game *)game)->regrets.size() : 0; }
+
+int pr_game_enable_average(void *game) {
+    Game *g = (Game *)game;
+    if (!g) return 2;
+    if (g->avg_on) return 0;
+    const int st = pr_enable_average(g->builder);
+    if (st) return st;
+    g->avg_upper.assign(g->regrets.size(), 0.0f);
+    g->avg_on = true;
+    return 0;
+}
+
+int pr_game_get_average(void *game, float *upper, float *river) {
+    Game *g = (Game *)game;
+    if (!g || !g->avg_on) return 2;
+    if (upper) memcpy(upper, g->avg_upper.data(), g->avg_upper.size() * sizeof(float));
+    if (river) return pr_get_average(g->builder, river);
+    return 0;
+}
 
 }  // extern "C"

@@ -56,7 +56,7 @@ constexpr int kRowW = 12;              // group rows: 9 showdown channels padded
 
 // Byte offsets of the shared-memory arrays; computed the same way on host and device.
 struct Layout {
-    unsigned pio, wown, Pg, VG, VC, abar, r, out, Cf, Tf, Tsd, gwarp, scale, stage, stage_key, total;
+    unsigned pio, wown, Pg, VG, VC, abar, r, own, out, Cf, Tf, Tsd, gwarp, scale, stage, stage_key, total;
 };
 
 __host__ __device__ inline unsigned take(unsigned *o, unsigned bytes) {
@@ -65,7 +65,10 @@ __host__ __device__ inline unsigned take(unsigned *o, unsigned bytes) {
     return at;
 }
 
-__host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned groups, unsigned card_groups) {
+// acc: per-bucket sums carried over the rivers (the 17 leaves, plus the updater's own range
+// mass when average strategies are accumulated).
+__host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned groups, unsigned card_groups,
+                                              unsigned acc = kNumLeaves) {
     Layout L;
     unsigned o = 0;
     L.pio = take(&o, kBuckets * kPioW * vb);
@@ -73,36 +76,38 @@ __host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned gr
     L.Pg = take(&o, (groups + 1) * kNumSD * vb);
     L.VG = take(&o, groups * kRowW * vb);
     L.VC = take(&o, card_groups * kRowW * vb);
-    L.abar = cfr ? take(&o, kBuckets * kNumLeaves * 4) : 0;
+    L.abar = cfr ? take(&o, kBuckets * acc * 4) : 0;
     L.r = take(&o, kRangeStride * vb);
+    L.own = acc > kNumLeaves ? take(&o, kRangeStride * 4) : 0;
     L.out = take(&o, kRangeStride * vb);
     L.Cf = take(&o, 52 * kNumFold * vb);
     L.Tf = take(&o, kNumFold * vb);
     L.Tsd = take(&o, kNumSD * vb);
     L.gwarp = take(&o, 4 * kNumLeaves * vb);
     L.scale = take(&o, kNumLeaves * 4);
-    L.stage = cfr ? take(&o, kOutWarps * 2 * kNumLeaves * 4) : 0;
+    L.stage = cfr ? take(&o, kOutWarps * 2 * acc * 4) : 0;
     L.stage_key = cfr ? take(&o, kOutWarps * 2 * 4) : 0;
     L.total = o;
     return L;
 }
 
-template <typename V>
+template <typename V, int ACC = kNumLeaves>
 struct Smem {
     V (*pio)[kPioW];             // opponent reach per bucket and leaf
     float (*wown)[kPioW];        // updater reach * leaf scale per bucket and leaf (CFR)
     V (*Pg)[kNumSD];             // rank-list prefix sum at each tie group's start; [G] = total
     V (*VG)[kRowW];              // W - B of each rank-list tie group
     V (*VC)[kRowW];              // W - B of each group of each card list
-    float (*abar)[kNumLeaves];   // per-bucket leaf sums over rivers (CFR)
+    float (*abar)[ACC];          // per-bucket leaf sums (and own-range mass) over rivers (CFR)
     V *r;                        // opponent range of the subgame
+    float *own;                  // updater's own range (average strategies only)
     V *out;                      // updater's value, summed over rivers
     V (*Cf)[kNumFold];           // card sums, fold channels
     V *Tf;                       // totals, fold channels
     V *Tsd;                      // totals, showdown channels
     V (*gwarp)[kNumLeaves];      // rank-list warp totals
     float *scale;                // leaf scales
-    float (*stage)[2][kNumLeaves];  // bucket runs touching an output warp's ends (CFR)
+    float (*stage)[2][ACC];      // bucket runs touching an output warp's ends (CFR)
     int (*stage_key)[2];
 
     __device__ Smem(unsigned char *base, const Layout &L)
@@ -111,15 +116,16 @@ struct Smem {
           Pg(reinterpret_cast<V(*)[kNumSD]>(base + L.Pg)),
           VG(reinterpret_cast<V(*)[kRowW]>(base + L.VG)),
           VC(reinterpret_cast<V(*)[kRowW]>(base + L.VC)),
-          abar(reinterpret_cast<float(*)[kNumLeaves]>(base + L.abar)),
+          abar(reinterpret_cast<float(*)[ACC]>(base + L.abar)),
           r(reinterpret_cast<V *>(base + L.r)),
+          own(reinterpret_cast<float *>(base + L.own)),
           out(reinterpret_cast<V *>(base + L.out)),
           Cf(reinterpret_cast<V(*)[kNumFold]>(base + L.Cf)),
           Tf(reinterpret_cast<V *>(base + L.Tf)),
           Tsd(reinterpret_cast<V *>(base + L.Tsd)),
           gwarp(reinterpret_cast<V(*)[kNumLeaves]>(base + L.gwarp)),
           scale(reinterpret_cast<float *>(base + L.scale)),
-          stage(reinterpret_cast<float(*)[2][kNumLeaves]>(base + L.stage)),
+          stage(reinterpret_cast<float(*)[2][ACC]>(base + L.stage)),
           stage_key(reinterpret_cast<int(*)[2]>(base + L.stage_key)) {}
 };
 
@@ -148,8 +154,8 @@ __device__ __forceinline__ void load_row(const double *p, double *o, int n) {
 }
 
 // x for all 17 channels of one list element (one bucket-row load).
-template <typename V>
-__device__ __forceinline__ void elem_x(const Smem<V> &S, uint32_t e, V x[kNumLeaves]) {
+template <typename V, int ACC>
+__device__ __forceinline__ void elem_x(const Smem<V, ACC> &S, uint32_t e, V x[kNumLeaves]) {
     const int h = e & 2047;
     const int b = (e >> 11) & 255;
     const V rh = h != (int)kNoHand ? S.r[h] : V(0);
@@ -163,8 +169,8 @@ __device__ __forceinline__ void elem_x(const Smem<V> &S, uint32_t e, V x[kNumLea
 
 // Leaf values (before the leaf's bet/sign scale) of live hand l for all 17 channels:
 // showdowns from the group values of the scans, folds from totals and card sums.
-template <typename V>
-__device__ __forceinline__ int hand_values(const Smem<V> &S, const BoardPack *__restrict__ pk, int l,
+template <typename V, int ACC>
+__device__ __forceinline__ int hand_values(const Smem<V, ACC> &S, const BoardPack *__restrict__ pk, int l,
                                            V v[kNumLeaves]) {
     const uint4 m = __ldg(&pk->meta[l]);
     const int h = m.x & 2047;
@@ -190,7 +196,8 @@ __device__ __forceinline__ int hand_values(const Smem<V> &S, const BoardPack *__
 
 // Adds the staged warp-boundary bucket runs of the last output phase into abar, in a fixed
 // order (one thread per leaf channel), so that bucket sums do not depend on scheduling.
-__device__ __forceinline__ void resolve_stage(Smem<float> &S, int c) {
+template <int ACC>
+__device__ __forceinline__ void resolve_stage(Smem<float, ACC> &S, int c) {
 #pragma unroll 1
     for (int w = 0; w < kOutWarps; w++) {
 #pragma unroll
@@ -206,15 +213,18 @@ __device__ __forceinline__ V vmax(V a, V b) {
     return a > b ? a : b;
 }
 
-template <int MODE, typename V>
+template <int MODE, typename V, bool AVG>
 __global__ void __launch_bounds__(NT, 1)
     river_kernel(const SubgameDesc *__restrict__ desc, const V *__restrict__ ranges, V *__restrict__ results,
                  float *__restrict__ regrets, const BoardPack *__restrict__ packs, unsigned long long flop,
-                 int updater, int max_groups, int max_card_groups) {
+                 int updater, int max_groups, int max_card_groups, const float *__restrict__ own_ranges,
+                 float *__restrict__ avg_sums) {
     static_assert(MODE == kModeBR || sizeof(V) == 4, "CFR runs in single precision");
+    static_assert(!AVG || MODE == kModeCFR, "average strategies accumulate in CFR passes");
+    constexpr int ACC = kNumLeaves + (AVG ? 1 : 0);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Layout L = make_layout(MODE == kModeCFR, sizeof(V), max_groups, max_card_groups);
-    Smem<V> S(smem_raw, L);
+    const Layout L = make_layout(MODE == kModeCFR, sizeof(V), max_groups, max_card_groups, ACC);
+    Smem<V, ACC> S(smem_raw, L);
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -227,6 +237,7 @@ __global__ void __launch_bounds__(NT, 1)
     for (int i = tid; i < kRangeStride; i += NT) {
         S.r[i] = ranges[(size_t)sg * kRangeStride + i];
         S.out[i] = V(0);
+        if constexpr (AVG) S.own[i] = own_ranges[(size_t)sg * kRangeStride + i];
     }
     if (tid < kNumLeaves) S.scale[tid] = leaf_scale(kLeaf(tid), updater, bet);
     if (tid < kBuckets) {
@@ -274,6 +285,7 @@ __global__ void __launch_bounds__(NT, 1)
                 S.abar[b][Lf] = 0.0f;
             }
         }
+        if constexpr (AVG) S.abar[b][kNumLeaves] = 0.0f;
         if constexpr (MODE == kModeCFR) {
 #pragma unroll
             for (int i = kNumSD; i < kFoldCol; i++) S.wown[b][i] = 0.0f;
@@ -290,7 +302,7 @@ __global__ void __launch_bounds__(NT, 1)
         const BoardPack *__restrict__ pk = packs + slot;
         __syncthreads();  // previous river's readers are done with Pg, VC, Cf, Tf
         if constexpr (MODE == kModeCFR) {
-            if (warp == NT / 32 - 1 && lane < kNumLeaves && rc_done > 0) resolve_stage(S, lane);
+            if (warp == NT / 32 - 1 && lane < ACC && rc_done > 0) resolve_stage(S, lane);
         }
         rc_done++;
 
@@ -469,11 +481,11 @@ __global__ void __launch_bounds__(NT, 1)
         // ---- per live hand, in bucket order: root value and per-bucket leaf sums ----
         if (warp < kOutWarps) {
             const unsigned FULL = 0xffffffffu;
-            float F[kNumLeaves], Lr[kNumLeaves];  // first run / last run of this lane's hands
+            float F[ACC], Lr[ACC];  // first run / last run of this lane's hands
             int nr = 0, kf = -1, kl = -1;
             if constexpr (MODE == kModeCFR) {
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) F[c] = Lr[c] = 0.0f;
+                for (int c = 0; c < ACC; c++) F[c] = Lr[c] = 0.0f;
             }
 #pragma unroll
             for (int i = 0; i < kOutPer; i++) {
@@ -481,8 +493,9 @@ __global__ void __launch_bounds__(NT, 1)
                 const uint32_t be = j < kLive ? __ldg(&pk->border[j]) : (kNoBucket << 16);
                 const int key = be >> 16;
                 if (key == (int)kNoBucket) continue;
-                V v[kNumLeaves];
+                V v[ACC];
                 const int h = hand_values(S, pk, be & 0xffff, v);
+                if constexpr (AVG) v[kNumLeaves] = S.own[h];
                 if constexpr (MODE == kModeCFR) {
                     float w[kPioW];
                     load_row(S.wown[key], w, kPioW);
@@ -497,22 +510,22 @@ __global__ void __launch_bounds__(NT, 1)
                         kf = kl = key;
                         nr = 1;
 #pragma unroll
-                        for (int c = 0; c < kNumLeaves; c++) F[c] = v[c];
+                        for (int c = 0; c < ACC; c++) F[c] = v[c];
                     } else if (key == kl) {
                         if (nr == 1) {
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) F[c] += v[c];
+                            for (int c = 0; c < ACC; c++) F[c] += v[c];
                         } else {
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) Lr[c] += v[c];
+                            for (int c = 0; c < ACC; c++) Lr[c] += v[c];
                         }
                     } else {
                         if (nr >= 2) {
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) S.abar[kl][c] += Lr[c];
+                            for (int c = 0; c < ACC; c++) S.abar[kl][c] += Lr[c];
                         }
 #pragma unroll
-                        for (int c = 0; c < kNumLeaves; c++) Lr[c] = v[c];
+                        for (int c = 0; c < ACC; c++) Lr[c] = v[c];
                         kl = key;
                         nr = nr + 1;
                     }
@@ -550,20 +563,20 @@ __global__ void __launch_bounds__(NT, 1)
                 const bool link = single && join;
                 const unsigned starts = __ballot_sync(FULL, !link);
                 const int seg_start = 31 - __clz(starts & (FULL >> (31 - lane)));
-                float R[kNumLeaves];
+                float R[ACC];
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) R[c] = single ? F[c] : Lr[c];
+                for (int c = 0; c < ACC; c++) R[c] = single ? F[c] : Lr[c];
 #pragma unroll
                 for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
-                    for (int c = 0; c < kNumLeaves; c++) {
+                    for (int c = 0; c < ACC; c++) {
                         const float t = __shfl_up_sync(FULL, R[c], off);
                         if (lane - off >= seg_start) R[c] += t;
                     }
                 }
-                float Cin[kNumLeaves];
+                float Cin[ACC];
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) {
+                for (int c = 0; c < ACC; c++) {
                     const float t = __shfl_up_sync(FULL, R[c], 1);
                     Cin[c] = join ? t : 0.0f;
                 }
@@ -579,33 +592,33 @@ __global__ void __launch_bounds__(NT, 1)
                         if (lane == hend) {
                             S.stage_key[warp][0] = kfirst;
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) S.stage[warp][0][c] = Cin[c] + F[c];
+                            for (int c = 0; c < ACC; c++) S.stage[warp][0][c] = Cin[c] + F[c];
                         } else {
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) S.abar[kfirst][c] += Cin[c] + F[c];
+                            for (int c = 0; c < ACC; c++) S.abar[kfirst][c] += Cin[c] + F[c];
                         }
                         // last run (R == Lr here) ends here unless the next lane joins it
                         if (lane == 31) {
                             S.stage_key[warp][1] = klast;
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) S.stage[warp][1][c] = R[c];
+                            for (int c = 0; c < ACC; c++) S.stage[warp][1][c] = R[c];
                         } else if (!next_join) {
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) S.abar[klast][c] += R[c];
+                            for (int c = 0; c < ACC; c++) S.abar[klast][c] += R[c];
                         }
                     } else if (!next_join) {
                         // the lane's only run ends here, total R
                         if (lane == hend) {
                             S.stage_key[warp][0] = klast;
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) S.stage[warp][0][c] = R[c];
+                            for (int c = 0; c < ACC; c++) S.stage[warp][0][c] = R[c];
                         } else if (lane == 31) {
                             S.stage_key[warp][1] = klast;
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) S.stage[warp][1][c] = R[c];
+                            for (int c = 0; c < ACC; c++) S.stage[warp][1][c] = R[c];
                         } else {
 #pragma unroll
-                            for (int c = 0; c < kNumLeaves; c++) S.abar[klast][c] += R[c];
+                            for (int c = 0; c < ACC; c++) S.abar[klast][c] += R[c];
                         }
                     }
                 }
@@ -614,7 +627,7 @@ __global__ void __launch_bounds__(NT, 1)
     }
     __syncthreads();
     if constexpr (MODE == kModeCFR) {
-        if (warp == NT / 32 - 1 && lane < kNumLeaves) resolve_stage(S, lane);
+        if (warp == NT / 32 - 1 && lane < ACC) resolve_stage(S, lane);
         __syncthreads();
     }
 
@@ -632,6 +645,31 @@ __global__ void __launch_bounds__(NT, 1)
             float reg[kEdges];
 #pragma unroll
             for (int e = 0; e < kEdges; e++) reg[e] = greg[e * kBuckets + b];
+            if constexpr (AVG) {
+                // average-strategy sums: own range mass of the bucket over the rivers, times the
+                // updater's reach into the state, times the action probability (current regrets)
+                float reach[kStates];
+                reach[1] = S.abar[b][kNumLeaves];
+                float *gavg = avg_sums + (size_t)sg * kEdges * kBuckets;
+#pragma unroll
+                for (int di = 0; di < kNumDecision; di++) {
+                    const int s = kDecision(di);
+                    const int nk = kNChild(s);
+                    float sum = 0.0f;
+#pragma unroll
+                    for (int k = 0; k < 3; k++)
+                        if (k < nk) sum += reg[kEdge(s, k)];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        if (k < nk) {
+                            const float sig = sum <= 1e-4f ? 1.0f / (float)nk : reg[kEdge(s, k)] / sum;
+                            const int c = kChild(s, k);
+                            reach[c] = kActor(s) == updater ? reach[s] * sig : reach[s];
+                            if (kActor(s) == updater) gavg[kEdge(s, k) * kBuckets + b] += reach[s] * sig;
+                        }
+                    }
+                }
+            }
             float A[kStates];
 #pragma unroll
             for (int Lf = 0; Lf < kNumLeaves; Lf++) A[kLeaf(Lf)] = S.abar[b][Lf] * S.scale[Lf];
@@ -673,41 +711,48 @@ __global__ void __launch_bounds__(NT, 1)
     }
 }
 
-template <int MODE, typename V>
+template <int MODE, typename V, bool AVG>
 cudaError_t launch_one(const SubgameDesc *desc, int n, const V *ranges, V *results, float *regrets,
                        const BoardPack *packs, unsigned long long flop, int updater, int max_groups,
-                       int max_card_groups, cudaStream_t stream) {
-    const Layout L = make_layout(MODE == kModeCFR, sizeof(V), max_groups, max_card_groups);
+                       int max_card_groups, const float *own, float *avg, cudaStream_t stream) {
+    const Layout L = make_layout(MODE == kModeCFR, sizeof(V), max_groups, max_card_groups,
+                                 kNumLeaves + (AVG ? 1 : 0));
     if (L.total > 227u * 1024u) return cudaErrorInvalidConfiguration;
-    cudaError_t e = cudaFuncSetAttribute(river_kernel<MODE, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)L.total);
+    cudaError_t e = cudaFuncSetAttribute(river_kernel<MODE, V, AVG>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
     if (e != cudaSuccess) return e;
-    river_kernel<MODE, V><<<n, NT, L.total, stream>>>(desc, ranges, results, regrets, packs, flop, updater,
-                                                      max_groups, max_card_groups);
+    river_kernel<MODE, V, AVG><<<n, NT, L.total, stream>>>(desc, ranges, results, regrets, packs, flop,
+                                                           updater, max_groups, max_card_groups, own, avg);
     return cudaGetLastError();
 }
 
 }  // namespace
 
 size_t river_smem_bytes(int mode, int fp64, int max_groups, int max_card_groups) {
-    return make_layout(mode == kModeCFR, fp64 ? 8 : 4, max_groups, max_card_groups).total;
+    return make_layout(mode == kModeCFR, fp64 ? 8 : 4, max_groups, max_card_groups,
+                       mode == kModeCFR ? kNumLeaves + 1 : kNumLeaves)
+        .total;
 }
 
 cudaError_t launch_river(int mode, const SubgameDesc *desc, int n, const float *ranges, float *results,
                          float *regrets, const BoardPack *packs, unsigned long long flop, int updater,
-                         int max_groups, int max_card_groups, cudaStream_t stream) {
+                         int max_groups, int max_card_groups, const float *own_ranges, float *avg_sums,
+                         cudaStream_t stream) {
+    if (mode == kModeCFR && own_ranges && avg_sums)
+        return launch_one<kModeCFR, float, true>(desc, n, ranges, results, regrets, packs, flop, updater,
+                                                 max_groups, max_card_groups, own_ranges, avg_sums, stream);
     if (mode == kModeCFR)
-        return launch_one<kModeCFR, float>(desc, n, ranges, results, regrets, packs, flop, updater, max_groups,
-                                           max_card_groups, stream);
-    return launch_one<kModeBR, float>(desc, n, ranges, results, regrets, packs, flop, updater, max_groups,
-                                      max_card_groups, stream);
+        return launch_one<kModeCFR, float, false>(desc, n, ranges, results, regrets, packs, flop, updater,
+                                                  max_groups, max_card_groups, nullptr, nullptr, stream);
+    return launch_one<kModeBR, float, false>(desc, n, ranges, results, regrets, packs, flop, updater,
+                                             max_groups, max_card_groups, nullptr, nullptr, stream);
 }
 
 cudaError_t launch_river_br64(const SubgameDesc *desc, int n, const double *ranges, double *results,
                               float *regrets, const BoardPack *packs, unsigned long long flop, int updater,
                               int max_groups, int max_card_groups, cudaStream_t stream) {
-    return launch_one<kModeBR, double>(desc, n, ranges, results, regrets, packs, flop, updater, max_groups,
-                                       max_card_groups, stream);
+    return launch_one<kModeBR, double, false>(desc, n, ranges, results, regrets, packs, flop, updater,
+                                              max_groups, max_card_groups, nullptr, nullptr, stream);
 }
 
 }  // namespace prb

@@ -89,8 +89,17 @@ def lib():
         L.pr_game_timings.argtypes = [vp, vp, vp]
         L.pr_game_upper_regret_count.restype = ctypes.c_size_t
         L.pr_game_upper_regret_count.argtypes = [vp]
+        L.pr_game_enable_average.restype = i32
+        L.pr_game_enable_average.argtypes = [vp]
+        L.pr_game_get_average.restype = i32
+        L.pr_game_get_average.argtypes = [vp, vp, vp]
         L.pr_game_get_regrets.restype = i32
         L.pr_game_get_regrets.argtypes = [vp, vp, vp]
+        L.pr_enable_average.restype = i32
+        L.pr_enable_average.argtypes = [vp]
+        L.pr_upload_own.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_float)]
+        L.pr_get_average.restype = i32
+        L.pr_get_average.argtypes = [vp, vp]
         L.pr_evaluate_br64.restype = i32
         L.pr_evaluate_br64.argtypes = [vp, vp, i32, vp, vp]
         L.pr_tables_build.restype = vp
@@ -240,6 +249,21 @@ class Builder:
         _check(lib().pr_get_regrets(self.ptr, _ptr(out)), "pr_get_regrets")
         return out
 
+    def enable_average(self):
+        _check(lib().pr_enable_average(self.ptr), "pr_enable_average")
+
+    def upload_own_all(self, ranges):
+        ranges = np.ascontiguousarray(ranges, dtype=np.float32)
+        assert ranges.shape == (self.count, HANDS)
+        fp = ctypes.POINTER(ctypes.c_float)
+        for i in range(self.count):
+            lib().pr_upload_own(self.ptr, i, ranges[i].ctypes.data_as(fp))
+
+    def average_sums(self):
+        out = np.zeros((self.count, EDGES, BUCKETS), dtype=np.float32)
+        _check(lib().pr_get_average(self.ptr, _ptr(out)), "pr_get_average")
+        return out
+
     def set_regrets(self, regrets):
         regrets = np.ascontiguousarray(regrets, dtype=np.float32)
         assert regrets.shape == (self.count, EDGES, BUCKETS)
@@ -321,6 +345,15 @@ class Game:
         up = np.zeros(lib().pr_game_upper_regret_count(self.ptr), np.float32)
         riv = np.zeros((self.num_rivers, EDGES, BUCKETS), np.float32)
         _check(lib().pr_game_get_regrets(self.ptr, _ptr(up), _ptr(riv)), "pr_game_get_regrets")
+        return up, riv
+
+    def enable_average(self):
+        _check(lib().pr_game_enable_average(self.ptr), "pr_game_enable_average")
+
+    def average_sums(self):
+        up = np.zeros(lib().pr_game_upper_regret_count(self.ptr), np.float32)
+        riv = np.zeros((self.num_rivers, EDGES, BUCKETS), np.float32)
+        _check(lib().pr_game_get_average(self.ptr, _ptr(up), _ptr(riv)), "pr_game_get_average")
         return up, riv
 
     def close(self):

@@ -266,3 +266,37 @@ def test_shared_memory_sized_by_flop(P, gpu_tables):
     for exploit, fp64 in ((0, 0), (1, 0), (1, 1)):
         smem = P.lib().pr_river_smem_bytes(gpu_tables, exploit, fp64)
         assert 0 < smem <= 227 * 1024
+
+
+@pytest.mark.parametrize("player", [0, 1])
+def test_average_strategy_sums(P, gpu_tables, flop_tables, player):
+    # average-strategy sums of one CFR pass and of a second pass on top (the reference keeps
+    # none; checked against the oracle's restatement, oracle/river.cpp)
+    rng = np.random.default_rng(50 + player)
+    n = 8
+    board4, bet, opp = subgames(rng, n)
+    _, _, own = subgames(rng, n, turns=[(int(x) ^ O.REFERENCE_FLOP).bit_length() - 1 for x in board4])
+    reg = random_regrets(rng, n)
+    e, _, a = flop_tables
+    b = P.Builder()
+    for cards, bt in zip(board4, bet):
+        b.add(int(cards), float(bt))
+    b.enable_average()
+    b.set_regrets(reg)
+    ref_reg = reg.copy()
+    ref_avg = np.zeros((n, 26, 256), np.float32)
+    for _ in range(2):
+        b.upload_all(opp)
+        b.upload_own_all(own)
+        P.evaluate_gpu(b.ptr, gpu_tables, player, False)
+        got = b.download_all()
+        want = O.river_batch_avg(O.REFERENCE_FLOP, e, a, board4, bet, opp, own, ref_reg, ref_avg, player)
+        assert_close(got, want, "values")
+    avg = b.average_sums()
+    b.close()
+    assert_close(avg.reshape(n, -1), ref_avg.reshape(n, -1), "average-strategy sums")
+    # only the updater's edges accumulate
+    t = O.river_tree()
+    other = [int(t["edge"][s][k]) for s in range(28) if t["terminal"][s] == 0 and t["actor"][s] != player
+             for k in range(t["nchild"][s])]
+    assert np.all(avg[:, other, :] == 0)
