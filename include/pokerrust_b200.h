@@ -93,6 +93,7 @@ int pr_download_batch(void *builder, int first, int count, float *v);
 int pr_enable_average(void *builder);
 void pr_upload_own(void *builder, int index, const float *v);
 int pr_get_average(void *builder, float *out);
+int pr_set_average(void *builder, const float *in);
 
 /* Number of river subgames in the builder, and the row stride (floats) of pr_* buffers. */
 int pr_builder_count(void *builder);
@@ -155,6 +156,11 @@ int pr_game_get_regrets(void *game, float *upper, float *river);
  * river sums (per bucket, pr_get_average layout) from the next iteration on. */
 int pr_game_enable_average(void *game);
 int pr_game_get_average(void *game, float *upper, float *river);
+/* Checkpoints: regrets (and average sums, when enabled) of the whole game in a versioned,
+ * checksummed binary file; loading checks the flop and sizes. 0 = success, 3 = wrong or
+ * corrupted file. */
+int pr_game_save(void *game, const char *path);
+int pr_game_load(void *game, const char *path);
 
 #ifdef __cplusplus
 }

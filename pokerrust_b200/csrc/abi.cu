@@ -583,6 +583,18 @@ int pr_get_average(void *builder, float *out) {
     return e == cudaSuccess ? kOk : fail(kErrCuda, "average download", e);
 }
 
+int pr_set_average(void *builder, const float *in) {
+    Builder *b = (Builder *)builder;
+    if (!b || !in || !b->avg_on) return fail(kErrArg, "pr_set_average: averages not enabled");
+    int st = sync_device(b);
+    if (st) return st;
+    if ((st = sync_average(b))) return st;
+    cudaError_t e = cudaMemcpyAsync(b->d_avg, in, (size_t)b->dev_count * kEdges * kBuckets * sizeof(float),
+                                    cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? kOk : fail(kErrCuda, "average upload", e);
+}
+
 int pr_builder_count(void *builder) { return builder ? (int)((Builder *)builder)->desc.size() : 0; }
 
 int pr_range_stride(void) { return kRangeStride; }

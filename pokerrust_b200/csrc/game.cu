@@ -12,6 +12,7 @@
 // The upload pass only propagates ranges: in the reference its utilities are discarded.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
@@ -626,6 +627,98 @@ int pr_game_enable_average(void *game) {
     if (st) return st;
     g->avg_upper.assign(g->regrets.size(), 0.0f);
     g->avg_on = true;
+    return 0;
+}
+
+// ---- checkpoints -------------------------------------------------------------------
+// File layout (little endian):
+//   magic "PRBCKPT1" | u32 version (1) | u32 flags (bit 0: average sums present)
+//   u64 flop | u64 river roots | u64 upper regret floats
+//   u64 FNV-1a 64 hash of everything after this header
+//   f32 river regrets [roots][26][256] | f32 upper regrets [upper]
+//   if flags & 1: f32 river average sums [roots][26][256] | f32 upper average sums [upper]
+// Tables are not stored: they follow from the flop and are rebuilt on the device.
+namespace {
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, flags;
+    uint64_t flop, rivers, upper, hash;
+};
+uint64_t fnv1a(const void *p, size_t n, uint64_t h) {
+    const unsigned char *c = (const unsigned char *)p;
+    for (size_t i = 0; i < n; i++) h = (h ^ c[i]) * 1099511628211ull;
+    return h;
+}
+}  // namespace
+
+int pr_game_save(void *game, const char *path) {
+    Game *g = (Game *)game;
+    if (!g || !path) return 2;
+    const size_t nr = g->river_board.size() * 26 * 256, nu = g->regrets.size();
+    std::vector<float> river(nr), river_avg;
+    if (pr_get_regrets(g->builder, river.data())) return 1;
+    if (g->avg_on) {
+        river_avg.resize(nr);
+        if (pr_get_average(g->builder, river_avg.data())) return 1;
+    }
+    CkptHeader hd{};
+    memcpy(hd.magic, "PRBCKPT1", 8);
+    hd.version = 1;
+    hd.flags = g->avg_on ? 1u : 0u;
+    hd.flop = g->flop;
+    hd.rivers = g->river_board.size();
+    hd.upper = nu;
+    uint64_t h = 1469598103934665603ull;
+    h = fnv1a(river.data(), nr * 4, h);
+    h = fnv1a(g->regrets.data(), nu * 4, h);
+    if (g->avg_on) {
+        h = fnv1a(river_avg.data(), nr * 4, h);
+        h = fnv1a(g->avg_upper.data(), nu * 4, h);
+    }
+    hd.hash = h;
+    FILE *f = fopen(path, "wb");
+    if (!f) return 2;
+    bool ok = fwrite(&hd, sizeof(hd), 1, f) == 1 && fwrite(river.data(), 4, nr, f) == nr &&
+              fwrite(g->regrets.data(), 4, nu, f) == nu;
+    if (ok && g->avg_on)
+        ok = fwrite(river_avg.data(), 4, nr, f) == nr && fwrite(g->avg_upper.data(), 4, nu, f) == nu;
+    ok = (fclose(f) == 0) && ok;
+    return ok ? 0 : 1;
+}
+
+int pr_game_load(void *game, const char *path) {
+    Game *g = (Game *)game;
+    if (!g || !path) return 2;
+    FILE *f = fopen(path, "rb");
+    if (!f) return 2;
+    CkptHeader hd{};
+    const size_t nr = g->river_board.size() * 26 * 256, nu = g->regrets.size();
+    bool ok = fread(&hd, sizeof(hd), 1, f) == 1 && memcmp(hd.magic, "PRBCKPT1", 8) == 0 && hd.version == 1 &&
+              hd.flop == g->flop && hd.rivers == g->river_board.size() && hd.upper == nu;
+    std::vector<float> river(nr), upper(nu), river_avg, upper_avg;
+    ok = ok && fread(river.data(), 4, nr, f) == nr && fread(upper.data(), 4, nu, f) == nu;
+    if (ok && (hd.flags & 1)) {
+        river_avg.resize(nr);
+        upper_avg.resize(nu);
+        ok = fread(river_avg.data(), 4, nr, f) == nr && fread(upper_avg.data(), 4, nu, f) == nu;
+    }
+    fclose(f);
+    if (!ok) return 3;
+    uint64_t h = 1469598103934665603ull;
+    h = fnv1a(river.data(), nr * 4, h);
+    h = fnv1a(upper.data(), nu * 4, h);
+    if (hd.flags & 1) {
+        h = fnv1a(river_avg.data(), nr * 4, h);
+        h = fnv1a(upper_avg.data(), nu * 4, h);
+    }
+    if (h != hd.hash) return 3;  // corrupted file
+    if (pr_set_regrets(g->builder, river.data())) return 1;
+    g->regrets = upper;
+    if (hd.flags & 1) {
+        if (pr_game_enable_average(g)) return 1;
+        if (pr_set_average(g->builder, river_avg.data())) return 1;
+        g->avg_upper = upper_avg;
+    }
     return 0;
 }
 

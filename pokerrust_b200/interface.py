@@ -93,6 +93,12 @@ def lib():
         L.pr_game_enable_average.argtypes = [vp]
         L.pr_game_get_average.restype = i32
         L.pr_game_get_average.argtypes = [vp, vp, vp]
+        L.pr_set_average.restype = i32
+        L.pr_set_average.argtypes = [vp, vp]
+        L.pr_game_save.restype = i32
+        L.pr_game_save.argtypes = [vp, ctypes.c_char_p]
+        L.pr_game_load.restype = i32
+        L.pr_game_load.argtypes = [vp, ctypes.c_char_p]
         L.pr_game_get_regrets.restype = i32
         L.pr_game_get_regrets.argtypes = [vp, vp, vp]
         L.pr_enable_average.restype = i32
@@ -349,6 +355,16 @@ class Game:
 
     def enable_average(self):
         _check(lib().pr_game_enable_average(self.ptr), "pr_game_enable_average")
+
+    def save(self, path):
+        st = lib().pr_game_save(self.ptr, os.fsencode(path))
+        if st:
+            raise PokerLibError(f"pr_game_save failed ({st})")
+
+    def load(self, path):
+        st = lib().pr_game_load(self.ptr, os.fsencode(path))
+        if st:
+            raise PokerLibError(f"pr_game_load failed ({st}): wrong game, corrupted or unreadable file")
 
     def average_sums(self):
         up = np.zeros(lib().pr_game_upper_regret_count(self.ptr), np.float32)

@@ -74,3 +74,33 @@ def test_exploitability_and_two_iterations(game, golden):
                     for i in range(len(want))])
     assert np.median(err) < 1e-4, np.sort(err)
     assert np.mean(err < 1e-3) >= 0.9, np.sort(err)
+
+
+def test_checkpoint_round_trip(tmp_path):
+    import pokerrust_b200 as P
+    a = P.Game(O.REFERENCE_FLOP)
+    a.enable_average()
+    a.iterate(2)
+    path = str(tmp_path / "ckpt.bin")
+    a.save(path)
+    b = P.Game(O.REFERENCE_FLOP)
+    b.load(path)
+    ua, ra = a.regrets()
+    ub, rb = b.regrets()
+    assert np.array_equal(ua, ub) and np.array_equal(ra, rb)
+    aa, ar = a.average_sums()
+    ba, br = b.average_sums()
+    assert np.array_equal(aa, ba) and np.array_equal(ar, br)
+    # the solver is deterministic: one more iteration from the same state is identical
+    a.iterate(1)
+    b.iterate(1)
+    assert np.array_equal(a.regrets()[1], b.regrets()[1])
+    assert np.array_equal(a.regrets()[0], b.regrets()[0])
+    # a corrupted file is refused
+    data = bytearray(open(path, "rb").read())
+    data[200] ^= 0xFF
+    open(path, "wb").write(bytes(data))
+    with pytest.raises(P.PokerLibError):
+        b.load(path)
+    a.close()
+    b.close()
