@@ -128,6 +128,17 @@ size_t pr_river_smem_bytes(void *eval, int calc_exploit, int fp64);
 int pr_evaluate_br64(void *builder, void *eval, int updating_player, const double *ranges,
                      double *results);
 
+/* The same passes on caller-owned device rows of 1328 (pr_range_stride) on `stream`
+ * (null = the builder's stream), asynchronous:
+ * pr_evaluate_device_own is a CFR pass that also accumulates average-strategy sums from the
+ * updater's own ranges d_own (pr_enable_average first); pr_evaluate_br64_device is the
+ * double-precision best response. No reference counterparts: they let a device-side upper
+ * tree feed the river solver without host copies. */
+int pr_evaluate_device_own(void *builder, void *eval, int updating_player, const float *d_ranges,
+                           const float *d_own, float *d_results, void *stream);
+int pr_evaluate_br64_device(void *builder, void *eval, int updating_player, const double *d_ranges,
+                            double *d_results, void *stream);
+
 /* ---- whole-game driver (extension): the host side of the reference's GPU build ----
  * (src/builder.rs, src/state.rs, src/strategy.rs:37-82, src/permutation_handler.rs,
  * src/game.rs) over the functions above. Tables are built on the device. */
@@ -144,6 +155,11 @@ void *pr_game_builder(void *game);
 void *pr_game_tables(void *game);
 /* CFR iterations (game.rs:68-119): small blind update, then big blind update. */
 int pr_game_iterate(void *game, int iterations);
+/* Where the preflop/flop/turn tree is traversed: 1 (default) on the device, level by level,
+ * with each iteration replayed as one CUDA graph; 0 on the host through upload_c /
+ * evaluate_cuda / download_c, the reference's protocol (game.rs:68-119). Both give the
+ * same results bit for bit. Returns the previous setting, or -1 on error. */
+int pr_game_set_device_tree(void *game, int on);
 /* Best-response sums of both players and the reference's mb/h figure (game.rs:120-178);
  * fp64 = 1 runs the whole best response in double precision. */
 int pr_game_exploitability(void *game, int fp64, double *sum_sb, double *sum_bb, double *mbh);

@@ -265,7 +265,7 @@ int sync_device(Builder *b) {
 }
 
 int evaluate_impl(Builder *b, EvalTables *t, int player, int exploit, const float *d_in, float *d_out,
-                  cudaStream_t stream, bool staged) {
+                  cudaStream_t stream, bool staged, const float *d_own = nullptr) {
     if (!b || !t) return fail(kErrArg, "evaluate: null builder or tables");
     if (t->status) return fail(kErrTables, "evaluate: tables failed validation on upload");
     if (player != 0 && player != 1) return fail(kErrArg, "evaluate: updating_player must be 0 or 1");
@@ -284,12 +284,14 @@ int evaluate_impl(Builder *b, EvalTables *t, int player, int exploit, const floa
     if (n == 0) return kOk;
     cudaStream_t s = stream ? stream : b->stream;
     cudaError_t e;
-    const bool avg = staged && b->avg_on && !exploit;
+    const bool avg = (staged || d_own) && b->avg_on && !exploit;
     if (avg) {
         if ((st = sync_average(b))) return st;
-        e = cudaMemcpyAsync(b->d_own, b->comm_own, (size_t)n * kRangeStride * sizeof(float),
-                            cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) return fail(kErrCuda, "own range upload", e);
+        if (staged) {
+            e = cudaMemcpyAsync(b->d_own, b->comm_own, (size_t)n * kRangeStride * sizeof(float),
+                                cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess) return fail(kErrCuda, "own range upload", e);
+        }
     }
     if (staged) {
         e = cudaMemcpyAsync(b->d_ranges, b->comm, (size_t)n * kRangeStride * sizeof(float),
@@ -299,7 +301,7 @@ int evaluate_impl(Builder *b, EvalTables *t, int player, int exploit, const floa
         d_out = b->d_results;
     }
     e = launch_river(exploit ? kModeBR : kModeCFR, b->d_desc, n, d_in, d_out, b->d_regrets, t->packs,
-                     t->flop, player, t->max_groups, t->max_card_groups, avg ? b->d_own : nullptr,
+                     t->flop, player, t->max_groups, t->max_card_groups, avg ? (staged ? b->d_own : d_own) : nullptr,
                      avg ? b->d_avg : nullptr, s);
     if (e != cudaSuccess) return fail(kErrCuda, "river kernel launch", e);
     if (staged) {
@@ -529,6 +531,15 @@ int pr_evaluate_device(void *builder, void *eval, int updating_player, int calc_
                          d_results, (cudaStream_t)stream, false);
 }
 
+int pr_evaluate_device_own(void *builder, void *eval, int updating_player, const float *d_ranges,
+                           const float *d_own, float *d_results, void *stream) {
+    Builder *b = (Builder *)builder;
+    if (!d_ranges || !d_results || !d_own) return fail(kErrArg, "pr_evaluate_device_own: null buffer");
+    if (!b || !b->avg_on) return fail(kErrArg, "pr_evaluate_device_own: average strategies are not enabled");
+    return evaluate_impl(b, (EvalTables *)eval, updating_player, 0, d_ranges, d_results, (cudaStream_t)stream,
+                         false, d_own);
+}
+
 int pr_upload_batch(void *builder, int first, int count, const float *v) {
     Builder *b = (Builder *)builder;
     if (!b || !v || first < 0 || count < 0 || first + count > (int)b->desc.size())
@@ -679,9 +690,11 @@ size_t pr_river_smem_bytes(void *eval, int calc_exploit, int fp64) {
     return river_smem_bytes(calc_exploit ? kModeBR : kModeCFR, fp64, t->max_groups, t->max_card_groups);
 }
 
-int pr_evaluate_br64(void *builder, void *eval, int updating_player, const double *ranges, double *results) {
-    Builder *b = (Builder *)builder;
-    EvalTables *t = (EvalTables *)eval;
+namespace {
+// Double-precision best response: host rows of 1326 (staged through the builder's device
+// buffers) or device rows of kRangeStride on the caller's stream.
+int br64_impl(Builder *b, EvalTables *t, int updating_player, const double *ranges, double *results,
+              bool staged, cudaStream_t stream) {
     if (!b || !t || !ranges || !results) return fail(kErrArg, "pr_evaluate_br64: null argument");
     if (t->status) return fail(kErrTables, "pr_evaluate_br64: tables failed validation");
     if (updating_player != 0 && updating_player != 1) return fail(kErrArg, "pr_evaluate_br64: bad player");
@@ -693,6 +706,11 @@ int pr_evaluate_br64(void *builder, void *eval, int updating_player, const doubl
     const int n = b->dev_count;
     if (n == 0) return kOk;
     cudaError_t e;
+    if (!staged) {
+        e = launch_river_br64(b->d_desc, n, ranges, results, b->d_regrets, t->packs, t->flop, updating_player,
+                              t->max_groups, t->max_card_groups, stream ? stream : b->stream);
+        return e == cudaSuccess ? kOk : fail(kErrCuda, "double best-response launch", e);
+    }
     if (b->cap64 < b->dev_capacity) {
         cudaFree(b->d_ranges64);
         cudaFree(b->d_results64);
@@ -717,6 +735,17 @@ int pr_evaluate_br64(void *builder, void *eval, int updating_player, const doubl
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return fail(kErrCuda, "double best-response pass", e);
     return kOk;
+}
+}  // namespace
+
+int pr_evaluate_br64(void *builder, void *eval, int updating_player, const double *ranges, double *results) {
+    return br64_impl((Builder *)builder, (EvalTables *)eval, updating_player, ranges, results, true, nullptr);
+}
+
+int pr_evaluate_br64_device(void *builder, void *eval, int updating_player, const double *d_ranges,
+                            double *d_results, void *stream) {
+    return br64_impl((Builder *)builder, (EvalTables *)eval, updating_player, d_ranges, d_results, false,
+                     (cudaStream_t)stream);
 }
 
 }  // extern "C"

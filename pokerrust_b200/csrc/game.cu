@@ -29,6 +29,8 @@
 #include <vector>
 
 #include "../../include/pokerrust_b200.h"
+#include "layout.h"
+#include "upper_tree.h"
 
 namespace prb {
 namespace {
@@ -123,6 +125,23 @@ struct Scratch {
 
 enum Pass { kUpload = 0, kDownload = 1 };
 
+// Device copy of the upper tree (upper_tree.cu): nodes, the level lists of the two sweeps,
+// regrets and average sums, reach vectors and values of every node, the river rows.
+struct DevTree {
+    cudaStream_t stream = nullptr;
+    DevNode *nodes = nullptr;
+    int32_t *kids = nullptr, *perm_maps = nullptr, *levels = nullptr;
+    std::vector<int> level_off;  // level d = levels[level_off[d], level_off[d + 1])
+    float *regrets = nullptr, *avg = nullptr;
+    float *Rf = nullptr, *Vf = nullptr;   // [node][2][kRangeStride], [node][kRangeStride]
+    double *Rd = nullptr, *Vd = nullptr;  // double-precision best response (lazily allocated)
+    float *opp = nullptr, *val = nullptr, *own = nullptr;  // [river][kRangeStride]
+    double *opp64 = nullptr, *val64 = nullptr;
+    cudaGraphExec_t graph = nullptr;      // one CFR iteration, replayed
+    bool graph_avg = false, graph_failed = false;
+    bool ready = false;
+};
+
 struct Game {
     uint64_t flop = 0;
     void *tables = nullptr;
@@ -142,6 +161,10 @@ struct Game {
     int max_depth = 0;
     double t_host = 0, t_gpu = 0;
     int status = 0;
+    bool device_tree = true;
+    DevTree dt;
+    bool host_stale = false;  // the device holds newer upper regrets / sums than the host
+    bool dev_stale = true;    // the host holds newer ones than the device
 
     // ---- tree construction (builder.rs:34-79, state.rs:66-217) ----
     static int popc(uint64_t x) { return __builtin_popcountll(x); }
@@ -311,8 +334,225 @@ struct Game {
 
     ~Game() {
         delete pool;
+        dt_release();
         if (builder) pr_free_builder(builder);
         if (tables) free_eval_cuda(tables);
+    }
+
+    // ---- device upper tree ----
+    void dt_release() {
+        if (dt.graph) cudaGraphExecDestroy(dt.graph);
+        if (dt.stream) cudaStreamSynchronize(dt.stream);
+        for (void *p : {(void *)dt.nodes, (void *)dt.kids, (void *)dt.perm_maps, (void *)dt.levels,
+                        (void *)dt.regrets, (void *)dt.avg, (void *)dt.Rf, (void *)dt.Vf, (void *)dt.Rd,
+                        (void *)dt.Vd, (void *)dt.opp, (void *)dt.val, (void *)dt.own, (void *)dt.opp64,
+                        (void *)dt.val64})
+            cudaFree(p);
+        if (dt.stream) cudaStreamDestroy(dt.stream);
+        dt = DevTree();
+    }
+
+    static int cuda_fail(const char *what, cudaError_t e) {
+        fprintf(stderr, "pokerrust_b200: device upper tree: %s: %s\n", what, cudaGetErrorString(e));
+        return 1;
+    }
+
+    template <typename X>
+    static cudaError_t upload(X **dst, const X *src, size_t n) {
+        cudaError_t e = cudaMalloc((void **)dst, n * sizeof(X));
+        if (e == cudaSuccess && src) e = cudaMemcpy(*dst, src, n * sizeof(X), cudaMemcpyHostToDevice);
+        return e;
+    }
+
+    int dt_init() {
+        if (dt.ready) return 0;
+        cudaError_t e;
+        if ((e = cudaStreamCreateWithFlags(&dt.stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_fail("stream", e);
+        const size_t N = nodes.size(), R = river_board.size();
+        std::vector<DevNode> dn(N);
+        std::vector<int> depth(N, 0);
+        int D = 1;
+        for (size_t i = 0; i < N; i++) {
+            const UNode &u = nodes[i];
+            DevNode &d = dn[i];
+            d = DevNode{};
+            d.kind = u.kind;
+            d.actor = u.actor;
+            d.nchild = u.nchild;
+            d.first = u.first;
+            d.cards = u.cards;
+            d.sb = u.sb;
+            d.bb = u.bb;
+            d.regret = u.regret;
+            d.river = u.river;
+            d.perm_first = u.perm_first;
+            d.nperm = u.nperm;
+            for (int k = 0; k < u.nchild; k++) {  // children follow their parent in `nodes`
+                depth[kids[u.first + k]] = depth[i] + 1;
+                D = std::max(D, depth[i] + 2);
+            }
+        }
+        std::vector<int32_t> lv;
+        dt.level_off.assign(1, 0);
+        for (int d = 0; d < D; d++) {
+            for (size_t i = 0; i < N; i++)
+                if (depth[i] == d) lv.push_back((int32_t)i);
+            dt.level_off.push_back((int)lv.size());
+        }
+        std::vector<int32_t> pm;
+        for (auto &m : perm_maps) pm.insert(pm.end(), m.begin(), m.end());
+        if ((e = upload(&dt.nodes, dn.data(), N)) != cudaSuccess || (e = upload(&dt.kids, kids.data(), kids.size())) ||
+            (e = upload(&dt.perm_maps, pm.data(), pm.size())) || (e = upload(&dt.levels, lv.data(), lv.size())) ||
+            (e = upload(&dt.regrets, regrets.data(), regrets.size())) ||
+            (e = upload<float>(&dt.Rf, nullptr, N * 2 * kRangeStride)) ||
+            (e = upload<float>(&dt.Vf, nullptr, N * kRangeStride)) ||
+            (e = upload<float>(&dt.opp, nullptr, R * kRangeStride)) ||
+            (e = upload<float>(&dt.val, nullptr, R * kRangeStride)))
+            return cuda_fail("allocation", e);
+        dt.ready = true;
+        dev_stale = true;
+        return 0;
+    }
+
+    int dt_alloc64() {
+        if (dt.Rd) return 0;
+        const size_t N = nodes.size(), R = river_board.size();
+        cudaError_t e;
+        if ((e = upload<double>(&dt.Rd, nullptr, N * 2 * kRangeStride)) ||
+            (e = upload<double>(&dt.Vd, nullptr, N * kRangeStride)) ||
+            (e = upload<double>(&dt.opp64, nullptr, R * kRangeStride)) ||
+            (e = upload<double>(&dt.val64, nullptr, R * kRangeStride)))
+            return cuda_fail("double-precision allocation", e);
+        return 0;
+    }
+
+    // host -> device copies of the upper regrets and sums when the host changed them
+    int dt_push() {
+        if (int st = dt_init()) return st;
+        if (!dev_stale) return 0;
+        cudaError_t e = cudaMemcpy(dt.regrets, regrets.data(), regrets.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && avg_on) {
+            const size_t rows = (size_t)river_board.size() * kRangeStride;
+            if (!dt.avg && (e = cudaMalloc(&dt.avg, avg_upper.size() * 4)) == cudaSuccess)
+                e = cudaMalloc(&dt.own, rows * 4);
+            if (e == cudaSuccess) e = cudaMemset(dt.own, 0, rows * 4);
+            if (e == cudaSuccess) e = cudaMemcpy(dt.avg, avg_upper.data(), avg_upper.size() * 4, cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) return cuda_fail("regret upload", e);
+        dev_stale = false;
+        return 0;
+    }
+
+    // device -> host copies when the device changed them
+    int dt_pull() {
+        if (!host_stale) return 0;
+        cudaError_t e = cudaStreamSynchronize(dt.stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(regrets.data(), dt.regrets, regrets.size() * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && avg_on && dt.avg)
+            e = cudaMemcpy(avg_upper.data(), dt.avg, avg_upper.size() * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail("regret download", e);
+        host_stale = false;
+        return 0;
+    }
+
+    // One half-iteration or best-response pass on the device, enqueued on dt.stream:
+    // root ranges, top-down levels, the river pass, bottom-up levels.
+    template <typename T>
+    int dt_half(int upd, bool br) {
+        const bool f64 = sizeof(T) == 8;
+        T *R = f64 ? (T *)dt.Rd : (T *)dt.Rf;
+        T *V = f64 ? (T *)dt.Vd : (T *)dt.Vf;
+        T *opp = f64 ? (T *)dt.opp64 : (T *)dt.opp;
+        T *val = f64 ? (T *)dt.val64 : (T *)dt.val;
+        const bool avg = avg_on && !br;
+        UpperView v{dt.nodes, dt.kids, dt.perm_maps, dt.regrets};
+        cudaError_t e = upper_set_root(f64 ? nullptr : dt.Rf, f64 ? dt.Rd : nullptr, dt.stream);
+        const int D = (int)dt.level_off.size() - 1;
+        for (int d = 0; d < D && e == cudaSuccess; d++)
+            e = upper_down<T>(v, dt.levels + dt.level_off[d], dt.level_off[d + 1] - dt.level_off[d], upd, R,
+                              opp, avg ? dt.own : nullptr, dt.stream);
+        if (e != cudaSuccess) return cuda_fail("top-down sweep", e);
+        int st;
+        if (f64) st = pr_evaluate_br64_device(builder, tables, upd, dt.opp64, dt.val64, dt.stream);
+        else if (avg) st = pr_evaluate_device_own(builder, tables, upd, dt.opp, dt.own, dt.val, dt.stream);
+        else st = pr_evaluate_device(builder, tables, upd, br ? 1 : 0, dt.opp, dt.val, dt.stream);
+        if (st) return st;
+        for (int d = D - 1; d >= 0 && e == cudaSuccess; d--)
+            e = upper_up<T>(v, dt.levels + dt.level_off[d], dt.level_off[d + 1] - dt.level_off[d], upd, br ? 1 : 0,
+                            R, V, val, dt.regrets, avg ? dt.avg : nullptr, dt.stream);
+        if (e != cudaSuccess) return cuda_fail("bottom-up sweep", e);
+        return 0;
+    }
+
+    // A CFR iteration as one graph: captured after an eager first iteration (which sets up
+    // everything the river pass allocates lazily); eager launches if capture is refused.
+    int dt_iterate(int iterations) {
+        using clk = std::chrono::steady_clock;
+        auto t0 = clk::now();
+        if (int st = dt_push()) return st;
+        if (dt.graph && dt.graph_avg != avg_on) {
+            cudaGraphExecDestroy(dt.graph);
+            dt.graph = nullptr;
+        }
+        int it = 0;
+        if (!dt.graph && !dt.graph_failed && iterations > 0) {
+            for (int upd = 0; upd < 2; upd++)
+                if (int st = dt_half<float>(upd, false)) return st;
+            it++;
+            cudaError_t e = cudaStreamSynchronize(dt.stream);
+            if (e != cudaSuccess) return cuda_fail("iteration", e);
+            cudaGraph_t g = nullptr;
+            int st = 0;
+            e = cudaStreamBeginCapture(dt.stream, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                for (int upd = 0; upd < 2 && !st; upd++) st = dt_half<float>(upd, false);
+                e = cudaStreamEndCapture(dt.stream, &g);
+            }
+            if (e == cudaSuccess && !st && g) e = cudaGraphInstantiate(&dt.graph, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess || st || !dt.graph) {
+                cudaGetLastError();
+                dt.graph = nullptr;
+                dt.graph_failed = true;
+                pr_clear_error();
+            }
+            dt.graph_avg = avg_on;
+        }
+        for (; it < iterations; it++) {
+            if (dt.graph) {
+                cudaError_t e = cudaGraphLaunch(dt.graph, dt.stream);
+                if (e != cudaSuccess) return cuda_fail("graph launch", e);
+            } else {
+                for (int upd = 0; upd < 2; upd++)
+                    if (int st = dt_half<float>(upd, false)) return st;
+            }
+        }
+        cudaError_t e = cudaStreamSynchronize(dt.stream);
+        if (e != cudaSuccess) return cuda_fail("iteration", e);
+        host_stale = true;
+        t_gpu += std::chrono::duration<double>(clk::now() - t0).count();
+        return 0;
+    }
+
+    // Best-response values of both players at the root, on the device.
+    template <typename T>
+    int dt_exploit(T *sb, T *bb) {
+        using clk = std::chrono::steady_clock;
+        auto t0 = clk::now();
+        if (int st = dt_push()) return st;
+        if (sizeof(T) == 8)
+            if (int st = dt_alloc64()) return st;
+        T *V = sizeof(T) == 8 ? (T *)dt.Vd : (T *)dt.Vf;
+        for (int upd = 0; upd < 2; upd++) {
+            if (int st = dt_half<T>(upd, true)) return st;
+            cudaError_t e = cudaMemcpyAsync(upd == 0 ? sb : bb, V, sizeof(T) * H, cudaMemcpyDeviceToHost, dt.stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(dt.stream);
+            if (e != cudaSuccess) return cuda_fail("best response", e);
+        }
+        t_gpu += std::chrono::duration<double>(clk::now() - t0).count();
+        return 0;
     }
 
     // ---- traversal (state.rs:219-376) ----
@@ -480,6 +720,8 @@ struct Game {
     // One half-iteration or best-response pass of `upd` (game.rs:73-96 / 122-168).
     template <typename T>
     int half(int upd, bool br, T *out) {
+        if (int st = dt_pull()) return st;
+        if (!br) dev_stale = true;
         using clk = std::chrono::steady_clock;
         Scratch<T> sc(max_depth + 2);
         std::vector<T> ones(H, T(1));
@@ -555,6 +797,7 @@ void *pr_game_tables(void *game) { return game ? ((Game *)game)->tables : nullpt
 int pr_game_iterate(void *game, int iterations) {
     Game *g = (Game *)game;
     if (!g) return 2;
+    if (g->device_tree) return g->dt_iterate(iterations);
     std::vector<float> out(prb::H);
     for (int it = 0; it < iterations; it++) {
         for (int upd = 0; upd < 2; upd++) {
@@ -569,12 +812,19 @@ int pr_game_exploitability(void *game, int fp64, double *sum_sb, double *sum_bb,
     Game *g = (Game *)game;
     if (!g) return 2;
     if (fp64) {
-        const size_t n = g->river_board.size() * prb::H;
-        g->ranges64.assign(n, 0.0);
-        g->results64.assign(n, 0.0);
+        if (!g->device_tree) {
+            const size_t n = g->river_board.size() * prb::H;
+            g->ranges64.assign(n, 0.0);
+            g->results64.assign(n, 0.0);
+        }
         std::vector<double> sb(prb::H), bb(prb::H);
-        int st = g->half<double>(0, true, sb.data());
-        if (!st) st = g->half<double>(1, true, bb.data());
+        int st;
+        if (g->device_tree) {
+            st = g->dt_exploit<double>(sb.data(), bb.data());
+        } else {
+            st = g->half<double>(0, true, sb.data());
+            if (!st) st = g->half<double>(1, true, bb.data());
+        }
         if (st) return st;
         double s1 = 0, s2 = 0;
         for (int i = 0; i < prb::H; i++) {
@@ -587,8 +837,13 @@ int pr_game_exploitability(void *game, int fp64, double *sum_sb, double *sum_bb,
         return 0;
     }
     std::vector<float> sb(prb::H), bb(prb::H);
-    int st = g->half<float>(0, true, sb.data());
-    if (!st) st = g->half<float>(1, true, bb.data());
+    int st;
+    if (g->device_tree) {
+        st = g->dt_exploit<float>(sb.data(), bb.data());
+    } else {
+        st = g->half<float>(0, true, sb.data());
+        if (!st) st = g->half<float>(1, true, bb.data());
+    }
     if (st) return st;
     float s1 = 0, s2 = 0;
     for (int i = 0; i < prb::H; i++) {
@@ -609,9 +864,18 @@ int pr_game_timings(void *game, double *host_seconds, double *device_seconds) {
     return 0;
 }
 
+int pr_game_set_device_tree(void *game, int on) {
+    Game *g = (Game *)game;
+    if (!g) return -1;
+    const int was = g->device_tree ? 1 : 0;
+    g->device_tree = on != 0;
+    return was;
+}
+
 int pr_game_get_regrets(void *game, float *upper, float *river) {
     Game *g = (Game *)game;
     if (!g) return 2;
+    if (int st = g->dt_pull()) return st;
     if (upper) memcpy(upper, g->regrets.data(), g->regrets.size() * sizeof(float));
     if (river) return pr_get_regrets(g->builder, river);
     return 0;
@@ -623,10 +887,12 @@ int pr_game_enable_average(void *game) {
     Game *g = (Game *)game;
     if (!g) return 2;
     if (g->avg_on) return 0;
+    if (int st = g->dt_pull()) return st;
     const int st = pr_enable_average(g->builder);
     if (st) return st;
     g->avg_upper.assign(g->regrets.size(), 0.0f);
     g->avg_on = true;
+    g->dev_stale = true;
     return 0;
 }
 
@@ -654,6 +920,7 @@ uint64_t fnv1a(const void *p, size_t n, uint64_t h) {
 int pr_game_save(void *game, const char *path) {
     Game *g = (Game *)game;
     if (!g || !path) return 2;
+    if (int st = g->dt_pull()) return st;
     const size_t nr = g->river_board.size() * 26 * 256, nu = g->regrets.size();
     std::vector<float> river(nr), river_avg;
     if (pr_get_regrets(g->builder, river.data())) return 1;
@@ -712,6 +979,7 @@ int pr_game_load(void *game, const char *path) {
         h = fnv1a(upper_avg.data(), nu * 4, h);
     }
     if (h != hd.hash) return 3;  // corrupted file
+    if (g->dt_pull()) return 1;
     if (pr_set_regrets(g->builder, river.data())) return 1;
     g->regrets = upper;
     if (hd.flags & 1) {
@@ -719,12 +987,14 @@ int pr_game_load(void *game, const char *path) {
         if (pr_set_average(g->builder, river_avg.data())) return 1;
         g->avg_upper = upper_avg;
     }
+    g->dev_stale = true;
     return 0;
 }
 
 int pr_game_get_average(void *game, float *upper, float *river) {
     Game *g = (Game *)game;
     if (!g || !g->avg_on) return 2;
+    if (int st = g->dt_pull()) return st;
     if (upper) memcpy(upper, g->avg_upper.data(), g->avg_upper.size() * sizeof(float));
     if (river) return pr_get_average(g->builder, river);
     return 0;

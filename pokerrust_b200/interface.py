@@ -83,6 +83,12 @@ def lib():
         L.pr_game_tables.argtypes = [vp]
         L.pr_game_iterate.restype = i32
         L.pr_game_iterate.argtypes = [vp, i32]
+        L.pr_game_set_device_tree.restype = i32
+        L.pr_game_set_device_tree.argtypes = [vp, i32]
+        L.pr_evaluate_device_own.restype = i32
+        L.pr_evaluate_device_own.argtypes = [vp, vp, i32, vp, vp, vp, vp]
+        L.pr_evaluate_br64_device.restype = i32
+        L.pr_evaluate_br64_device.argtypes = [vp, vp, i32, vp, vp, vp]
         L.pr_game_exploitability.restype = i32
         L.pr_game_exploitability.argtypes = [vp, i32, vp, vp, vp]
         L.pr_game_timings.restype = i32
@@ -306,13 +312,19 @@ class Builder:
 
 
 class Game:
-    """The whole fixed-flop game (src/game.rs) driven on the device: upper tree on the host,
-    river subgames on the GPU, tables generated on the GPU."""
+    """The whole fixed-flop game (src/game.rs) on the device: tables generated on the GPU,
+    river subgames on the GPU, and the preflop/flop/turn tree on the GPU as well
+    (device_tree=True, one CUDA graph per iteration) or on the host through the reference's
+    upload / evaluate / download protocol (device_tree=False)."""
 
-    def __init__(self, flop, nthreads=0):
+    def __init__(self, flop, nthreads=0, device_tree=True):
         self.ptr = lib().pr_game_new(int(flop), int(nthreads))
         if not self.ptr:
             raise PokerLibError(f"pr_game_new failed (status {lib().pr_last_error()})")
+        self.set_device_tree(device_tree)
+
+    def set_device_tree(self, on):
+        return bool(lib().pr_game_set_device_tree(self.ptr, int(bool(on))))
 
     @property
     def num_rivers(self):

@@ -27,10 +27,10 @@ def golden():
     return dict(np.load(GOLDEN))
 
 
-@pytest.fixture(scope="module")
-def game():
+@pytest.fixture(scope="module", params=[True, False], ids=["device_tree", "host_tree"])
+def game(request):
     import pokerrust_b200 as P
-    g = P.Game(O.REFERENCE_FLOP)
+    g = P.Game(O.REFERENCE_FLOP, device_tree=request.param)
     yield g
     g.close()
 
@@ -104,3 +104,30 @@ def test_checkpoint_round_trip(tmp_path):
         b.load(path)
     a.close()
     b.close()
+
+
+def test_device_tree_matches_host_tree_bit_for_bit():
+    """The device sweeps round every product like the host traversal and sum in the same
+    order, so two iterations with average sums give identical regrets, sums and
+    exploitability on both paths."""
+    import pokerrust_b200 as P
+    dev = P.Game(O.REFERENCE_FLOP, device_tree=True)
+    host = P.Game(O.REFERENCE_FLOP, device_tree=False)
+    for g in (dev, host):
+        g.enable_average()
+        g.iterate(2)
+    for a, b in zip(dev.regrets(), host.regrets()):
+        assert np.array_equal(a, b)
+    for a, b in zip(dev.average_sums(), host.average_sums()):
+        assert np.array_equal(a, b)
+    assert dev.exploitability(fp64=False) == host.exploitability(fp64=False)
+    assert dev.exploitability(fp64=True) == host.exploitability(fp64=True)
+    # switching paths mid-run carries the state over
+    dev.set_device_tree(False)
+    host.set_device_tree(True)
+    dev.iterate(1)
+    host.iterate(1)
+    for a, b in zip(dev.regrets(), host.regrets()):
+        assert np.array_equal(a, b)
+    dev.close()
+    host.close()
