@@ -119,6 +119,14 @@ def cpu_sample(boards, bets, ranges, tables, nthreads, subgames):
     return subgames * NODES_PER_SUBGAME / dt, dt
 
 
+def sized_sample(boards, bets, ranges, tables, nthreads, seconds):
+    """Number of roots whose oracle pass takes about `seconds` on these host threads, from a
+    timed probe of 4 roots per thread."""
+    probe = max(4 * nthreads, 32)
+    _, dt = cpu_sample(boards, bets, ranges, tables, nthreads, probe)
+    return int(min(len(boards), max(probe, probe * seconds / max(dt, 1e-6))))
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -136,7 +144,9 @@ def run_reference(args):
     boards, bets = game.river_roots()
     ranges = synthetic_ranges(O.card_order(), boards)
     tables = O.pack_flop_tables(O.REFERENCE_FLOP, nthreads)
-    sample = max(8 * nthreads, 64)
+    # each timed step is a bounded sample (about 10 s, less for long runs) of the pass
+    per_step = min(10.0, 150.0 / max(1, args.steps))
+    sample = sized_sample(boards, bets, ranges, tables, nthreads, per_step)
     for _ in range(args.warmup):
         cpu_sample(boards, bets, ranges, tables, nthreads, max(nthreads, 8))
     rates, times = [], []
@@ -277,7 +287,8 @@ def run_gpu(args):
         achieved = ab / (kernel_ms / 1e3) / 1e9
         cpu_threads = os.cpu_count() or 1
         tables_host = O.pack_flop_tables(O.REFERENCE_FLOP, cpu_threads)
-        cpu_rate, cpu_dt = cpu_sample(boards, bets, ranges, tables_host, cpu_threads, max(8 * cpu_threads, 64))
+        cpu_n = sized_sample(boards, bets, ranges, tables_host, cpu_threads, 10.0)
+        cpu_rate, cpu_dt = cpu_sample(boards, bets, ranges, tables_host, cpu_threads, cpu_n)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -295,7 +306,7 @@ def run_gpu(args):
                          "note": "algorithmic bytes per pass / kernel time; the pass is bound "
                                  "on-chip (shared memory and issue), not by HBM"},
             "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": cpu_threads, "kind": "port",
-                             "sample": f"{max(8 * cpu_threads, 64)} of {n} river subgames, one pass, "
+                             "sample": f"{cpu_n} of {n} river subgames, one pass, "
                                        f"{cpu_dt:.2f} s, scaled to nodes/s"},
             "gpu_launches": args.steps,
             "clocks": clk,
