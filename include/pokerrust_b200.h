@@ -178,6 +178,65 @@ int pr_game_get_average(void *game, float *upper, float *river);
 int pr_game_save(void *game, const char *path);
 int pr_game_load(void *game, const char *path);
 
+/* ---- batched general river subgames (extension; no reference counterpart) ----
+ * Many independent river subgames, each with its own 5-card board, pot, stack and bet tree,
+ * solved with per-hand regrets (CFR with regrets clipped at zero, the reference's update
+ * rule) by one persistent kernel fed from a device work queue; each CFR iteration is
+ * replayed as one CUDA graph. Tree rules: player 0 acts first; bets of 0.5 pot (sizes bit
+ * 0), 1 pot (bit 1) and all-in (bit 2), at most max_raises (1..3) bets and raises; a fold
+ * loses pot/2 plus the folder's river chips, a showdown moves pot/2 plus the river chips.
+ * Hands are colex indexes (1326; hands that touch the board are ignored). */
+typedef struct {
+    uint64_t board;     /* 5 cards, bit i = card i (13 * suit + rank) */
+    float pot;          /* chips in the pot before the river, pot/2 from each player */
+    float stack;        /* chips behind each player */
+    uint32_t sizes;     /* bet sizes enabled: bit 0 half pot, bit 1 pot, bit 2 all-in */
+    int32_t max_raises; /* bets + raises on the river, 1..3 */
+} pr_subgame;
+
+/* Builds one subgame's tree on the host (16-byte nodes in pre-order; nodes_out may be null,
+ * else room for 128 nodes). 0 on success, 2 if the spec is invalid. */
+int pr_batch_tree(const pr_subgame *spec, void *nodes_out, int *num_nodes, int *num_edges, int *num_leaves);
+/* ranges: [count][2][1326] floats (player 0, player 1). Null on failure. */
+void *pr_batch_new(const pr_subgame *specs, int count, const float *ranges);
+void pr_batch_free(void *batch);
+int pr_batch_count(void *batch);
+int pr_batch_shape(void *batch, int s, int *num_nodes, int *num_edges, int *num_leaves);
+int pr_batch_enable_average(void *batch);
+/* CFR iterations: player 0 update, then player 1. */
+int pr_batch_iterate(void *batch, int iterations);
+/* Per subgame: best-response sums of each player (range-weighted root values) and the
+ * exploitability (br0 + br1) / 2 per unit of joint range mass, in chips; against the
+ * current (use_average 0) or average strategies; fp64 = 1 in double precision. */
+int pr_batch_exploitability(void *batch, int use_average, int fp64, double *br0, double *br1, double *expl);
+/* Counterfactual values of `player` at the root ([count][1326], double) under the current or
+ * average strategies, and their range-weighted sums (the player's subgame value). */
+int pr_batch_root_values(void *batch, int player, int use_average, double *values, double *sums);
+/* Adjoint pair. Forward: the subgame value V = r0^T U(sigma) r1 (player 0's expected chips
+ * times the joint range mass) under the current or average strategies, double precision.
+ * Backward: dV/dr0 = player 0's counterfactual values, dV/dr1 = minus player 1's
+ * ([count][1326] each), and dV/dsigma(a, h) = r0(h) x value of root action a for hand h
+ * ([count][8][1326]; player 0 acts at the root). Reach vectors are recomputed in the
+ * backward pass, not stored per node. Null outputs are skipped. */
+int pr_batch_value(void *batch, int use_average, double *V);
+int pr_batch_value_grad(void *batch, int use_average, double *d_r0, double *d_r1, double *d_sigma);
+/* Replaces subgame s's ranges ([2][1326] floats). */
+int pr_batch_set_ranges(void *batch, int s, const float *r);
+/* Regrets / average sums of subgame s: [edges][1326] floats, edges in tree order. */
+int pr_batch_get_regrets(void *batch, int s, float *out);
+int pr_batch_set_regrets(void *batch, int s, const float *in);
+int pr_batch_get_average(void *batch, int s, float *out);
+int pr_batch_set_average(void *batch, int s, const float *in);
+/* Launch configuration per tree-shape class (0: up to 16 leaves, 1: more): hands per
+ * thread (2, 3, 4), resident CTAs per SM, queue order (0 most work first, 1 input order). */
+int pr_batch_config(void *batch, int c, int *K, int *per_sm, int *order, int *count);
+int pr_batch_set_config(void *batch, int c, int K, int per_sm, int order);
+/* Autotuner: times every configuration per class and keeps the fastest; the solver state
+ * is restored afterwards. ms_out[2]: the chosen per-pass times. */
+int pr_batch_tune(void *batch, double *ms_out);
+/* Algorithmic HBM bytes of one CFR iteration (roofline numerator). */
+double pr_batch_iteration_bytes(void *batch);
+
 #ifdef __cplusplus
 }
 #endif

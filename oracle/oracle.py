@@ -72,6 +72,22 @@ def load():
         L.or_game_iterate.argtypes = [vp]
         L.or_game_exploitability.argtypes = [vp, i32, vp, vp, vp]
         L.or_game_river_regrets.argtypes = [vp, vp]
+        L.or_bet_tree.restype = i32
+        L.or_bet_tree.argtypes = [f32, f32, ctypes.c_uint32, i32] + [vp] * 7 + [i32, vp, vp, vp]
+        L.or_sub_new.restype = vp
+        L.or_sub_new.argtypes = [u64, f32, f32, ctypes.c_uint32, i32, vp, vp]
+        L.or_sub_free.argtypes = [vp]
+        L.or_sub_edges.restype = i32
+        L.or_sub_edges.argtypes = [vp]
+        L.or_sub_get.argtypes = [vp, i32, vp]
+        L.or_sub_set.argtypes = [vp, i32, vp]
+        L.or_sub_cfr_half.argtypes = [vp, i32, i32]
+        L.or_sub_best_response.restype = ctypes.c_double
+        L.or_sub_best_response.argtypes = [vp, i32, i32, vp]
+        L.or_sub_value.restype = ctypes.c_double
+        L.or_sub_value.argtypes = [vp, i32, i32, vp]
+        L.or_sub_joint.restype = ctypes.c_double
+        L.or_sub_joint.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -215,3 +231,77 @@ class Game:
                 load().or_game_free(self.ptr)
         except Exception:
             pass
+
+
+# ---- general river subgames (the batch solver's rules) ----
+
+def bet_tree(pot, stack, sizes, max_raises, max_nodes=512):
+    """The subgame's tree in pre-order: dict of per-node arrays and counts."""
+    i = lambda: np.zeros(max_nodes, np.int32)
+    kind, actor, parent, in_edge, nchild, depth = i(), i(), i(), i(), i(), i()
+    stake = np.zeros(max_nodes, np.float32)
+    n, e, l = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    st = load().or_bet_tree(float(pot), float(stack), int(sizes), int(max_raises), _p(kind), _p(actor),
+                            _p(parent), _p(in_edge), _p(nchild), _p(stake), _p(depth), max_nodes,
+                            ctypes.byref(n), ctypes.byref(e), ctypes.byref(l))
+    if st:
+        raise ValueError(f"or_bet_tree failed ({st})")
+    k = n.value
+    return dict(kind=kind[:k], actor=actor[:k], parent=parent[:k], in_edge=in_edge[:k], nchild=nchild[:k],
+                stake=stake[:k], depth=depth[:k], num_edges=e.value, num_leaves=l.value)
+
+
+class Subgame:
+    """One general river subgame on the CPU: per-hand CFR in single precision, best
+    response and strategy evaluation in double precision (colex hand order)."""
+
+    def __init__(self, board, pot, stack, sizes, max_raises, r0, r1):
+        self._r = [np.ascontiguousarray(r0, np.float32), np.ascontiguousarray(r1, np.float32)]
+        self.ptr = load().or_sub_new(int(board), float(pot), float(stack), int(sizes), int(max_raises),
+                                     _p(self._r[0]), _p(self._r[1]))
+        if not self.ptr:
+            raise ValueError("bad subgame")
+        self.edges = load().or_sub_edges(self.ptr)
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            load().or_sub_free(self.ptr)
+            self.ptr = None
+
+    def _get(self, which):
+        out = np.zeros((self.edges, HANDS), np.float32)
+        load().or_sub_get(self.ptr, which, _p(out))
+        return out
+
+    def _set(self, which, v):
+        v = np.ascontiguousarray(v, np.float32).reshape(self.edges, HANDS)
+        load().or_sub_set(self.ptr, which, _p(v))
+
+    regrets = property(lambda self: self._get(0), lambda self, v: self._set(0, v))
+    average = property(lambda self: self._get(1), lambda self, v: self._set(1, v))
+
+    def cfr_half(self, player, accumulate=False):
+        load().or_sub_cfr_half(self.ptr, int(player), int(bool(accumulate)))
+
+    def iterate(self, n=1, accumulate=False):
+        for _ in range(n):
+            self.cfr_half(0, accumulate)
+            self.cfr_half(1, accumulate)
+
+    def best_response(self, player, use_average=False):
+        root = np.zeros(HANDS, np.float64)
+        s = load().or_sub_best_response(self.ptr, int(player), int(bool(use_average)), _p(root))
+        return s, root
+
+    def value(self, player, use_average=False):
+        root = np.zeros(HANDS, np.float64)
+        s = load().or_sub_value(self.ptr, int(player), int(bool(use_average)), _p(root))
+        return s, root
+
+    def joint(self):
+        return load().or_sub_joint(self.ptr)
+
+    def exploitability(self, use_average=False):
+        b0, _ = self.best_response(0, use_average)
+        b1, _ = self.best_response(1, use_average)
+        return b0, b1, (b0 + b1) / 2.0 / self.joint()

@@ -7,9 +7,13 @@ The CUDA library sits behind the reference's C ABI (include/pokerrust_b200.h);
 from .interface import (  # noqa: F401
     HANDS,
     RANGE_STRIDE,
+    SPEC_DTYPE,
+    Batch,
     Builder,
     Game,
     PokerLibError,
+    bet_tree,
+    random_subgames,
     build_flop_tables,
     build_river,
     card_order,

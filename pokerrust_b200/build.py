@@ -9,7 +9,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 SO_PATH = os.path.join(LIB_DIR, "libpokerrust_b200.so")
 A_PATH = os.path.join(LIB_DIR, "libpoker.a")
-SOURCES = ["abi.cu", "river_cfr.cu", "pack_boards.cu", "gen_tables.cu", "game.cu", "upper_tree.cu"]
+SOURCES = ["abi.cu", "river_cfr.cu", "pack_boards.cu", "gen_tables.cu", "game.cu", "upper_tree.cu",
+           "batch_solver.cu", "batch_api.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",

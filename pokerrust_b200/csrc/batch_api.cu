@@ -1,0 +1,683 @@
+// C ABI of the batched general-subgame solver (pr_batch_*; no reference counterpart): batch
+// construction, CFR iterations replayed as a CUDA graph, per-subgame exploitability in
+// single or double precision, strategy evaluation (root values), regret / average access
+// and the autotuner that picks the launch configuration per tree-shape class.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "../../include/pokerrust_b200.h"
+#include "batch_solver.h"
+#include "device_common.cuh"
+
+namespace prb {
+namespace {
+
+int bfail(const char *what, cudaError_t e = cudaSuccess) {
+    if (e != cudaSuccess) fprintf(stderr, "pokerrust_b200: batch: %s: %s\n", what, cudaGetErrorString(e));
+    else fprintf(stderr, "pokerrust_b200: batch: %s\n", what);
+    fflush(stderr);
+    return e != cudaSuccess ? 1 : 2;
+}
+
+// Launch configuration of one tree-shape class.
+struct ClassCfg {
+    int first = 0, count = 0;  // slice of the work queue
+    int max_leaves = 0;
+    int K = 2;                 // hands per thread
+    int per_sm = 1;            // resident CTAs per SM
+    int order = 0;             // 0: most work first, 1: input order
+};
+
+constexpr int kClasses = 2;    // trees with <= 16 leaves / more
+
+struct Batch {
+    int count = 0;
+    std::vector<pr_subgame> specs;
+    std::vector<BSub> subs;
+    std::vector<BNode> nodes;
+    std::vector<double> joint;  // sum over clash-free hand pairs of r0(h) r1(o)
+    std::vector<float> ranges0; // [count][1326] player 0's ranges (for the root adjoint)
+    int total_edges = 0;
+    int sms = 148;
+    ClassCfg cls[kClasses];
+    bool avg_on = false;
+    bool tuned = false;
+    cudaStream_t stream = nullptr;
+    BSub *d_subs = nullptr;
+    BNode *d_nodes = nullptr;
+    BPack *d_packs = nullptr;
+    float *d_ranges = nullptr;
+    float *d_regrets = nullptr, *d_avg = nullptr;
+    int *d_order = nullptr, *d_head = nullptr, *d_err = nullptr;
+    void *d_sum = nullptr;   // [count] doubles
+    void *d_root = nullptr;  // [count][kBRow] doubles, lazily
+    void *d_child = nullptr; // [count][8][kBRow] doubles, lazily
+    std::vector<uint16_t> hand;  // [count][kBRow] colex hand of each position
+    cudaGraphExec_t graph = nullptr;
+    bool graph_avg = false, graph_failed = false;
+
+    ~Batch() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *p : {(void *)d_subs, (void *)d_nodes, (void *)d_packs, (void *)d_ranges, (void *)d_regrets,
+                        (void *)d_avg, (void *)d_order, (void *)d_head, (void *)d_err, d_sum, d_root, d_child})
+            cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    // the order of the work queue: per class, most work first or input order
+    void build_order(std::vector<int> &order) const {
+        order.clear();
+        for (int c = 0; c < kClasses; c++) {
+            std::vector<int> ids;
+            for (int s = 0; s < count; s++)
+                if ((subs[s].num_leaves > batch_group_leaves(0)) == (c == 1)) ids.push_back(s);
+            if (cls[c].order == 0)
+                std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) {
+                    const long wa = (long)subs[a].num_edges * 4 + subs[a].num_leaves;
+                    const long wb = (long)subs[b].num_edges * 4 + subs[b].num_leaves;
+                    return wa > wb;
+                });
+            order.insert(order.end(), ids.begin(), ids.end());
+        }
+    }
+
+    int upload_order() {
+        std::vector<int> order;
+        build_order(order);
+        cudaError_t e = cudaMemcpy(d_order, order.data(), sizeof(int) * count, cudaMemcpyHostToDevice);
+        return e == cudaSuccess ? 0 : bfail("queue upload", e);
+    }
+
+    // one pass of `mode` for `player` over every class; heads [slot*kClasses + c] must be zero
+    int pass(int mode, int player, int fp64, int use_average, void *root_out, void *sum_out, int slot,
+             void *child_out = nullptr) {
+        for (int c = 0; c < kClasses; c++) {
+            const ClassCfg &k = cls[c];
+            if (!k.count) continue;
+            BLaunch a{};
+            a.subs = d_subs;
+            a.nodes = d_nodes;
+            a.packs = d_packs;
+            a.ranges = d_ranges;
+            a.regrets = d_regrets;
+            a.avg = (avg_on || use_average) ? d_avg : nullptr;
+            a.order = d_order + k.first;
+            a.head = d_head + slot * kClasses + c;
+            a.count = k.count;
+            a.player = player;
+            a.use_average = use_average;
+            a.root_out = root_out;
+            a.sum_out = sum_out;
+            a.child_out = child_out;
+            const int ctas = std::min(k.count, std::max(1, k.per_sm) * sms);
+            const int group = batch_group_leaves(fp64);
+            cudaError_t e = launch_batch_pass(mode, k.K, fp64, mode == kBModeCFR && avg_on, a, ctas, group, stream);
+            if (e != cudaSuccess) return bfail("pass launch", e);
+        }
+        return 0;
+    }
+
+    int iteration() {
+        cudaError_t e = cudaMemsetAsync(d_head, 0, sizeof(int) * 4 * kClasses, stream);
+        if (e != cudaSuccess) return bfail("queue reset", e);
+        for (int pl = 0; pl < 2; pl++)
+            if (int st = pass(kBModeCFR, pl, 0, 0, nullptr, nullptr, pl)) return st;
+        return 0;
+    }
+};
+
+}  // namespace
+}  // namespace prb
+
+using namespace prb;
+
+extern "C" {
+
+int pr_batch_tree(const pr_subgame *spec, void *nodes_out, int *num_nodes, int *num_edges, int *num_leaves) {
+    if (!spec) return 2;
+    BTree t;
+    if (spec->max_raises < 1 || spec->max_raises > 3) return 2;
+    if (!build_bet_tree(spec->pot, spec->stack, spec->sizes, spec->max_raises, &t) || t.depth >= 6) return 2;
+    if (nodes_out) memcpy(nodes_out, t.nodes.data(), t.nodes.size() * sizeof(BNode));
+    if (num_nodes) *num_nodes = (int)t.nodes.size();
+    if (num_edges) *num_edges = t.num_edges;
+    if (num_leaves) *num_leaves = t.num_leaves;
+    return 0;
+}
+
+void *pr_batch_new(const pr_subgame *specs, int count, const float *ranges) {
+    if (!specs || count <= 0 || !ranges) {
+        bfail("pr_batch_new: bad arguments");
+        return nullptr;
+    }
+    Batch *b = new Batch();
+    b->count = count;
+    b->specs.assign(specs, specs + count);
+    b->subs.resize(count);
+    b->joint.resize(count);
+    int edges = 0;
+    for (int s = 0; s < count; s++) {
+        const pr_subgame &sp = specs[s];
+        BTree t;
+        if (__builtin_popcountll(sp.board) != 5 || (sp.board >> 52) || sp.max_raises < 1 || sp.max_raises > 3 ||
+            !build_bet_tree(sp.pot, sp.stack, sp.sizes, sp.max_raises, &t) || t.depth >= 6) {
+            fprintf(stderr, "pokerrust_b200: batch: subgame %d has a bad board or bet tree\n", s);
+            delete b;
+            return nullptr;
+        }
+        BSub &d = b->subs[s];
+        d.board = sp.board;
+        d.node_off = (int)b->nodes.size();
+        d.num_nodes = (int)t.nodes.size();
+        d.edge_off = edges;
+        d.num_edges = t.num_edges;
+        d.num_leaves = t.num_leaves;
+        d.pot = sp.pot;
+        b->nodes.insert(b->nodes.end(), t.nodes.begin(), t.nodes.end());
+        edges += t.num_edges;
+        // joint mass of clash-free hand pairs (double)
+        const float *r0 = ranges + (size_t)s * 2 * 1326, *r1 = r0 + 1326;
+        double tot = 0, card[52] = {0};
+        for (int h = 0; h < 1326; h++) {
+            int c1, c2;
+            hand_cards(h, &c1, &c2);
+            if (((1ull << c1) | (1ull << c2)) & sp.board) continue;
+            tot += r1[h];
+            card[c1] += r1[h];
+            card[c2] += r1[h];
+        }
+        double j = 0;
+        for (int h = 0; h < 1326; h++) {
+            int c1, c2;
+            hand_cards(h, &c1, &c2);
+            if (((1ull << c1) | (1ull << c2)) & sp.board) continue;
+            j += (double)r0[h] * (tot - card[c1] - card[c2] + r1[h]);
+        }
+        b->joint[s] = j;
+    }
+    b->total_edges = edges;
+    b->ranges0.resize((size_t)count * 1326);
+    for (int s = 0; s < count; s++)
+        memcpy(b->ranges0.data() + (size_t)s * 1326, ranges + (size_t)s * 2 * 1326, sizeof(float) * 1326);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    // shape classes
+    int first = 0;
+    for (int c = 0; c < kClasses; c++) {
+        b->cls[c].first = first;
+        b->cls[c].count = 0;
+        for (int s = 0; s < count; s++)
+            if ((b->subs[s].num_leaves > batch_group_leaves(0)) == (c == 1)) {
+                b->cls[c].count++;
+                b->cls[c].max_leaves = std::max(b->cls[c].max_leaves, b->subs[s].num_leaves);
+            }
+        first += b->cls[c].count;
+    }
+    cudaError_t e;
+    const size_t rows = (size_t)edges * kBRow * sizeof(float);
+    float *d_in = nullptr;
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_subs, sizeof(BSub) * count)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_nodes, sizeof(BNode) * b->nodes.size())) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_packs, sizeof(BPack) * count)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_ranges, sizeof(float) * 2 * kBRow * count)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_regrets, rows)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_order, sizeof(int) * count)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_head, sizeof(int) * 4 * kClasses)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_err, sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_sum, sizeof(double) * count)) != cudaSuccess ||
+        (e = cudaMalloc(&d_in, sizeof(float) * 2 * 1326 * count)) != cudaSuccess) {
+        bfail("allocation", e);
+        cudaFree(d_in);
+        delete b;
+        return nullptr;
+    }
+    int err = 0;
+    if ((e = cudaMemcpy(b->d_subs, b->subs.data(), sizeof(BSub) * count, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(b->d_nodes, b->nodes.data(), sizeof(BNode) * b->nodes.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(d_in, ranges, sizeof(float) * 2 * 1326 * count, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemset(b->d_regrets, 0, rows)) != cudaSuccess ||
+        (e = cudaMemset(b->d_err, 0, sizeof(int))) != cudaSuccess ||
+        (e = launch_batch_setup(b->d_subs, count, b->d_packs, d_in, b->d_ranges, b->d_err, b->stream)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(b->stream)) != cudaSuccess ||
+        (e = cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+        bfail("setup", e);
+        cudaFree(d_in);
+        delete b;
+        return nullptr;
+    }
+    cudaFree(d_in);
+    if (err) {
+        bfail("setup found an inconsistent board");
+        delete b;
+        return nullptr;
+    }
+    b->hand.resize((size_t)count * kBRow);
+    for (int s = 0; s < count; s++) {
+        e = cudaMemcpy(b->hand.data() + (size_t)s * kBRow, (const char *)(b->d_packs + s) + offsetof(BPack, hand),
+                       sizeof(uint16_t) * kBRow, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            bfail("pack download", e);
+            delete b;
+            return nullptr;
+        }
+    }
+    if (b->upload_order()) {
+        delete b;
+        return nullptr;
+    }
+    return b;
+}
+
+void pr_batch_free(void *batch) { delete (Batch *)batch; }
+
+int pr_batch_count(void *batch) { return batch ? ((Batch *)batch)->count : 0; }
+
+int pr_batch_shape(void *batch, int s, int *num_nodes, int *num_edges, int *num_leaves) {
+    Batch *b = (Batch *)batch;
+    if (!b || s < 0 || s >= b->count) return 2;
+    if (num_nodes) *num_nodes = b->subs[s].num_nodes;
+    if (num_edges) *num_edges = b->subs[s].num_edges;
+    if (num_leaves) *num_leaves = b->subs[s].num_leaves;
+    return 0;
+}
+
+int pr_batch_enable_average(void *batch) {
+    Batch *b = (Batch *)batch;
+    if (!b) return 2;
+    if (b->avg_on) return 0;
+    const size_t rows = (size_t)b->total_edges * kBRow * sizeof(float);
+    cudaError_t e;
+    if ((e = cudaMalloc(&b->d_avg, rows)) != cudaSuccess || (e = cudaMemset(b->d_avg, 0, rows)) != cudaSuccess)
+        return bfail("average-strategy allocation", e);
+    b->avg_on = true;
+    return 0;
+}
+
+int pr_batch_iterate(void *batch, int iterations) {
+    Batch *b = (Batch *)batch;
+    if (!b || iterations < 0) return 2;
+    if (b->graph && b->graph_avg != b->avg_on) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    int it = 0;
+    if (!b->graph && !b->graph_failed && iterations > 0) {
+        if (int st = b->iteration()) return st;
+        it++;
+        cudaError_t e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) return bfail("iteration", e);
+        cudaGraph_t g = nullptr;
+        int st = 0;
+        e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            st = b->iteration();
+            e = cudaStreamEndCapture(b->stream, &g);
+        }
+        if (e == cudaSuccess && !st && g) e = cudaGraphInstantiate(&b->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess || st || !b->graph) {
+            cudaGetLastError();
+            b->graph = nullptr;
+            b->graph_failed = true;
+        }
+        b->graph_avg = b->avg_on;
+    }
+    for (; it < iterations; it++) {
+        if (b->graph) {
+            cudaError_t e = cudaGraphLaunch(b->graph, b->stream);
+            if (e != cudaSuccess) return bfail("graph launch", e);
+        } else if (int st = b->iteration()) {
+            return st;
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? 0 : bfail("iteration", e);
+}
+
+// Best-response sums of both players per subgame, and exploitability = (BR0 + BR1) / 2 per
+// unit of joint range mass, in chips.
+int pr_batch_exploitability(void *batch, int use_average, int fp64, double *br0, double *br1, double *expl) {
+    Batch *b = (Batch *)batch;
+    if (!b || (use_average && !b->avg_on)) return 2;
+    std::vector<double> sums[2];
+    std::vector<float> sumsf(b->count);
+    cudaError_t e = cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
+    if (e != cudaSuccess) return bfail("queue reset", e);
+    for (int pl = 0; pl < 2; pl++) {
+        sums[pl].resize(b->count);
+        if (int st = b->pass(kBModeBR, pl, fp64, use_average, nullptr, b->d_sum, 2 + pl)) return st;
+        if (fp64) {
+            e = cudaMemcpyAsync(sums[pl].data(), b->d_sum, sizeof(double) * b->count, cudaMemcpyDeviceToHost, b->stream);
+        } else {
+            e = cudaMemcpyAsync(sumsf.data(), b->d_sum, sizeof(float) * b->count, cudaMemcpyDeviceToHost, b->stream);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) return bfail("best response", e);
+        if (!fp64)
+            for (int s = 0; s < b->count; s++) sums[pl][s] = sumsf[s];
+    }
+    for (int s = 0; s < b->count; s++) {
+        if (br0) br0[s] = sums[0][s];
+        if (br1) br1[s] = sums[1][s];
+        if (expl) expl[s] = (sums[0][s] + sums[1][s]) / 2.0 / b->joint[s];
+    }
+    return 0;
+}
+
+// Root values (counterfactual values of `player` at the root, per colex hand; blocked hands
+// 0) under the current or average strategies, in double precision, and their
+// range-weighted sums (the subgame value for that player).
+int pr_batch_root_values(void *batch, int player, int use_average, double *values, double *sums) {
+    Batch *b = (Batch *)batch;
+    if (!b || (player != 0 && player != 1) || (use_average && !b->avg_on)) return 2;
+    cudaError_t e;
+    if (!b->d_root && (e = cudaMalloc(&b->d_root, sizeof(double) * kBRow * b->count)) != cudaSuccess)
+        return bfail("root value allocation", e);
+    e = cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
+    if (e != cudaSuccess) return bfail("queue reset", e);
+    if (int st = b->pass(kBModeEval, player, 1, use_average, b->d_root, b->d_sum, 3)) return st;
+    std::vector<double> rv((size_t)kBRow * b->count);
+    e = cudaMemcpyAsync(rv.data(), b->d_root, sizeof(double) * rv.size(), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess && sums)
+        e = cudaMemcpyAsync(sums, b->d_sum, sizeof(double) * b->count, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bfail("evaluation", e);
+    if (values) {
+        for (int s = 0; s < b->count; s++) {
+            double *out = values + (size_t)s * 1326;
+            for (int h = 0; h < 1326; h++) out[h] = 0.0;
+            for (int p = 0; p < kBLive; p++) out[b->hand[(size_t)s * kBRow + p]] = rv[(size_t)s * kBRow + p];
+        }
+    }
+    return 0;
+}
+
+// Subgame value V = r0^T U(sigma) r1 = sum_h r0(h) cfv0(h): player 0's expected chips times
+// the joint range mass, under the current or average strategies (double precision).
+int pr_batch_value(void *batch, int use_average, double *V) {
+    Batch *b = (Batch *)batch;
+    if (!b || !V || (use_average && !b->avg_on)) return 2;
+    cudaError_t e = cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
+    if (e != cudaSuccess) return bfail("queue reset", e);
+    if (int st = b->pass(kBModeEval, 0, 1, use_average, nullptr, b->d_sum, 0)) return st;
+    e = cudaMemcpyAsync(V, b->d_sum, sizeof(double) * b->count, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? 0 : bfail("value", e);
+}
+
+// Adjoint of pr_batch_value: dV/dr0 = cfv0 and dV/dr1 = -cfv1 per colex hand ([count][1326]),
+// and dV/dsigma(a, h) = r0(h) cfv0(child a, h) for the root's actions (player 0 acts at the
+// root; [count][8][1326], rows past the root's action count are zero). Two evaluation
+// passes; reach vectors are recomputed from the strategies, not stored per node.
+int pr_batch_value_grad(void *batch, int use_average, double *d_r0, double *d_r1, double *d_sigma) {
+    Batch *b = (Batch *)batch;
+    if (!b || (use_average && !b->avg_on)) return 2;
+    cudaError_t e;
+    if (!b->d_root && (e = cudaMalloc(&b->d_root, sizeof(double) * kBRow * b->count)) != cudaSuccess)
+        return bfail("root value allocation", e);
+    if (!b->d_child && (e = cudaMalloc(&b->d_child, sizeof(double) * 8 * kBRow * b->count)) != cudaSuccess)
+        return bfail("root value allocation", e);
+    std::vector<double> rv((size_t)kBRow * b->count), cv;
+    for (int pl = 0; pl < 2; pl++) {
+        e = cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
+        if (e == cudaSuccess && pl == 0) e = cudaMemsetAsync(b->d_child, 0, sizeof(double) * 8 * kBRow * b->count, b->stream);
+        if (e != cudaSuccess) return bfail("queue reset", e);
+        if (int st = b->pass(kBModeEval, pl, 1, use_average, b->d_root, nullptr, 0, pl == 0 ? b->d_child : nullptr))
+            return st;
+        e = cudaMemcpyAsync(rv.data(), b->d_root, sizeof(double) * rv.size(), cudaMemcpyDeviceToHost, b->stream);
+        if (e == cudaSuccess && pl == 0 && d_sigma) {
+            cv.resize((size_t)8 * kBRow * b->count);
+            e = cudaMemcpyAsync(cv.data(), b->d_child, sizeof(double) * cv.size(), cudaMemcpyDeviceToHost, b->stream);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) return bfail("adjoint", e);
+        double *out = pl == 0 ? d_r0 : d_r1;
+        for (int s = 0; s < b->count && out; s++) {
+            double *o = out + (size_t)s * 1326;
+            for (int h = 0; h < 1326; h++) o[h] = 0.0;
+            for (int p = 0; p < kBLive; p++)
+                o[b->hand[(size_t)s * kBRow + p]] = (pl == 0 ? 1.0 : -1.0) * rv[(size_t)s * kBRow + p];
+        }
+        if (pl == 0 && d_sigma) {
+            for (int s = 0; s < b->count; s++) {
+                const float *r0 = b->ranges0.data() + (size_t)s * 1326;
+                for (int a = 0; a < 8; a++) {
+                    double *o = d_sigma + ((size_t)s * 8 + a) * 1326;
+                    for (int h = 0; h < 1326; h++) o[h] = 0.0;
+                    if (a >= b->nodes[b->subs[s].node_off].nchild) continue;
+                    for (int p = 0; p < kBLive; p++) {
+                        const int h = b->hand[(size_t)s * kBRow + p];
+                        o[h] = (double)r0[h] * cv[((size_t)s * 8 + a) * kBRow + p];
+                    }
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+// Replaces the ranges of subgame s ([2][1326] floats, colex order).
+int pr_batch_set_ranges(void *batch, int s, const float *r) {
+    Batch *b = (Batch *)batch;
+    if (!b || s < 0 || s >= b->count || !r) return 2;
+    std::vector<float> rows(2 * kBRow, 0.0f);
+    const uint16_t *hand = b->hand.data() + (size_t)s * kBRow;
+    for (int pl = 0; pl < 2; pl++)
+        for (int p = 0; p < kBLive; p++) rows[pl * kBRow + p] = r[pl * 1326 + hand[p]];
+    memcpy(b->ranges0.data() + (size_t)s * 1326, r, sizeof(float) * 1326);
+    cudaStreamSynchronize(b->stream);
+    cudaError_t e = cudaMemcpy(b->d_ranges + (size_t)s * 2 * kBRow, rows.data(), sizeof(float) * 2 * kBRow,
+                               cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return bfail("range upload", e);
+    // joint mass of clash-free pairs
+    const float *r0 = r, *r1 = r + 1326;
+    const uint64_t board = b->subs[s].board;
+    double tot = 0, card[52] = {0};
+    for (int h = 0; h < 1326; h++) {
+        int c1, c2;
+        hand_cards(h, &c1, &c2);
+        if (((1ull << c1) | (1ull << c2)) & board) continue;
+        tot += r1[h];
+        card[c1] += r1[h];
+        card[c2] += r1[h];
+    }
+    double j = 0;
+    for (int h = 0; h < 1326; h++) {
+        int c1, c2;
+        hand_cards(h, &c1, &c2);
+        if (((1ull << c1) | (1ull << c2)) & board) continue;
+        j += (double)r0[h] * (tot - card[c1] - card[c2] + r1[h]);
+    }
+    b->joint[s] = j;
+    return 0;
+}
+
+namespace {
+// device rows [edge][kBRow] (position order) <-> host rows [edge][1326] (colex order)
+int rows_io(Batch *b, float *dev, int s, float *host, bool to_host) {
+    const BSub &d = b->subs[s];
+    std::vector<float> buf((size_t)d.num_edges * kBRow);
+    float *src = dev + (size_t)d.edge_off * kBRow;
+    cudaError_t e = cudaSuccess;
+    const uint16_t *hand = b->hand.data() + (size_t)s * kBRow;
+    if (to_host) {
+        e = cudaMemcpy(buf.data(), src, sizeof(float) * buf.size(), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return bfail("row download", e);
+        for (int k = 0; k < d.num_edges; k++) {
+            float *o = host + (size_t)k * 1326;
+            for (int h = 0; h < 1326; h++) o[h] = 0.0f;
+            for (int p = 0; p < kBLive; p++) o[hand[p]] = buf[(size_t)k * kBRow + p];
+        }
+    } else {
+        for (int k = 0; k < d.num_edges; k++)
+            for (int p = 0; p < kBRow; p++)
+                buf[(size_t)k * kBRow + p] = p < kBLive ? host[(size_t)k * 1326 + hand[p]] : 0.0f;
+        e = cudaMemcpy(src, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return bfail("row upload", e);
+    }
+    return 0;
+}
+}  // namespace
+
+int pr_batch_get_regrets(void *batch, int s, float *out) {
+    Batch *b = (Batch *)batch;
+    if (!b || s < 0 || s >= b->count || !out) return 2;
+    cudaStreamSynchronize(b->stream);
+    return rows_io(b, b->d_regrets, s, out, true);
+}
+
+int pr_batch_set_regrets(void *batch, int s, const float *in) {
+    Batch *b = (Batch *)batch;
+    if (!b || s < 0 || s >= b->count || !in) return 2;
+    cudaStreamSynchronize(b->stream);
+    return rows_io(b, b->d_regrets, s, const_cast<float *>(in), false);
+}
+
+int pr_batch_get_average(void *batch, int s, float *out) {
+    Batch *b = (Batch *)batch;
+    if (!b || !b->avg_on || s < 0 || s >= b->count || !out) return 2;
+    cudaStreamSynchronize(b->stream);
+    return rows_io(b, b->d_avg, s, out, true);
+}
+
+int pr_batch_set_average(void *batch, int s, const float *in) {
+    Batch *b = (Batch *)batch;
+    if (!b || !b->avg_on || s < 0 || s >= b->count || !in) return 2;
+    cudaStreamSynchronize(b->stream);
+    return rows_io(b, b->d_avg, s, const_cast<float *>(in), false);
+}
+
+// Configuration of class c: hands per thread, resident CTAs per SM, queue order.
+int pr_batch_config(void *batch, int c, int *K, int *per_sm, int *order, int *count) {
+    Batch *b = (Batch *)batch;
+    if (!b || c < 0 || c >= kClasses) return 2;
+    if (K) *K = b->cls[c].K;
+    if (per_sm) *per_sm = b->cls[c].per_sm;
+    if (order) *order = b->cls[c].order;
+    if (count) *count = b->cls[c].count;
+    return 0;
+}
+
+int pr_batch_set_config(void *batch, int c, int K, int per_sm, int order) {
+    Batch *b = (Batch *)batch;
+    if (!b || c < 0 || c >= kClasses || (K != 2 && K != 3 && K != 4) || per_sm < 1 || per_sm > 4 ||
+        (order != 0 && order != 1))
+        return 2;
+    const int fits = batch_ctas_per_sm(kBModeCFR, K, 0, b->avg_on);
+    if (per_sm > fits) return 2;
+    b->cls[c].K = K;
+    b->cls[c].per_sm = per_sm;
+    b->cls[c].order = order;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return b->upload_order();
+}
+
+// Autotuner: for each shape class, times one CFR pass of every configuration (hands per
+// thread 2/3/4, resident CTAs per SM up to what fits, queue order) on a copy of the
+// current regrets and keeps the fastest; the regrets and sums are restored afterwards, so
+// tuning does not change the solve. Writes the chosen class-0 / class-1 times (ms).
+int pr_batch_tune(void *batch, double *ms_out) {
+    Batch *b = (Batch *)batch;
+    if (!b) return 2;
+    const size_t rows = (size_t)b->total_edges * kBRow * sizeof(float);
+    float *save_r = nullptr, *save_a = nullptr;
+    cudaError_t e;
+    if ((e = cudaMalloc(&save_r, rows)) != cudaSuccess) return bfail("tuning allocation", e);
+    if (b->avg_on && (e = cudaMalloc(&save_a, rows)) != cudaSuccess) {
+        cudaFree(save_r);
+        return bfail("tuning allocation", e);
+    }
+    cudaMemcpyAsync(save_r, b->d_regrets, rows, cudaMemcpyDeviceToDevice, b->stream);
+    if (save_a) cudaMemcpyAsync(save_a, b->d_avg, rows, cudaMemcpyDeviceToDevice, b->stream);
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    int status = 0;
+    for (int c = 0; c < kClasses && !status; c++) {
+        if (!b->cls[c].count) {
+            if (ms_out) ms_out[c] = 0.0;
+            continue;
+        }
+        ClassCfg keep[kClasses];
+        for (int i = 0; i < kClasses; i++) keep[i] = b->cls[i];
+        for (int i = 0; i < kClasses; i++)
+            if (i != c) b->cls[i].count = 0;  // time this class alone
+        float best = 1e30f;
+        ClassCfg best_cfg = keep[c];
+        for (int K : {2, 3, 4}) {
+            const int fits = batch_ctas_per_sm(kBModeCFR, K, 0, b->avg_on);
+            for (int per = 1; per <= std::min(fits, 2); per++) {
+                for (int ord = 0; ord < 2; ord++) {
+                    b->cls[c].K = K;
+                    b->cls[c].per_sm = per;
+                    b->cls[c].order = ord;
+                    if ((status = b->upload_order())) break;
+                    float ms = 0;
+                    for (int rep = 0; rep < 3 && !status; rep++) {
+                        cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
+                        cudaEventRecord(t0, b->stream);
+                        status = b->pass(kBModeCFR, rep & 1, 0, 0, nullptr, nullptr, 0);
+                        cudaEventRecord(t1, b->stream);
+                        cudaEventSynchronize(t1);
+                        float t = 0;
+                        cudaEventElapsedTime(&t, t0, t1);
+                        if (rep > 0) ms += t;  // first run warms up
+                    }
+                    if (status) break;
+                    if (ms < best) {
+                        best = ms;
+                        best_cfg = b->cls[c];
+                    }
+                }
+                if (status) break;
+            }
+            if (status) break;
+        }
+        for (int i = 0; i < kClasses; i++) b->cls[i] = keep[i];
+        b->cls[c].K = best_cfg.K;
+        b->cls[c].per_sm = best_cfg.per_sm;
+        b->cls[c].order = best_cfg.order;
+        if (ms_out) ms_out[c] = best / 2.0;
+    }
+    if (!status) status = b->upload_order();
+    cudaMemcpyAsync(b->d_regrets, save_r, rows, cudaMemcpyDeviceToDevice, b->stream);
+    if (save_a) cudaMemcpyAsync(b->d_avg, save_a, rows, cudaMemcpyDeviceToDevice, b->stream);
+    e = cudaStreamSynchronize(b->stream);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaFree(save_r);
+    cudaFree(save_a);
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->tuned = true;
+    if (e != cudaSuccess) return bfail("tuning", e);
+    return status;
+}
+
+// Algorithmic HBM bytes of one CFR iteration (both players): per edge and hand, the
+// updater's regret read + write and average read + write, the other player's regret read
+// (20 B with averages, 12 B without), plus ranges in and the tables read per pass.
+double pr_batch_iteration_bytes(void *batch) {
+    Batch *b = (Batch *)batch;
+    if (!b) return 0;
+    const double per = b->avg_on ? 20.0 : 12.0;
+    return (double)b->total_edges * kBLive * per +
+           2.0 * b->count * (2.0 * kBRow * 4 + (double)sizeof(BPack) + 64.0);
+}
+
+}  // extern "C"

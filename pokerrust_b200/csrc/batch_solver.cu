@@ -1,0 +1,725 @@
+// Batched solver of general river subgames: per-hand CFR, best response and strategy
+// evaluation over many independent subgames in one persistent launch.
+//
+// A CTA takes subgames from a device work queue (atomicAdd on a head counter) until it is
+// empty. For one subgame, the 1081 live hands are held in rank order ("positions"); a
+// thread owns K consecutive positions. The bet tree (pre-order nodes) sits in shared
+// memory. A pass for player p walks the tree twice per thread, with all per-hand state of
+// the open path in registers:
+//  * top-down: reach of the opponent (times its range) and of p along the path, from
+//    regret matching (or the average strategy) of the acting player; at every leaf the
+//    opponent weights x(o) go to shared memory;
+//  * leaves: for each leaf a CTA-wide pass turns x into p's counterfactual values:
+//      showdown  stake * ([W - B] over all live hands - [W - B] over the hands holding each
+//                of p's two cards), W / B = weight of strictly worse / better hands, taken
+//                at the bounds of the hand's tie group (card removal by inclusion-exclusion);
+//      fold      +-stake * (T - C[c1] - C[c2] + x(h)), T the total and C the per-card sums.
+//    Prefix sums use a fixed summation tree (32-wide warp scans of fixed chunks and card
+//    lists), so results do not depend on the CTA size;
+//  * bottom-up: values flow to the root; at p's nodes the CFR pass updates regrets
+//    r <- max(r + v(child) - v(node), 0) (the child value is added when the child closes and
+//    the node value subtracted when the node closes, so no per-child storage is needed), the
+//    best response takes the maximum, the evaluation the strategy-weighted sum.
+// Leaves are processed in groups sized to shared memory; both walks advance group by group.
+// Average-strategy sums (avg += reach of p x action probability) are added in the top-down
+// walk of CFR passes.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "batch_solver.h"
+#include "device_common.cuh"
+#include "hand_eval.cuh"
+
+namespace prb {
+namespace {
+
+constexpr int kSetupThreads = 256;
+constexpr int DS = 6;  // stack depth: trees of depth <= 5 (max_raises <= 3)
+
+// ---------------------------------------------------------------- setup ----
+
+__global__ void __launch_bounds__(kSetupThreads) batch_setup_kernel(const BSub *__restrict__ subs,
+                                                                     BPack *__restrict__ packs,
+                                                                     const float *__restrict__ ranges_in,
+                                                                     float *__restrict__ ranges_pos,
+                                                                     int *__restrict__ err) {
+    const int s = blockIdx.x;
+    const int tid = threadIdx.x;
+    const unsigned long long board = subs[s].board;
+    BPack *pk = packs + s;
+    __shared__ unsigned long long key[2048];
+    __shared__ uint16_t hand_at[kBRow];
+    __shared__ uint16_t first[kBRow], last[kBRow];
+    __shared__ uint8_t lo_li[kBRow], hi_li[kBRow], lo_gs[kBRow], lo_ge[kBRow], hi_gs[kBRow], hi_ge[kBRow];
+    __shared__ uint8_t list_card[48];
+    __shared__ int8_t list_of_card[52];
+
+    if (__popcll(board) != 5 || (board >> 52)) {
+        if (tid == 0) atomicOr(err, 1);
+        return;
+    }
+    for (int i = tid; i < 2048; i += kSetupThreads) {
+        unsigned long long k = ~0ull;
+        if (i < 1326) {
+            int c1, c2;
+            hand_cards(i, &c1, &c2);
+            const unsigned long long hm = (1ull << c1) | (1ull << c2);
+            if (!(hm & board)) k = ((unsigned long long)(hand_value(hm | board) + 1u) << 11) | (unsigned)i;
+        }
+        key[i] = k;
+    }
+    // bitonic sort, ascending: weakest hand first, ties by hand index
+    for (int size = 2; size <= 2048; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            __syncthreads();
+            for (int t = tid; t < 1024; t += kSetupThreads) {
+                const int i = 2 * t - (t & (stride - 1));
+                const int j = i + stride;
+                const bool up = (i & size) == 0;
+                const unsigned long long a = key[i], b = key[j];
+                if ((a > b) == up) {
+                    key[i] = b;
+                    key[j] = a;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int p = tid; p < kBRow; p += kSetupThreads) hand_at[p] = p < kBLive ? (uint16_t)(key[p] & 2047) : 0xFFFF;
+    if (tid == 0) {
+        int n = 0;
+        for (int c = 0; c < 52; c++) {
+            list_of_card[c] = -1;
+            if (!((board >> c) & 1)) {
+                list_of_card[c] = (int8_t)n;
+                list_card[n++] = (uint8_t)c;
+            }
+        }
+        list_card[47] = 0;
+        // tie groups: equal hand values
+        int f = 0;
+        for (int p = 0; p < kBLive; p++) {
+            if (p > 0 && (key[p] >> 11) != (key[p - 1] >> 11)) f = p;
+            first[p] = (uint16_t)f;
+        }
+        int l = kBLive - 1;
+        for (int p = kBLive - 1; p >= 0; p--) {
+            if (p < kBLive - 1 && (key[p] >> 11) != (key[p + 1] >> 11)) l = p;
+            last[p] = (uint16_t)l;
+        }
+        for (int p = kBLive; p < kBRow; p++) first[p] = last[p] = (uint16_t)p;
+    }
+    __syncthreads();
+    if (tid < kBLists) {
+        // card list: live hands holding the card, in rank order, and each element's tie group
+        // bounds inside the list
+        const int li = tid;
+        const int card = list_card[li];
+        uint16_t pos[kBListLen];
+        int k = 0;
+        for (int p = 0; p < kBLive && k < kBListLen; p++) {
+            int c1, c2;
+            hand_cards(hand_at[p], &c1, &c2);
+            if (c1 == card || c2 == card) pos[k++] = (uint16_t)p;
+        }
+        if (k != kBListLen) atomicOr(err, 2);
+        for (int j = 0; j < 48; j++) pk->clpos[li][j] = j < k ? pos[j] : (uint16_t)(kBRow - 1);
+        int j = 0;
+        while (j < k) {
+            int e = j;
+            while (e + 1 < k && first[pos[e + 1]] == first[pos[j]]) e++;
+            for (int q = j; q <= e; q++) {
+                int c1, c2;
+                hand_cards(hand_at[pos[q]], &c1, &c2);
+                if (c1 == card) {
+                    lo_li[pos[q]] = (uint8_t)li;
+                    lo_gs[pos[q]] = (uint8_t)j;
+                    lo_ge[pos[q]] = (uint8_t)e;
+                } else {
+                    hi_li[pos[q]] = (uint8_t)li;
+                    hi_gs[pos[q]] = (uint8_t)j;
+                    hi_ge[pos[q]] = (uint8_t)e;
+                }
+            }
+            j = e + 1;
+        }
+    }
+    if (tid == kBLists) {
+        for (int c = 0; c < 48; c++) pk->list_card[c] = list_card[c];
+    }
+    __syncthreads();
+    for (int p = tid; p < kBRow; p += kSetupThreads) {
+        const bool live = p < kBLive;
+        pk->grp[p] = (uint32_t)first[p] | ((uint32_t)last[p] << 16);
+        pk->lists[p] = live ? ((uint32_t)lo_li[p] | ((uint32_t)hi_li[p] << 8) | ((uint32_t)lo_gs[p] << 16) |
+                               ((uint32_t)lo_ge[p] << 24))
+                            : 0u;
+        pk->lists2[p] = live ? ((uint32_t)hi_gs[p] | ((uint32_t)hi_ge[p] << 8)) : 0u;
+        pk->hand[p] = hand_at[p];
+    }
+    for (int h = tid; h < 1328; h += kSetupThreads) pk->pos_of[h] = 0xFFFF;
+    __syncthreads();
+    for (int p = tid; p < kBLive; p += kSetupThreads) pk->pos_of[hand_at[p]] = (uint16_t)p;
+    for (int i = tid; i < 2 * kBRow; i += kSetupThreads) {
+        const int pl = i / kBRow, p = i % kBRow;
+        ranges_pos[((size_t)s * 2 + pl) * kBRow + p] =
+            p < kBLive ? ranges_in[((size_t)s * 2 + pl) * 1326 + hand_at[p]] : 0.0f;
+    }
+}
+
+// ---------------------------------------------------------------- solver ----
+
+template <int K>
+struct Cfg {
+    static constexpr int NT = K == 2 ? 544 : (K == 3 ? 384 : 288);
+};
+
+// depth-indexed register stacks: every access is an unrolled select, so nothing spills to
+// local memory
+template <typename T, int N>
+__device__ __forceinline__ T sget(const T (&a)[N], int d) {
+    T v = a[0];
+#pragma unroll
+    for (int i = 1; i < N; i++)
+        if (i == d) v = a[i];
+    return v;
+}
+template <typename T, int N>
+__device__ __forceinline__ void sset(T (&a)[N], int d, T v) {
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        if (i == d) a[i] = v;
+}
+
+template <typename V>
+__device__ __forceinline__ V neg_inf();
+template <>
+__device__ __forceinline__ float neg_inf<float>() {
+    return -__int_as_float(0x7f800000);
+}
+template <>
+__device__ __forceinline__ double neg_inf<double>() {
+    return -__longlong_as_double(0x7ff0000000000000ll);
+}
+
+// products rounded on their own (no contraction into a following add)
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+
+template <typename V>
+struct Smem {
+    V *X;     // [group][kBRow] opponent weights, then leaf values
+    V *I;     // [2][kBRow] chunk-local inclusive scans
+    V *CT;    // [2][kBChunks] chunk totals
+    V *SC;    // [2][kBLists][48] inclusive scans of the card lists
+    BNode *tn;
+    uint16_t *leaf_node;
+    V *wsum;  // [32] warp partial sums
+};
+
+template <typename V>
+__host__ __device__ inline size_t smem_bytes(int group) {
+    size_t b = 0;
+    b += (size_t)group * kBRow * sizeof(V);
+    b += 2 * (size_t)kBRow * sizeof(V);
+    b += 2 * (size_t)kBChunks * sizeof(V);
+    b += 2 * (size_t)kBLists * 48 * sizeof(V);
+    b += (size_t)kBMaxNodes * sizeof(BNode);
+    b += (size_t)kBMaxLeaves * sizeof(uint16_t);
+    b += 32 * sizeof(V);
+    return (b + 15) & ~(size_t)15;
+}
+
+template <typename V>
+__device__ inline Smem<V> carve(unsigned char *base, int group) {
+    Smem<V> S;
+    V *v = reinterpret_cast<V *>(base);
+    S.X = v;
+    v += (size_t)group * kBRow;
+    S.I = v;
+    v += 2 * kBRow;
+    S.CT = v;
+    v += 2 * kBChunks;
+    S.SC = v;
+    v += 2 * kBLists * 48;
+    S.wsum = v;
+    v += 32;
+    S.tn = reinterpret_cast<BNode *>(v);
+    S.leaf_node = reinterpret_cast<uint16_t *>(S.tn + kBMaxNodes);
+    return S;
+}
+
+// Strategy of edge `e` at a node whose out-edges have positive-part sum `S`.
+template <typename V, bool USEAVG>
+__device__ __forceinline__ V sigma(V val, V S, int n) {
+    const V cut = USEAVG ? V(0) : V(1e-4f);
+    return S <= cut ? V(1) / V(n) : (val > V(0) ? val : V(0)) / S;
+}
+
+template <int K, typename V, int MODE, bool AVG, bool USEAVG>
+__global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int group) {
+    constexpr int NT = Cfg<K>::NT;
+    constexpr int NW = NT / 32;
+    static_assert(MODE == kBModeCFR || !AVG, "average sums accumulate in CFR passes");
+    static_assert(MODE != kBModeCFR || (sizeof(V) == 4 && !USEAVG), "CFR runs on regrets in single precision");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem<V> S = carve<V>(smem_raw, group);
+    __shared__ int s_next;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const unsigned FULL = 0xffffffffu;
+    const int p = a.player, o = 1 - p;
+    const float *src_all = USEAVG ? a.avg : a.regrets;
+
+    for (;;) {
+        if (tid == 0) s_next = atomicAdd(a.head, 1);
+        __syncthreads();
+        const int qi = s_next;
+        __syncthreads();
+        if (qi >= a.count) break;
+        const int s = a.order[qi];
+        const BSub sub = a.subs[s];
+        const BPack *__restrict__ pk = a.packs + s;
+        const int N = sub.num_nodes, L = sub.num_leaves;
+        for (int i = tid; i < N; i += NT) {
+            const BNode nd = a.nodes[sub.node_off + i];
+            S.tn[i] = nd;
+            if (nd.kind != kBDecision) S.leaf_node[nd.edge] = (uint16_t)i;
+        }
+        __syncthreads();
+        float *R = a.regrets + (size_t)sub.edge_off * kBRow;
+        float *A = a.avg ? a.avg + (size_t)sub.edge_off * kBRow : nullptr;
+        const float *Src = src_all + (size_t)sub.edge_off * kBRow;
+        const float *rng = a.ranges + (size_t)s * 2 * kBRow;
+        const int pos0 = tid * K;
+
+        // walker state, per owned hand: depth-indexed stacks of the open path
+        V po[K][DS], pp[K][DS], St[K][DS];   // top-down: opponent weight, own reach, strategy sums
+        V acc[K][DS], Sb[K][DS];             // bottom-up: node values, strategy sums
+        int open_id[DS];
+        int open_top = -1;
+        int td = 0, bu = 0;
+        V root[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) root[k] = V(0);
+
+        // closes the open nodes at depth >= d, passing each value to its parent
+        auto close_to = [&](int d) {
+            while (open_top >= d) {
+                const int m = sget(open_id, open_top);
+                const BNode nm = S.tn[m];
+                V v[K];
+#pragma unroll
+                for (int k = 0; k < K; k++) v[k] = sget(acc[k], open_top);
+                if (MODE == kBModeCFR && nm.actor == p) {
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        const int pos = pos0 + k;
+                        if (pos >= kBRow) continue;
+                        for (int e = 0; e < nm.nchild; e++) {
+                            float &r = R[(size_t)(nm.edge + e) * kBRow + pos];
+                            r = fmaxf(r - float(v[k]), 0.0f);
+                        }
+                    }
+                }
+                open_top--;
+                if (m == 0) {
+#pragma unroll
+                    for (int k = 0; k < K; k++) root[k] = v[k];
+                } else {
+                    // deliver to the parent (open at depth open_top)
+                    const BNode pq = S.tn[nm.parent];
+                    if (a.child_out && nm.parent == 0) {
+                        V *co = reinterpret_cast<V *>(a.child_out) + ((size_t)s * 8 + (nm.in_edge - pq.edge)) * kBRow;
+#pragma unroll
+                        for (int k = 0; k < K; k++)
+                            if (pos0 + k < kBRow) co[pos0 + k] = v[k];
+                    }
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        V ak = sget(acc[k], open_top);
+                        const int pos = pos0 + k;
+                        if (pq.actor == p) {
+                            if (MODE == kBModeBR) {
+                                ak = ak > v[k] ? ak : v[k];
+                            } else {
+                                const V sb = sget(Sb[k], open_top);
+                                V val = V(0);
+                                if (pos < kBRow) {
+                                    if (MODE == kBModeCFR) {
+                                        float &r = R[(size_t)nm.in_edge * kBRow + pos];
+                                        val = V(r);
+                                        r = r + float(v[k]);
+                                    } else {
+                                        val = V(Src[(size_t)nm.in_edge * kBRow + pos]);
+                                    }
+                                }
+                                ak = ak + mul(sigma<V, USEAVG>(val, sb, pq.nchild), v[k]);
+                            }
+                        } else {
+                            ak = ak + v[k];
+                        }
+                        sset(acc[k], open_top, ak);
+                    }
+                }
+            }
+        };
+        for (int g0 = 0; g0 < L; g0 += group) {
+            const int g1 = min(L, g0 + group);
+            const int end = g1 == L ? N : S.leaf_node[g1];
+            // ---- top-down walk over nodes [td, end) ----
+            for (; td < end; td++) {
+                const BNode nd = S.tn[td];
+                const int d = nd.depth;
+                V npo[K], npp[K];
+                if (td == 0) {
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        const int pos = pos0 + k;
+                        npo[k] = pos < kBRow ? V(rng[o * kBRow + pos]) : V(0);
+                        npp[k] = V(1);
+                    }
+                } else {
+                    const BNode pm = S.tn[nd.parent];
+                    const bool own = pm.actor == p;
+                    const bool need = !own || AVG;
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        const V po_par = sget(po[k], d - 1);
+                        const V pp_par = sget(pp[k], d - 1);
+                        V sg = V(1);
+                        if (need) {
+                            const int pos = pos0 + k;
+                            const V val = pos < kBRow ? V(Src[(size_t)nd.in_edge * kBRow + pos]) : V(0);
+                            sg = sigma<V, USEAVG>(val, sget(St[k], d - 1), pm.nchild);
+                        }
+                        if (own) {
+                            npo[k] = po_par;
+                            npp[k] = mul(pp_par, sg);
+                            if constexpr (AVG) {
+                                const int pos = pos0 + k;
+                                if (pos < kBRow) {
+                                    float &av = A[(size_t)nd.in_edge * kBRow + pos];
+                                    av += float(mul(pp_par, sg));
+                                }
+                            }
+                        } else {
+                            npo[k] = mul(po_par, sg);
+                            npp[k] = pp_par;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    sset(po[k], d, npo[k]);
+                    sset(pp[k], d, npp[k]);
+                }
+                if (nd.kind == kBDecision) {
+                    // strategy sums of the node, for its children
+                    const bool own = nd.actor == p;
+                    const bool need = !own || AVG;
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        V sum = V(0);
+                        if (need) {
+                            const int pos = pos0 + k;
+                            for (int e = 0; e < nd.nchild; e++) {
+                                const V val = pos < kBRow ? V(Src[(size_t)(nd.edge + e) * kBRow + pos]) : V(0);
+                                sum += val > V(0) ? val : V(0);
+                            }
+                        }
+                        sset(St[k], d, sum);
+                    }
+                } else {
+                    V *x = S.X + (size_t)(nd.edge - g0) * kBRow;
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        const int pos = pos0 + k;
+                        if (pos < kBRow) x[pos] = pos < kBLive ? npo[k] : V(0);
+                    }
+                }
+            }
+            __syncthreads();
+
+            // ---- leaves of the group: opponent weights -> p's values ----
+            for (int j = g0; j < g1; j++) {
+                const int buf = (j - g0) & 1;
+                V *x = S.X + (size_t)(j - g0) * kBRow;
+                V *I = S.I + buf * kBRow;
+                V *CT = S.CT + buf * kBChunks;
+                V *SC = S.SC + buf * kBLists * 48;
+                // phase A: chunk scans of the rank order and scans of the card lists
+                for (int u = warp; u < kBChunks + kBLists; u += NW) {
+                    if (u < kBChunks) {
+                        V v = x[u * 32 + lane];
+#pragma unroll
+                        for (int off = 1; off < 32; off <<= 1) {
+                            const V t = __shfl_up_sync(FULL, v, off);
+                            if (lane >= off) v += t;
+                        }
+                        I[u * 32 + lane] = v;
+                        if (lane == 31) CT[u] = v;
+                    } else {
+                        const int li = u - kBChunks;
+                        V a0 = V(0), a1 = V(0);
+                        if (lane < kBListLen / 2) {
+                            a0 = x[pk->clpos[li][2 * lane]];
+                            a1 = a0 + x[pk->clpos[li][2 * lane + 1]];
+                        }
+                        V v = a1;
+#pragma unroll
+                        for (int off = 1; off < 32; off <<= 1) {
+                            const V t = __shfl_up_sync(FULL, v, off);
+                            if (lane >= off) v += t;
+                        }
+                        V ex = __shfl_up_sync(FULL, v, 1);
+                        if (lane == 0) ex = V(0);
+                        if (lane < kBListLen / 2) {
+                            SC[li * 48 + 2 * lane] = ex + a0;
+                            SC[li * 48 + 2 * lane + 1] = v;
+                        }
+                    }
+                }
+                __syncthreads();
+                // phase C: chunk offsets (every warp, same arithmetic), then values
+                V c0 = V(0), c1 = V(0);
+                if (lane < kBChunks / 2) {
+                    c0 = CT[2 * lane];
+                    c1 = c0 + CT[2 * lane + 1];
+                }
+                V inc = c1;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const V t = __shfl_up_sync(FULL, inc, off);
+                    if (lane >= off) inc += t;
+                }
+                V ex = __shfl_up_sync(FULL, inc, 1);
+                if (lane == 0) ex = V(0);
+                const V off_even = ex, off_odd = ex + c0;
+                const V T = __shfl_sync(FULL, inc, kBChunks / 2 - 1);
+                const BNode ln = S.tn[S.leaf_node[j]];
+                const V stake = V(ln.stake);
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    const int pos = pos0 + k;
+                    const int pq = pos < kBRow ? pos : kBRow - 1;
+                    const uint32_t gr = __ldg(&pk->grp[pq]);
+                    const uint32_t l1 = __ldg(&pk->lists[pq]);
+                    const uint32_t l2 = __ldg(&pk->lists2[pq]);
+                    const int gs = gr & 0xFFFF, ge = gr >> 16;
+                    const int li1 = l1 & 255, li2 = (l1 >> 8) & 255;
+                    const int gs1 = (l1 >> 16) & 255, ge1 = l1 >> 24;
+                    const int gs2 = l2 & 255, ge2 = (l2 >> 8) & 255;
+                    // chunk offsets by shuffle (all lanes take part)
+                    const int ce = ge >> 5, cs = (gs - 1) >> 5;
+                    const V oe_e = __shfl_sync(FULL, off_even, ce >> 1);
+                    const V oe_o = __shfl_sync(FULL, off_odd, ce >> 1);
+                    const V os_e = __shfl_sync(FULL, off_even, (gs > 0 ? cs : 0) >> 1);
+                    const V os_o = __shfl_sync(FULL, off_odd, (gs > 0 ? cs : 0) >> 1);
+                    if (pos >= kBRow) continue;
+                    V val = V(0);
+                    if (pos < kBLive) {
+                        const V *sc1 = SC + li1 * 48;
+                        const V *sc2 = SC + li2 * 48;
+                        const V T1 = sc1[kBListLen - 1], T2 = sc2[kBListLen - 1];
+                        if (ln.kind == kBShowdown) {
+                            const V Pe = ((ce & 1) ? oe_o : oe_e) + I[ge];
+                            const V Ps = gs > 0 ? ((cs & 1) ? os_o : os_e) + I[gs - 1] : V(0);
+                            const V vg = (Pe + Ps) - T;
+                            const V v1 = (sc1[ge1] + (gs1 > 0 ? sc1[gs1 - 1] : V(0))) - T1;
+                            const V v2 = (sc2[ge2] + (gs2 > 0 ? sc2[gs2 - 1] : V(0))) - T2;
+                            val = mul(stake, (vg - v1) - v2);
+                        } else {
+                            const V free = ((T - T1) - T2) + x[pos];
+                            val = mul(ln.actor == p ? -stake : stake, free);
+                        }
+                    }
+                    x[pos] = val;
+                }
+            }
+            __syncthreads();
+
+            // ---- bottom-up walk over nodes [bu, end) ----
+            for (; bu < end; bu++) {
+                const BNode nd = S.tn[bu];
+                const int d = nd.depth;
+                close_to(d);
+                if (nd.kind == kBDecision) {
+                    open_top = d;
+                    sset(open_id, d, bu);
+                    const bool own = nd.actor == p;
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        sset(acc[k], d, (own && MODE == kBModeBR) ? neg_inf<V>() : V(0));
+                        V sum = V(0);
+                        if (own && MODE != kBModeBR) {
+                            const int pos = pos0 + k;
+                            for (int e = 0; e < nd.nchild; e++) {
+                                const V val = pos < kBRow ? V(Src[(size_t)(nd.edge + e) * kBRow + pos]) : V(0);
+                                sum += val > V(0) ? val : V(0);
+                            }
+                        }
+                        sset(Sb[k], d, sum);
+                    }
+                } else {
+                    // a leaf: its value goes straight to the parent (open at depth d - 1)
+                    const V *x = S.X + (size_t)(nd.edge - g0) * kBRow;
+                    const BNode pq = S.tn[nd.parent];
+                    if (a.child_out && nd.parent == 0) {
+                        V *co = reinterpret_cast<V *>(a.child_out) + ((size_t)s * 8 + (nd.in_edge - pq.edge)) * kBRow;
+#pragma unroll
+                        for (int k = 0; k < K; k++)
+                            if (pos0 + k < kBRow) co[pos0 + k] = x[pos0 + k];
+                    }
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        const int pos = pos0 + k;
+                        const V v = pos < kBRow ? x[pos] : V(0);
+                        V ak = sget(acc[k], d - 1);
+                        if (pq.actor == p) {
+                            if (MODE == kBModeBR) {
+                                ak = ak > v ? ak : v;
+                            } else {
+                                const V sb = sget(Sb[k], d - 1);
+                                V val = V(0);
+                                if (pos < kBRow) {
+                                    if (MODE == kBModeCFR) {
+                                        float &r = R[(size_t)nd.in_edge * kBRow + pos];
+                                        val = V(r);
+                                        r = r + float(v);
+                                    } else {
+                                        val = V(Src[(size_t)nd.in_edge * kBRow + pos]);
+                                    }
+                                }
+                                ak = ak + mul(sigma<V, USEAVG>(val, sb, pq.nchild), v);
+                            }
+                        } else {
+                            ak = ak + v;
+                        }
+                        sset(acc[k], d - 1, ak);
+                    }
+                }
+            }
+            __syncthreads();  // X is rewritten by the next group
+        }
+        close_to(0);
+
+        // ---- outputs: root values and their range-weighted sum ----
+        if (a.root_out) {
+            V *ro = reinterpret_cast<V *>(a.root_out) + (size_t)s * kBRow;
+#pragma unroll
+            for (int k = 0; k < K; k++)
+                if (pos0 + k < kBRow) ro[pos0 + k] = root[k];
+        }
+        if (a.sum_out) {
+            V part = V(0);
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const int pos = pos0 + k;
+                if (pos < kBRow) part += mul(V(rng[p * kBRow + pos]), root[k]);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(FULL, part, off);
+            if (lane == 0) S.wsum[warp] = part;
+            __syncthreads();
+            if (tid == 0) {
+                V t = V(0);
+                for (int w = 0; w < NW; w++) t += S.wsum[w];
+                reinterpret_cast<V *>(a.sum_out)[s] = t;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int K, typename V, int MODE, bool AVG, bool USEAVG>
+cudaError_t launch_one(const BLaunch &a, int ctas, int group, cudaStream_t stream) {
+    const size_t smem = smem_bytes<V>(group);
+    cudaError_t e = cudaFuncSetAttribute(batch_kernel<K, V, MODE, AVG, USEAVG>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    batch_kernel<K, V, MODE, AVG, USEAVG><<<ctas, Cfg<K>::NT, smem, stream>>>(a, group);
+    return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_k(int mode, int fp64, int avg, const BLaunch &a, int ctas, int group, cudaStream_t st) {
+    if (mode == kBModeCFR) {
+        if (fp64) return cudaErrorInvalidValue;
+        return avg ? launch_one<K, float, kBModeCFR, true, false>(a, ctas, group, st)
+                   : launch_one<K, float, kBModeCFR, false, false>(a, ctas, group, st);
+    }
+    if (mode == kBModeBR) {
+        if (fp64)
+            return a.use_average ? launch_one<K, double, kBModeBR, false, true>(a, ctas, group, st)
+                                 : launch_one<K, double, kBModeBR, false, false>(a, ctas, group, st);
+        return a.use_average ? launch_one<K, float, kBModeBR, false, true>(a, ctas, group, st)
+                             : launch_one<K, float, kBModeBR, false, false>(a, ctas, group, st);
+    }
+    if (fp64)
+        return a.use_average ? launch_one<K, double, kBModeEval, false, true>(a, ctas, group, st)
+                             : launch_one<K, double, kBModeEval, false, false>(a, ctas, group, st);
+    return a.use_average ? launch_one<K, float, kBModeEval, false, true>(a, ctas, group, st)
+                         : launch_one<K, float, kBModeEval, false, false>(a, ctas, group, st);
+}
+
+}  // namespace
+
+cudaError_t launch_batch_setup(const BSub *subs, int count, BPack *packs, const float *ranges_in,
+                               float *ranges_pos, int *err, cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    batch_setup_kernel<<<count, kSetupThreads, 0, stream>>>(subs, packs, ranges_in, ranges_pos, err);
+    return cudaGetLastError();
+}
+
+int batch_threads(int K) { return K == 2 ? Cfg<2>::NT : (K == 3 ? Cfg<3>::NT : Cfg<4>::NT); }
+
+int batch_group_leaves(int fp64) { return fp64 ? 8 : 16; }
+
+size_t batch_smem_bytes(int K, int fp64, int group) {
+    (void)K;
+    return fp64 ? smem_bytes<double>(group) : smem_bytes<float>(group);
+}
+
+cudaError_t launch_batch_pass(int mode, int K, int fp64, int avg, const BLaunch &a, int ctas, int group,
+                              cudaStream_t stream) {
+    if (group < 1 || group > kBMaxLeaves || ctas < 1) return cudaErrorInvalidValue;
+    switch (K) {
+        case 2: return launch_k<2>(mode, fp64, avg, a, ctas, group, stream);
+        case 3: return launch_k<3>(mode, fp64, avg, a, ctas, group, stream);
+        case 4: return launch_k<4>(mode, fp64, avg, a, ctas, group, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int batch_ctas_per_sm(int mode, int K, int fp64, int avg) {
+    int n = 0;
+    const int group = batch_group_leaves(fp64);
+    const size_t smem = batch_smem_bytes(K, fp64, group);
+    cudaError_t e = cudaSuccess;
+#define PRB_OCC(KK, VV, MM, AA, UU)                                                                   \
+    do {                                                                                              \
+        cudaFuncSetAttribute(batch_kernel<KK, VV, MM, AA, UU>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             (int)smem);                                                              \
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<KK, VV, MM, AA, UU>,         \
+                                                          Cfg<KK>::NT, smem);                         \
+    } while (0)
+    if (mode == kBModeCFR) {
+        if (K == 2) { if (avg) PRB_OCC(2, float, kBModeCFR, true, false); else PRB_OCC(2, float, kBModeCFR, false, false); }
+        else if (K == 3) { if (avg) PRB_OCC(3, float, kBModeCFR, true, false); else PRB_OCC(3, float, kBModeCFR, false, false); }
+        else { if (avg) PRB_OCC(4, float, kBModeCFR, true, false); else PRB_OCC(4, float, kBModeCFR, false, false); }
+    } else if (fp64) {
+        if (K == 2) PRB_OCC(2, double, kBModeBR, false, false);
+        else if (K == 3) PRB_OCC(3, double, kBModeBR, false, false);
+        else PRB_OCC(4, double, kBModeBR, false, false);
+    } else {
+        if (K == 2) PRB_OCC(2, float, kBModeBR, false, false);
+        else if (K == 3) PRB_OCC(3, float, kBModeBR, false, false);
+        else PRB_OCC(4, float, kBModeBR, false, false);
+    }
+#undef PRB_OCC
+    return e == cudaSuccess ? n : 0;
+}
+
+}  // namespace prb

@@ -22,6 +22,16 @@ BUCKETS = 256
 _lib = None
 
 
+class SubgameSpec(ctypes.Structure):
+    """pr_subgame: one general river subgame (board, pot, stack, bet sizes, raise cap)."""
+    _fields_ = [("board", ctypes.c_uint64), ("pot", ctypes.c_float), ("stack", ctypes.c_float),
+                ("sizes", ctypes.c_uint32), ("max_raises", ctypes.c_int32)]
+
+
+SPEC_DTYPE = np.dtype([("board", "<u8"), ("pot", "<f4"), ("stack", "<f4"), ("sizes", "<u4"),
+                       ("max_raises", "<i4")])
+
+
 class PokerLibError(RuntimeError):
     pass
 
@@ -83,6 +93,42 @@ def lib():
         L.pr_game_tables.argtypes = [vp]
         L.pr_game_iterate.restype = i32
         L.pr_game_iterate.argtypes = [vp, i32]
+        sg = ctypes.POINTER(SubgameSpec)
+        L.pr_batch_tree.restype = i32
+        L.pr_batch_tree.argtypes = [sg, vp, vp, vp, vp]
+        L.pr_batch_new.restype = vp
+        L.pr_batch_new.argtypes = [sg, i32, vp]
+        L.pr_batch_free.argtypes = [vp]
+        L.pr_batch_count.restype = i32
+        L.pr_batch_count.argtypes = [vp]
+        L.pr_batch_shape.restype = i32
+        L.pr_batch_shape.argtypes = [vp, i32, vp, vp, vp]
+        L.pr_batch_enable_average.restype = i32
+        L.pr_batch_enable_average.argtypes = [vp]
+        L.pr_batch_iterate.restype = i32
+        L.pr_batch_iterate.argtypes = [vp, i32]
+        L.pr_batch_exploitability.restype = i32
+        L.pr_batch_exploitability.argtypes = [vp, i32, i32, vp, vp, vp]
+        L.pr_batch_root_values.restype = i32
+        L.pr_batch_root_values.argtypes = [vp, i32, i32, vp, vp]
+        for name in ("pr_batch_get_regrets", "pr_batch_set_regrets", "pr_batch_get_average",
+                     "pr_batch_set_average"):
+            getattr(L, name).restype = i32
+            getattr(L, name).argtypes = [vp, i32, vp]
+        L.pr_batch_config.restype = i32
+        L.pr_batch_config.argtypes = [vp, i32, vp, vp, vp, vp]
+        L.pr_batch_set_config.restype = i32
+        L.pr_batch_set_config.argtypes = [vp, i32, i32, i32, i32]
+        L.pr_batch_tune.restype = i32
+        L.pr_batch_tune.argtypes = [vp, vp]
+        L.pr_batch_value.restype = i32
+        L.pr_batch_value.argtypes = [vp, i32, vp]
+        L.pr_batch_value_grad.restype = i32
+        L.pr_batch_value_grad.argtypes = [vp, i32, vp, vp, vp]
+        L.pr_batch_set_ranges.restype = i32
+        L.pr_batch_set_ranges.argtypes = [vp, i32, vp]
+        L.pr_batch_iteration_bytes.restype = ctypes.c_double
+        L.pr_batch_iteration_bytes.argtypes = [vp]
         L.pr_game_set_device_tree.restype = i32
         L.pr_game_set_device_tree.argtypes = [vp, i32]
         L.pr_evaluate_device_own.restype = i32
@@ -387,6 +433,168 @@ class Game:
     def close(self):
         if self.ptr:
             lib().pr_game_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- batched general river subgames ----
+
+def bet_tree(pot, stack, sizes, max_raises):
+    """The library's tree of one subgame: structured array of nodes (pre-order) and counts."""
+    spec = SubgameSpec(0, float(pot), float(stack), int(sizes), int(max_raises))
+    nodes = np.zeros(128, np.dtype([("kind", "u1"), ("actor", "u1"), ("nchild", "u1"), ("depth", "u1"),
+                                    ("parent", "<u2"), ("in_edge", "<u2"), ("edge", "<u2"), ("pad", "<u2"),
+                                    ("stake", "<f4")]))
+    n, e, l = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().pr_batch_tree(ctypes.byref(spec), _ptr(nodes), ctypes.byref(n), ctypes.byref(e),
+                               ctypes.byref(l)), "pr_batch_tree")
+    return nodes[:n.value], e.value, l.value
+
+
+def random_subgames(count, seed=0, max_nodes=60):
+    """Seeded general river subgames: 5 distinct board cards; pot ~ U{2..200}; stack ~
+    U{pot..10 pot}; a non-empty subset of {half pot, pot, all-in} and 1-3 bets and raises,
+    redrawn until the tree has at most `max_nodes` nodes; ranges U(0,1) per hand with 25 %
+    zeroed, hands on the board zeroed, normalised to sum 1. Returns (specs, ranges[count][2][1326])."""
+    rng = np.random.default_rng(seed)
+    order = card_order()
+    specs = np.zeros(count, SPEC_DTYPE)
+    ranges = np.zeros((count, 2, HANDS), np.float32)
+    for i in range(count):
+        cards = rng.choice(52, 5, replace=False)
+        board = 0
+        for c in cards:
+            board |= 1 << int(c)
+        pot = int(rng.integers(2, 201))
+        stack = int(rng.integers(pot, 10 * pot + 1))
+        while True:
+            sizes = int(rng.integers(1, 8))
+            raises = int(rng.integers(1, 4))
+            try:
+                nodes, _, _ = bet_tree(pot, stack, sizes, raises)
+            except PokerLibError:
+                continue  # beyond the solver's tree limits
+            if len(nodes) <= max_nodes:
+                break
+        specs[i] = (board, pot, stack, sizes, raises)
+        live = (order & np.uint64(board)) == 0
+        for p in range(2):
+            r = rng.random(HANDS, dtype=np.float32)
+            r[rng.random(HANDS) < 0.25] = 0.0
+            r[~live] = 0.0
+            ranges[i, p] = r / r.sum()
+    return specs, ranges
+
+
+class Batch:
+    """Many general river subgames solved together on the device (pr_batch_*)."""
+
+    def __init__(self, specs, ranges):
+        specs = np.ascontiguousarray(specs, SPEC_DTYPE)
+        ranges = np.ascontiguousarray(ranges, np.float32)
+        assert ranges.shape == (len(specs), 2, HANDS)
+        self.count = len(specs)
+        self.specs = specs
+        self.ranges = ranges
+        self.ptr = lib().pr_batch_new(specs.ctypes.data_as(ctypes.POINTER(SubgameSpec)), self.count,
+                                      _ptr(ranges))
+        if not self.ptr:
+            raise PokerLibError("pr_batch_new failed (bad board or bet tree; see stderr)")
+
+    def shape(self, s):
+        n, e, l = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().pr_batch_shape(self.ptr, int(s), ctypes.byref(n), ctypes.byref(e), ctypes.byref(l)),
+               "pr_batch_shape")
+        return n.value, e.value, l.value
+
+    def enable_average(self):
+        _check(lib().pr_batch_enable_average(self.ptr), "pr_batch_enable_average")
+
+    def iterate(self, iterations=1):
+        _check(lib().pr_batch_iterate(self.ptr, int(iterations)), "pr_batch_iterate")
+
+    def exploitability(self, use_average=False, fp64=True):
+        b0 = np.zeros(self.count)
+        b1 = np.zeros(self.count)
+        ex = np.zeros(self.count)
+        _check(lib().pr_batch_exploitability(self.ptr, int(bool(use_average)), int(bool(fp64)), _ptr(b0),
+                                             _ptr(b1), _ptr(ex)), "pr_batch_exploitability")
+        return b0, b1, ex
+
+    def root_values(self, player, use_average=False):
+        v = np.zeros((self.count, HANDS))
+        s = np.zeros(self.count)
+        _check(lib().pr_batch_root_values(self.ptr, int(player), int(bool(use_average)), _ptr(v), _ptr(s)),
+               "pr_batch_root_values")
+        return v, s
+
+    def value(self, use_average=False):
+        """Forward: V = r0^T U(sigma) r1 per subgame (double)."""
+        v = np.zeros(self.count)
+        _check(lib().pr_batch_value(self.ptr, int(bool(use_average)), _ptr(v)), "pr_batch_value")
+        return v
+
+    def value_grad(self, use_average=False):
+        """Backward: (dV/dr0, dV/dr1, dV/dsigma at the root) per subgame."""
+        g0 = np.zeros((self.count, HANDS))
+        g1 = np.zeros((self.count, HANDS))
+        gs = np.zeros((self.count, 8, HANDS))
+        _check(lib().pr_batch_value_grad(self.ptr, int(bool(use_average)), _ptr(g0), _ptr(g1), _ptr(gs)),
+               "pr_batch_value_grad")
+        return g0, g1, gs
+
+    def set_ranges(self, s, r):
+        r = np.ascontiguousarray(r, np.float32).reshape(2, HANDS)
+        _check(lib().pr_batch_set_ranges(self.ptr, int(s), _ptr(r)), "pr_batch_set_ranges")
+        self.ranges[s] = r
+
+    def _rows(self, name, s, data=None):
+        edges = self.shape(s)[1]
+        if data is None:
+            out = np.zeros((edges, HANDS), np.float32)
+            _check(getattr(lib(), name)(self.ptr, int(s), _ptr(out)), name)
+            return out
+        data = np.ascontiguousarray(data, np.float32).reshape(edges, HANDS)
+        _check(getattr(lib(), name)(self.ptr, int(s), _ptr(data)), name)
+
+    def regrets(self, s):
+        return self._rows("pr_batch_get_regrets", s)
+
+    def set_regrets(self, s, v):
+        self._rows("pr_batch_set_regrets", s, v)
+
+    def average(self, s):
+        return self._rows("pr_batch_get_average", s)
+
+    def set_average(self, s, v):
+        self._rows("pr_batch_set_average", s, v)
+
+    def config(self, c):
+        k, per, order, count = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().pr_batch_config(self.ptr, int(c), ctypes.byref(k), ctypes.byref(per), ctypes.byref(order),
+                                     ctypes.byref(count)), "pr_batch_config")
+        return dict(K=k.value, per_sm=per.value, order=order.value, count=count.value)
+
+    def set_config(self, c, K, per_sm=1, order=0):
+        _check(lib().pr_batch_set_config(self.ptr, int(c), int(K), int(per_sm), int(order)),
+               "pr_batch_set_config")
+
+    def tune(self):
+        ms = np.zeros(2)
+        _check(lib().pr_batch_tune(self.ptr, _ptr(ms)), "pr_batch_tune")
+        return ms
+
+    def iteration_bytes(self):
+        return lib().pr_batch_iteration_bytes(self.ptr)
+
+    def close(self):
+        if self.ptr:
+            lib().pr_batch_free(self.ptr)
             self.ptr = None
 
     def __del__(self):
