@@ -127,6 +127,85 @@ def sized_sample(boards, bets, ranges, tables, nthreads, seconds):
     return int(min(len(boards), max(probe, probe * seconds / max(dt, 1e-6))))
 
 
+BATCH_SUBGAMES = 4096
+
+
+def batch_section(P, rank, peak, cpu_threads, with_cpu):
+    """General river subgames (4096 seeded boards, pots, stacks and bet trees): per-hand CFR
+    iterations through the batched solver, its HBM roofline, and iterations / seconds until
+    the mean FP64 exploitability of the average strategies is at most 0.5 % of the pot."""
+    specs, ranges = P.random_subgames(BATCH_SUBGAMES, seed=4321 + rank)
+    b = P.Batch(specs, ranges)
+    b.enable_average()
+    b.iterate(2)  # the first iteration runs eagerly, then one iteration is captured as a graph
+    tuned = b.tune()
+    steps = 20
+    t0 = time.perf_counter()
+    b.iterate(steps)
+    it_s = (time.perf_counter() - t0) / steps
+    nbytes = b.iteration_bytes()
+    edges = sum(b.shape(i)[1] for i in range(b.count))
+    out = {
+        "workload": f"{BATCH_SUBGAMES} river subgames, 5-card seeded boards, pot U{{2..200}}, stack U{{pot..10 pot}}, "
+                    "bets from {0.5 pot, pot, all-in}, 1-3 raises, ranges U(0,1) with 25 % zeroed",
+        "iteration_ms": it_s * 1e3, "edges": edges,
+        "hand_edge_updates_per_s": edges * 1081 * 2 / it_s,
+        "roofline": {"bound": "hbm", "achieved": nbytes / it_s / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": nbytes / it_s / 1e9 / peak, "bytes_per_iteration": nbytes},
+        "tuned_pass_ms": [float(x) for x in tuned],
+        "configs": [b.config(c) for c in range(2)],
+    }
+    # convergence: restart from zero regrets, check every 25 iterations
+    b2 = P.Batch(specs, ranges)
+    b2.enable_average()
+    for c in range(2):
+        cfg = b.config(c)
+        b2.set_config(c, cfg["K"], cfg["per_sm"], cfg["order"])
+    done, t_solve, reached = 0, 0.0, None
+    trace = []
+    while done < 1000:
+        t0 = time.perf_counter()
+        b2.iterate(25)
+        t_solve += time.perf_counter() - t0
+        done += 25
+        _, _, ex = b2.exploitability(use_average=True, fp64=True)
+        pct = float(np.mean(ex / specs["pot"]) * 100.0)
+        trace.append((done, round(pct, 4)))
+        if pct <= 0.5:
+            reached = {"iterations": done, "solve_s": t_solve}
+            break
+    out["exploitability_pct_pot"] = trace
+    out["time_to_0.5pct_pot"] = reached
+    b2.close()
+    b.close()
+    if with_cpu:
+        out["cpu_baseline"] = batch_cpu_sample(specs, ranges, cpu_threads)
+    return out
+
+
+def batch_cpu_sample(specs, ranges, threads):
+    """The oracle's per-hand CFR (one thread per subgame) on a sample of the subgames, one
+    iteration each, scaled to the whole batch."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    def timed(n):
+        subs = [O.Subgame(int(s["board"]), float(s["pot"]), float(s["stack"]), int(s["sizes"]),
+                          int(s["max_raises"]), r[0], r[1]) for s, r in zip(specs[:n], ranges[:n])]
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda o: o.iterate(1), subs))
+        return time.perf_counter() - t0
+
+    # a probe of one subgame per thread, then a sample sized to about 10 s
+    probe = max(threads, 8)
+    dt = timed(probe)
+    n = int(min(len(specs), max(probe, probe * 10.0 / max(dt, 1e-6))))
+    dt = timed(n)
+    per_iter = dt * len(specs) / n
+    return {"iteration_ms": per_iter * 1e3, "cores": threads, "kind": "port",
+            "sample": f"{n} of {len(specs)} subgames, one iteration, {dt:.2f} s, scaled"}
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -167,6 +246,27 @@ def run_reference(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch_profile(args):
+    """The batched solver alone (for profiling): args.batch_profile subgames, warm-up and
+    timed CFR iterations, one JSON line."""
+    import torch
+    rank, _, local = dist_env()
+    torch.cuda.set_device(local)
+    import pokerrust_b200 as P
+    specs, ranges = P.random_subgames(args.batch_profile, seed=4321 + rank)
+    b = P.Batch(specs, ranges)
+    b.enable_average()
+    b.iterate(max(2, args.warmup))
+    t0 = time.perf_counter()
+    b.iterate(args.steps)
+    dt = (time.perf_counter() - t0) / max(1, args.steps)
+    nbytes = b.iteration_bytes()
+    print(json.dumps({"batch_profile": True, "subgames": args.batch_profile, "iteration_ms": dt * 1e3,
+                      "achieved_gbs": nbytes / dt / 1e9, "bytes_per_iteration": nbytes}), flush=True)
+    b.close()
     return 0
 
 
@@ -279,6 +379,8 @@ def run_gpu(args):
     h1, d1 = game.timings()
     game.set_device_tree(True)
 
+    batch = batch_section(P, rank, measured_peaks()[0], os.cpu_count() or 1, rank == 0)
+
     line = None
     if rank == 0:
         from oracle import oracle as O  # CPU baseline only
@@ -310,6 +412,7 @@ def run_gpu(args):
                                        f"{cpu_dt:.2f} s, scaled to nodes/s"},
             "gpu_launches": args.steps,
             "clocks": clk,
+            "batch_subgames": batch,
             "game_iteration": {"ms": dev_iter_s * 1e3,
                                "note": "one full CFR iteration of the fixed-flop game (both players): "
                                        "upper tree and river passes on the device, one CUDA graph",
@@ -334,6 +437,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch-profile", type=int, default=0,
+                    help="only the batched general subgames: this many, a few timed iterations")
     ap.add_argument("--subgames", type=int, default=0,
                     help="use the first N river roots only (profiling runs); 0 = all 27783")
     ap.add_argument("--profile", action="store_true",
@@ -341,6 +446,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.batch_profile:
+        return run_batch_profile(args)
     return run_gpu(args)
 
 

@@ -172,24 +172,8 @@ __global__ void __launch_bounds__(kSetupThreads) batch_setup_kernel(const BSub *
 template <int K>
 struct Cfg {
     static constexpr int NT = K == 2 ? 544 : (K == 3 ? 384 : 288);
+    static constexpr int MINB = K == 2 ? 1 : 2;  // CTAs per SM the register budget is sized for
 };
-
-// depth-indexed register stacks: every access is an unrolled select, so nothing spills to
-// local memory
-template <typename T, int N>
-__device__ __forceinline__ T sget(const T (&a)[N], int d) {
-    T v = a[0];
-#pragma unroll
-    for (int i = 1; i < N; i++)
-        if (i == d) v = a[i];
-    return v;
-}
-template <typename T, int N>
-__device__ __forceinline__ void sset(T (&a)[N], int d, T v) {
-#pragma unroll
-    for (int i = 0; i < N; i++)
-        if (i == d) a[i] = v;
-}
 
 template <typename V>
 __device__ __forceinline__ V neg_inf();
@@ -200,6 +184,26 @@ __device__ __forceinline__ float neg_inf<float>() {
 template <>
 __device__ __forceinline__ double neg_inf<double>() {
     return -__longlong_as_double(0x7ff0000000000000ll);
+}
+
+// Asks L2 to fetch [p, p + bytes) (16-byte aligned, size a multiple of 16) ahead of use.
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+    const char *c = reinterpret_cast<const char *>(p);
+    while (bytes > 0) {
+        const unsigned n = bytes > 65536 ? 65536u : (unsigned)bytes;
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c), "r"(n) : "memory");
+        c += n;
+        bytes -= n;
+    }
+}
+
+// The regret (and average) rows of subgame s, prefetched into L2.
+__device__ __forceinline__ void prefetch_subgame(const BLaunch &a, int s) {
+    const BSub sub = a.subs[s];
+    const size_t off = (size_t)sub.edge_off * kBRow, bytes = (size_t)sub.num_edges * kBRow * sizeof(float);
+    prefetch_l2(a.regrets + off, bytes);
+    if (a.avg) prefetch_l2(a.avg + off, bytes);
+    prefetch_l2(a.ranges + (size_t)s * 2 * kBRow, 2 * kBRow * sizeof(float));
 }
 
 // products rounded on their own (no contraction into a following add)
@@ -257,7 +261,7 @@ __device__ __forceinline__ V sigma(V val, V S, int n) {
 }
 
 template <int K, typename V, int MODE, bool AVG, bool USEAVG>
-__global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int group) {
+__global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch a, int group) {
     constexpr int NT = Cfg<K>::NT;
     constexpr int NW = NT / 32;
     static_assert(MODE == kBModeCFR || !AVG, "average sums accumulate in CFR passes");
@@ -272,12 +276,21 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
     const int p = a.player, o = 1 - p;
     const float *src_all = USEAVG ? a.avg : a.regrets;
 
+    // The next queue entry is taken (and its rows prefetched into L2) while the current one
+    // is solved.
+    if (tid == 0) {
+        s_next = atomicAdd(a.head, 1);
+        if (s_next < a.count) prefetch_subgame(a, a.order[s_next]);
+    }
     for (;;) {
-        if (tid == 0) s_next = atomicAdd(a.head, 1);
         __syncthreads();
         const int qi = s_next;
         __syncthreads();
         if (qi >= a.count) break;
+        if (tid == 0) {
+            s_next = atomicAdd(a.head, 1);
+            if (s_next < a.count) prefetch_subgame(a, a.order[s_next]);
+        }
         const int s = a.order[qi];
         const BSub sub = a.subs[s];
         const BPack *__restrict__ pk = a.packs + s;
@@ -294,7 +307,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
         const float *rng = a.ranges + (size_t)s * 2 * kBRow;
         const int pos0 = tid * K;
 
-        // walker state, per owned hand: depth-indexed stacks of the open path
+        // walker state, per owned hand: depth-indexed stacks of the open path (indexed at run
+        // time, so they live in local memory, cached in L1)
         V po[K][DS], pp[K][DS], St[K][DS];   // top-down: opponent weight, own reach, strategy sums
         V acc[K][DS], Sb[K][DS];             // bottom-up: node values, strategy sums
         int open_id[DS];
@@ -307,11 +321,11 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
         // closes the open nodes at depth >= d, passing each value to its parent
         auto close_to = [&](int d) {
             while (open_top >= d) {
-                const int m = sget(open_id, open_top);
+                const int m = open_id[open_top];
                 const BNode nm = S.tn[m];
                 V v[K];
 #pragma unroll
-                for (int k = 0; k < K; k++) v[k] = sget(acc[k], open_top);
+                for (int k = 0; k < K; k++) v[k] = acc[k][open_top];
                 if (MODE == kBModeCFR && nm.actor == p) {
 #pragma unroll
                     for (int k = 0; k < K; k++) {
@@ -338,13 +352,13 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
                     }
 #pragma unroll
                     for (int k = 0; k < K; k++) {
-                        V ak = sget(acc[k], open_top);
+                        V ak = acc[k][open_top];
                         const int pos = pos0 + k;
                         if (pq.actor == p) {
                             if (MODE == kBModeBR) {
                                 ak = ak > v[k] ? ak : v[k];
                             } else {
-                                const V sb = sget(Sb[k], open_top);
+                                const V sb = Sb[k][open_top];
                                 V val = V(0);
                                 if (pos < kBRow) {
                                     if (MODE == kBModeCFR) {
@@ -360,7 +374,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
                         } else {
                             ak = ak + v[k];
                         }
-                        sset(acc[k], open_top, ak);
+                        acc[k][open_top] = ak;
                     }
                 }
             }
@@ -386,13 +400,13 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
                     const bool need = !own || AVG;
 #pragma unroll
                     for (int k = 0; k < K; k++) {
-                        const V po_par = sget(po[k], d - 1);
-                        const V pp_par = sget(pp[k], d - 1);
+                        const V po_par = po[k][d - 1];
+                        const V pp_par = pp[k][d - 1];
                         V sg = V(1);
                         if (need) {
                             const int pos = pos0 + k;
                             const V val = pos < kBRow ? V(Src[(size_t)nd.in_edge * kBRow + pos]) : V(0);
-                            sg = sigma<V, USEAVG>(val, sget(St[k], d - 1), pm.nchild);
+                            sg = sigma<V, USEAVG>(val, St[k][d - 1], pm.nchild);
                         }
                         if (own) {
                             npo[k] = po_par;
@@ -412,8 +426,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
                 }
 #pragma unroll
                 for (int k = 0; k < K; k++) {
-                    sset(po[k], d, npo[k]);
-                    sset(pp[k], d, npp[k]);
+                    po[k][d] = npo[k];
+                    pp[k][d] = npp[k];
                 }
                 if (nd.kind == kBDecision) {
                     // strategy sums of the node, for its children
@@ -429,7 +443,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
                                 sum += val > V(0) ? val : V(0);
                             }
                         }
-                        sset(St[k], d, sum);
+                        St[k][d] = sum;
                     }
                 } else {
                     V *x = S.X + (size_t)(nd.edge - g0) * kBRow;
@@ -547,11 +561,11 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
                 close_to(d);
                 if (nd.kind == kBDecision) {
                     open_top = d;
-                    sset(open_id, d, bu);
+                    open_id[d] = bu;
                     const bool own = nd.actor == p;
 #pragma unroll
                     for (int k = 0; k < K; k++) {
-                        sset(acc[k], d, (own && MODE == kBModeBR) ? neg_inf<V>() : V(0));
+                        acc[k][d] = (own && MODE == kBModeBR) ? neg_inf<V>() : V(0);
                         V sum = V(0);
                         if (own && MODE != kBModeBR) {
                             const int pos = pos0 + k;
@@ -560,7 +574,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
                                 sum += val > V(0) ? val : V(0);
                             }
                         }
-                        sset(Sb[k], d, sum);
+                        Sb[k][d] = sum;
                     }
                 } else {
                     // a leaf: its value goes straight to the parent (open at depth d - 1)
@@ -576,12 +590,12 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
                     for (int k = 0; k < K; k++) {
                         const int pos = pos0 + k;
                         const V v = pos < kBRow ? x[pos] : V(0);
-                        V ak = sget(acc[k], d - 1);
+                        V ak = acc[k][d - 1];
                         if (pq.actor == p) {
                             if (MODE == kBModeBR) {
                                 ak = ak > v ? ak : v;
                             } else {
-                                const V sb = sget(Sb[k], d - 1);
+                                const V sb = Sb[k][d - 1];
                                 V val = V(0);
                                 if (pos < kBRow) {
                                     if (MODE == kBModeCFR) {
@@ -597,7 +611,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, 1) batch_kernel(BLaunch a, int gro
                         } else {
                             ak = ak + v;
                         }
-                        sset(acc[k], d - 1, ak);
+                        acc[k][d - 1] = ak;
                     }
                 }
             }
