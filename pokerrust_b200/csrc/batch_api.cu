@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -131,6 +132,33 @@ struct Batch {
         return 0;
     }
 };
+
+// ---- no-allocation iteration ----
+// Work-queue scratch of pr_batch_iterate_noalloc: kClasses * 2 queue heads, then the queue
+// order of up to kNoAllocMaxSubgames subgames. A fixed device array of the library, so the
+// call allocates nothing.
+constexpr int kNoAllocMaxSubgames = 65536;
+constexpr int kNoAllocHeads = 2 * kClasses;
+__device__ __align__(256) int g_noalloc_scratch[kNoAllocHeads + kNoAllocMaxSubgames];
+
+std::mutex g_noalloc_mu;
+int *g_noalloc_ptr[64] = {};  // per device, looked up once with that device current
+
+int *noalloc_scratch() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            bfail("no-allocation scratch lookup", e);
+            return nullptr;
+        }
+        g_noalloc_ptr[dev] = (int *)p;
+    }
+    return g_noalloc_ptr[dev];
+}
 
 }  // namespace
 }  // namespace prb
@@ -400,6 +428,53 @@ int pr_batch_root_values(void *batch, int player, int use_average, double *value
         }
     }
     return 0;
+}
+
+// CFR iterations like pr_batch_iterate, launched eagerly, with the work queue (heads and
+// order) in the library's fixed device array instead of the batch's buffers: no allocation.
+int pr_batch_iterate_noalloc(void *batch, int iterations) {
+    Batch *b = (Batch *)batch;
+    if (!b || iterations < 0) return 2;
+    if (b->count > kNoAllocMaxSubgames) {
+        fprintf(stderr, "pokerrust_b200: pr_batch_iterate_noalloc: %d subgames exceed the limit of %d\n", b->count,
+                kNoAllocMaxSubgames);
+        return 2;
+    }
+    int *scratch = noalloc_scratch();
+    if (!scratch) return 1;
+    int *heads = scratch, *order = scratch + kNoAllocHeads;
+    std::vector<int> host_order;
+    b->build_order(host_order);
+    cudaError_t e = cudaMemcpyAsync(order, host_order.data(), sizeof(int) * b->count, cudaMemcpyHostToDevice,
+                                    b->stream);
+    if (e != cudaSuccess) return bfail("queue upload", e);
+    for (int it = 0; it < iterations; it++) {
+        // the queue heads must start at zero for every pass
+        e = cudaMemsetAsync(heads, 0, sizeof(int) * kNoAllocHeads, b->stream);
+        if (e != cudaSuccess) return bfail("queue reset", e);
+        for (int pl = 0; pl < 2; pl++) {
+            for (int c = 0; c < kClasses; c++) {
+                const ClassCfg &k = b->cls[c];
+                if (!k.count) continue;
+                BLaunch a{};
+                a.subs = b->d_subs;
+                a.nodes = b->d_nodes;
+                a.packs = b->d_packs;
+                a.ranges = b->d_ranges;
+                a.regrets = b->d_regrets;
+                a.avg = b->avg_on ? b->d_avg : nullptr;
+                a.order = order + k.first;
+                a.head = heads + pl * kClasses + c;
+                a.count = k.count;
+                a.player = pl;
+                const int ctas = std::min(k.count, std::max(1, k.per_sm) * b->sms);
+                e = launch_batch_pass(kBModeCFR, k.K, 0, b->avg_on, a, ctas, batch_group_leaves(0), b->stream);
+                if (e != cudaSuccess) return bfail("pass launch", e);
+            }
+        }
+    }
+    e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? 0 : bfail("iteration", e);
 }
 
 // Subgame value V = r0^T U(sigma) r1 = sum_h r0(h) cfv0(h): player 0's expected chips times

@@ -121,6 +121,8 @@ def lib():
         L.pr_batch_set_config.argtypes = [vp, i32, i32, i32, i32]
         L.pr_batch_tune.restype = i32
         L.pr_batch_tune.argtypes = [vp, vp]
+        L.pr_batch_iterate_noalloc.restype = i32
+        L.pr_batch_iterate_noalloc.argtypes = [vp, i32]
         L.pr_batch_value.restype = i32
         L.pr_batch_value.argtypes = [vp, i32, vp]
         L.pr_batch_value_grad.restype = i32
@@ -517,6 +519,11 @@ class Batch:
 
     def iterate(self, iterations=1):
         _check(lib().pr_batch_iterate(self.ptr, int(iterations)), "pr_batch_iterate")
+
+    def iterate_noalloc(self, iterations=1):
+        """pr_batch_iterate_noalloc: eager iterations with the queue scratch in a fixed device
+        array (no allocation; one call at a time)."""
+        _check(lib().pr_batch_iterate_noalloc(self.ptr, int(iterations)), "pr_batch_iterate_noalloc")
 
     def exploitability(self, use_average=False, fp64=True):
         b0 = np.zeros(self.count)
