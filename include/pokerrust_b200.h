@@ -245,6 +245,36 @@ int pr_batch_tune(void *batch, double *ms_out);
 /* Algorithmic HBM bytes of one CFR iteration (roofline numerator). */
 double pr_batch_iteration_bytes(void *batch);
 
+/* ---- turn-leaf value network (extension) ----
+ * D[M][N] (f32) = A[M][K] . B[N][K]^T for bf16 A, B on the tcgen05 tensor cores (device
+ * pointers; M % 128 == 0, N % bn == 0, K % 64 == 0, bn 128 or 256). Synchronous. */
+int pr_gemm_bf16(const void *A, const void *B, float *D, int M, int N, int K, int bn, void *stream);
+/* Asynchronous form; err is a device int that collects error bits of timed-out waits. */
+int pr_gemm_bf16_async(const void *A, const void *B, float *D, int M, int N, int K, int bn, int *err,
+                       void *stream);
+
+/* The network: 2706 inputs (both ranges, the 4 turn cards as 52 0/1 values, pot / 200 and
+ * stack / (10 pot)) -> 4 x 1024 GELU -> 2652 outputs (both players' counterfactual values per
+ * hand over the pot). BF16 weights and activations, FP32 accumulation and master weights,
+ * MSE loss, Adam. rows: the batch the buffers are sized for (a multiple of 256). Inputs and
+ * outputs are device pointers: ranges [n][2][1326], boards [n] (4-card masks), scalars [n][2],
+ * targets / out [n][2652]; n <= rows. */
+void *pr_mlp_new(int rows, uint64_t seed);
+void pr_mlp_free(void *net);
+int pr_mlp_rows(void *net);
+int pr_mlp_forward(void *net, const float *ranges, const uint64_t *boards, const float *scalars, float *out,
+                   int n);
+/* One step: forward, loss, backward, Adam with learning rate lr (lr = 0: gradients only).
+ * loss: the batch's mean squared error before the update. */
+int pr_mlp_train_step(void *net, const float *ranges, const uint64_t *boards, const float *scalars,
+                      const float *targets, int n, float lr, double *loss);
+/* Layer l (0..4): fan-out x fan-in of the live weights; host copies of W, b and of the last
+ * step's gradients. */
+int pr_mlp_layer_shape(int l, int *fan_out, int *fan_in);
+int pr_mlp_get_layer(void *net, int l, float *W, float *b);
+int pr_mlp_set_layer(void *net, int l, const float *W, const float *b);
+int pr_mlp_get_grad(void *net, int l, float *dW, float *db);
+
 #ifdef __cplusplus
 }
 #endif

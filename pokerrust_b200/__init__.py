@@ -12,6 +12,7 @@ from .interface import (  # noqa: F401
     Builder,
     Game,
     PokerLibError,
+    ValueNet,
     bet_tree,
     random_subgames,
     build_flop_tables,

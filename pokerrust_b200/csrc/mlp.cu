@@ -1,0 +1,479 @@
+// Turn-leaf value network: a 5-layer MLP (2706 -> 4 x 1024 GELU -> 2652) trained and run on
+// the device with the tcgen05 GEMM of mlp_gemm.cuh (BF16 operands, FP32 accumulation),
+// fused epilogues (bias + GELU, bias, GELU derivative), BF16 transposes, an MSE loss
+// kernel, bias-gradient reductions and Adam on FP32 master weights.
+//
+// Input per sample: both players' ranges over the 1326 hands, the 4 turn-board cards as a
+// 52-wide 0/1 vector, pot and stack scaled to [0, 1] (pot / 200, stack / (10 pot)).
+// Output: both players' counterfactual values per hand divided by the pot.
+// Shapes are padded for the GEMM tiles: input 2706 -> 2816 columns, output 2652 -> 2688.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../include/pokerrust_b200.h"
+#include "mlp_gemm.cuh"
+
+namespace prb {
+namespace mlp {
+
+using gemm::bf16;
+
+constexpr int kIn = 2706, kInPad = 2816, kHid = 1024, kOut = 2652, kOutPad = 2688;
+constexpr int kLayers = 5;
+constexpr int kK[kLayers] = {kInPad, kHid, kHid, kHid, kHid};       // padded fan-in
+constexpr int kN[kLayers] = {kHid, kHid, kHid, kHid, kOutPad};      // padded fan-out
+constexpr int kKLive[kLayers] = {kIn, kHid, kHid, kHid, kHid};
+constexpr int kNLive[kLayers] = {kHid, kHid, kHid, kHid, kOut};
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+    return cdf + z * pdf;
+}
+
+// ---- GEMM epilogues (called with 32 accumulator values of one row per thread) ----
+struct EpiBiasGelu {  // Z = acc + b, H = gelu(Z), both bf16
+    const float *bias;
+    bf16 *Z, *H;
+    int ld;
+    template <class R, class P>
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+#pragma unroll
+        for (int i = 0; i < cute::size(reg); i++) {
+            const int m = m0 + cute::get<0>(pos(i)), n = n0 + cute::get<1>(pos(i));
+            const float z = reg(i) + bias[n];
+            Z[(size_t)m * ld + n] = bf16(z);
+            H[(size_t)m * ld + n] = bf16(gelu(z));
+        }
+    }
+};
+struct EpiBiasF32 {  // Y = acc + b (f32)
+    const float *bias;
+    float *Y;
+    int ld;
+    template <class R, class P>
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+#pragma unroll
+        for (int i = 0; i < cute::size(reg); i++) {
+            const int m = m0 + cute::get<0>(pos(i)), n = n0 + cute::get<1>(pos(i));
+            Y[(size_t)m * ld + n] = reg(i) + bias[n];
+        }
+    }
+};
+struct EpiGeluGrad {  // dZ = acc * gelu'(Z), bf16
+    const bf16 *Z;
+    bf16 *dZ;
+    int ld;
+    template <class R, class P>
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+#pragma unroll
+        for (int i = 0; i < cute::size(reg); i++) {
+            const int m = m0 + cute::get<0>(pos(i)), n = n0 + cute::get<1>(pos(i));
+            const size_t at = (size_t)m * ld + n;
+            dZ[at] = bf16(reg(i) * gelu_grad(float(Z[at])));
+        }
+    }
+};
+struct EpiStore {  // D = acc (f32)
+    float *D;
+    int ld;
+    template <class R, class P>
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+#pragma unroll
+        for (int i = 0; i < cute::size(reg); i++) {
+            const int m = m0 + cute::get<0>(pos(i)), n = n0 + cute::get<1>(pos(i));
+            D[(size_t)m * ld + n] = reg(i);
+        }
+    }
+};
+
+// ---- element-wise kernels ----
+__global__ void transpose_kernel(const bf16 *__restrict__ in, bf16 *__restrict__ out, int rows, int cols) {
+    __shared__ bf16 tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int r = r0 + i, c = c0 + threadIdx.x;
+        tile[i][threadIdx.x] = (r < rows && c < cols) ? in[(size_t)r * cols + c] : bf16(0.0f);
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int c = c0 + i, r = r0 + threadIdx.x;
+        if (c < cols && r < rows) out[(size_t)c * rows + r] = tile[threadIdx.x][i];
+    }
+}
+
+// inputs: ranges [n][2][1326], boards (4 cards) [n], scalars [n][2] -> X [rows][kInPad] bf16
+__global__ void assemble_kernel(const float *__restrict__ ranges, const unsigned long long *__restrict__ boards,
+                                const float *__restrict__ scalars, bf16 *__restrict__ X, int n) {
+    const int s = blockIdx.x;
+    bf16 *x = X + (size_t)s * kInPad;
+    for (int i = threadIdx.x; i < kInPad; i += blockDim.x) {
+        float v = 0.0f;
+        if (s < n) {
+            if (i < 2 * 1326) v = ranges[(size_t)s * 2 * 1326 + i];
+            else if (i < 2 * 1326 + 52) v = (boards[s] >> (i - 2 * 1326)) & 1ull ? 1.0f : 0.0f;
+            else if (i < kIn) v = scalars[(size_t)s * 2 + (i - 2 * 1326 - 52)];
+        }
+        x[i] = bf16(v);
+    }
+}
+
+// dY = 2 (Y - T) / (n * kOut) on live outputs of live rows (bf16), and per-block squared errors
+__global__ void loss_kernel(const float *__restrict__ Y, const float *__restrict__ T, bf16 *__restrict__ dY,
+                            double *__restrict__ partial, int n, int rows) {
+    const int m = blockIdx.x;
+    __shared__ double red[256];
+    double acc = 0.0;
+    const float scale = 2.0f / ((float)n * (float)kOut);
+    for (int j = threadIdx.x; j < kOutPad; j += blockDim.x) {
+        float g = 0.0f;
+        if (m < n && j < kOut) {
+            const float d = Y[(size_t)m * kOutPad + j] - T[(size_t)m * kOut + j];
+            acc += (double)d * d;
+            g = d * scale;
+        }
+        dY[(size_t)m * kOutPad + j] = bf16(g);
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[m] = red[0];
+    (void)rows;
+}
+
+// db[j] = sum over rows of G^T[j][:]  (G^T: [cols][rows] bf16, one warp per column)
+__global__ void bias_grad_kernel(const bf16 *__restrict__ GT, float *__restrict__ db, int cols, int rows) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x % 32;
+    if (warp >= cols) return;
+    float acc = 0.0f;
+    for (int m = lane; m < rows; m += 32) acc += float(GT[(size_t)warp * rows + m]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) db[warp] = acc;
+}
+
+// Adam on f32 master weights; padding (rows >= n_live or columns >= k_live) stays zero.
+__global__ void adam_kernel(float *__restrict__ w, float *__restrict__ m1, float *__restrict__ m2,
+                            const float *__restrict__ g, bf16 *__restrict__ wb, int rows, int cols, int n_live,
+                            int k_live, float lr, float b1, float b2, float c1, float c2, float eps) {
+    const size_t total = (size_t)rows * cols;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / cols), c = (int)(i % cols);
+        if (r >= n_live || c >= k_live) {
+            w[i] = 0.0f;
+            if (wb) wb[i] = bf16(0.0f);
+            continue;
+        }
+        const float gi = g[i];
+        const float a = b1 * m1[i] + (1.0f - b1) * gi;
+        const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
+        m1[i] = a;
+        m2[i] = b;
+        const float upd = (a / c1) / (sqrtf(b / c2) + eps);
+        w[i] -= lr * upd;
+        if (wb) wb[i] = bf16(w[i]);
+    }
+}
+
+__global__ void to_bf16_kernel(const float *__restrict__ w, bf16 *__restrict__ wb, size_t total) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
+        wb[i] = bf16(w[i]);
+}
+
+__global__ void copy_out_kernel(const float *__restrict__ Y, float *__restrict__ out, int n) {
+    const int m = blockIdx.x;
+    if (m >= n) return;
+    for (int j = threadIdx.x; j < kOut; j += blockDim.x) out[(size_t)m * kOut + j] = Y[(size_t)m * kOutPad + j];
+}
+
+struct Net {
+    int rows = 0;  // batch rows (multiple of 256)
+    cudaStream_t stream = nullptr;
+    int *d_err = nullptr;
+    // parameters (f32 master, bf16 copy, bf16 transpose), gradients, Adam moments
+    float *W[kLayers] = {}, *b[kLayers] = {}, *dW[kLayers] = {}, *db[kLayers] = {};
+    float *mW[kLayers] = {}, *vW[kLayers] = {}, *mb[kLayers] = {}, *vb[kLayers] = {};
+    bf16 *Wb[kLayers] = {}, *WT[kLayers] = {};
+    // activations
+    bf16 *X = nullptr, *XT = nullptr;
+    bf16 *Z[4] = {}, *H[4] = {}, *HT[4] = {}, *dZ[4] = {}, *dZT[4] = {};
+    float *Y = nullptr;
+    bf16 *dY = nullptr, *dYT = nullptr;
+    double *partial = nullptr;
+    int step = 0;
+    std::vector<void *> owned;
+
+    template <class T>
+    bool alloc(T **p, size_t n) {
+        if (cudaMalloc((void **)p, n * sizeof(T)) != cudaSuccess) return false;
+        owned.push_back(*p);
+        return cudaMemsetAsync(*p, 0, n * sizeof(T), stream) == cudaSuccess;
+    }
+    ~Net() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *p : owned) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    int check(cudaError_t e, const char *what) {
+        if (e == cudaSuccess) return 0;
+        fprintf(stderr, "pokerrust_b200: value network: %s: %s\n", what, cudaGetErrorString(e));
+        return e == cudaErrorInvalidValue ? 2 : 1;
+    }
+
+    // forward pass over X (rows), Y = output pre-loss (f32)
+    int forward() {
+        cudaError_t e = cudaSuccess;
+        const bf16 *in = X;
+        for (int l = 0; l < 4 && e == cudaSuccess; l++) {
+            EpiBiasGelu epi{b[l], Z[l], H[l], kN[l]};
+            e = gemm::run<256>(in, Wb[l], rows, kN[l], kK[l], epi, d_err, stream);
+            in = H[l];
+        }
+        if (e == cudaSuccess) {
+            EpiBiasF32 epi{b[4], Y, kOutPad};
+            e = gemm::run<128>(in, Wb[4], rows, kOutPad, kHid, epi, d_err, stream);
+        }
+        return check(e, "forward");
+    }
+
+    void transpose(const bf16 *in, bf16 *out, int r, int c) {
+        dim3 grid((c + 31) / 32, (r + 31) / 32), block(32, 8);
+        transpose_kernel<<<grid, block, 0, stream>>>(in, out, r, c);
+    }
+
+    // backward from dY (bf16), gradients into dW / db
+    int backward() {
+        cudaError_t e = cudaSuccess;
+        transpose(dY, dYT, rows, kOutPad);
+        // output layer
+        transpose(H[3], HT[3], rows, kHid);
+        {
+            EpiStore epi{dW[4], kHid};
+            e = gemm::run<256>(dYT, HT[3], kOutPad, kHid, rows, epi, d_err, stream);
+        }
+        bias_grad_kernel<<<(kOutPad * 32 + 255) / 256, 256, 0, stream>>>(dYT, db[4], kOutPad, rows);
+        if (e == cudaSuccess) {
+            EpiGeluGrad epi{Z[3], dZ[3], kHid};
+            e = gemm::run<256>(dY, WT[4], rows, kHid, kOutPad, epi, d_err, stream);
+        }
+        for (int l = 3; l >= 0 && e == cudaSuccess; l--) {
+            transpose(dZ[l], dZT[l], rows, kHid);
+            const bf16 *inT = l > 0 ? HT[l - 1] : XT;
+            if (l > 0) transpose(H[l - 1], HT[l - 1], rows, kHid);
+            else transpose(X, XT, rows, kInPad);
+            EpiStore epi{dW[l], kK[l]};
+            e = gemm::run<256>(dZT[l], inT, kHid, kK[l], rows, epi, d_err, stream);
+            bias_grad_kernel<<<(kHid * 32 + 255) / 256, 256, 0, stream>>>(dZT[l], db[l], kHid, rows);
+            if (e == cudaSuccess && l > 0) {
+                EpiGeluGrad epi2{Z[l - 1], dZ[l - 1], kHid};
+                e = gemm::run<256>(dZ[l], WT[l], rows, kHid, kHid, epi2, d_err, stream);
+            }
+        }
+        if (e == cudaSuccess) e = cudaGetLastError();
+        return check(e, "backward");
+    }
+
+    int adam(float lr) {
+        step++;
+        const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+        const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+        for (int l = 0; l < kLayers; l++) {
+            adam_kernel<<<1184, 256, 0, stream>>>(W[l], mW[l], vW[l], dW[l], Wb[l], kN[l], kK[l], kNLive[l],
+                                                 kKLive[l], lr, b1, b2, c1, c2, eps);
+            adam_kernel<<<8, 256, 0, stream>>>(b[l], mb[l], vb[l], db[l], nullptr, 1, kN[l], 1, kNLive[l], lr, b1,
+                                               b2, c1, c2, eps);
+            transpose(Wb[l], WT[l], kN[l], kK[l]);
+        }
+        return check(cudaGetLastError(), "adam");
+    }
+
+    int refresh_copies() {
+        for (int l = 0; l < kLayers; l++) {
+            to_bf16_kernel<<<592, 256, 0, stream>>>(W[l], Wb[l], (size_t)kN[l] * kK[l]);
+            transpose(Wb[l], WT[l], kN[l], kK[l]);
+        }
+        return check(cudaGetLastError(), "weights");
+    }
+};
+
+uint64_t splitmix(uint64_t &x) {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+}  // namespace mlp
+}  // namespace prb
+
+using namespace prb::mlp;
+
+extern "C" {
+
+void *pr_mlp_new(int rows, uint64_t seed) {
+    if (rows <= 0 || rows % 256) {
+        fprintf(stderr, "pokerrust_b200: value network: batch rows must be a positive multiple of 256\n");
+        return nullptr;
+    }
+    Net *n = new Net();
+    n->rows = rows;
+    bool ok = cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking) == cudaSuccess && n->alloc(&n->d_err, 1);
+    for (int l = 0; l < kLayers && ok; l++) {
+        const size_t sz = (size_t)kN[l] * kK[l];
+        ok = n->alloc(&n->W[l], sz) && n->alloc(&n->dW[l], sz) && n->alloc(&n->mW[l], sz) && n->alloc(&n->vW[l], sz) &&
+             n->alloc(&n->Wb[l], sz) && n->alloc(&n->WT[l], sz) && n->alloc(&n->b[l], kN[l]) &&
+             n->alloc(&n->db[l], kN[l]) && n->alloc(&n->mb[l], kN[l]) && n->alloc(&n->vb[l], kN[l]);
+    }
+    ok = ok && n->alloc(&n->X, (size_t)rows * kInPad) && n->alloc(&n->XT, (size_t)rows * kInPad) &&
+         n->alloc(&n->Y, (size_t)rows * kOutPad) && n->alloc(&n->dY, (size_t)rows * kOutPad) &&
+         n->alloc(&n->dYT, (size_t)rows * kOutPad) && n->alloc(&n->partial, rows);
+    for (int l = 0; l < 4 && ok; l++)
+        ok = n->alloc(&n->Z[l], (size_t)rows * kHid) && n->alloc(&n->H[l], (size_t)rows * kHid) &&
+             n->alloc(&n->HT[l], (size_t)rows * kHid) && n->alloc(&n->dZ[l], (size_t)rows * kHid) &&
+             n->alloc(&n->dZT[l], (size_t)rows * kHid);
+    if (!ok) {
+        fprintf(stderr, "pokerrust_b200: value network: allocation failed\n");
+        delete n;
+        return nullptr;
+    }
+    // He-uniform weights on the live block, zero biases
+    uint64_t st = seed * 0x2545F4914F6CDD1Dull + 1;
+    for (int l = 0; l < kLayers; l++) {
+        std::vector<float> w((size_t)kN[l] * kK[l], 0.0f);
+        const float bound = sqrtf(6.0f / (float)kKLive[l]) * (l == kLayers - 1 ? 0.5f : 1.0f);
+        for (int r = 0; r < kNLive[l]; r++)
+            for (int c = 0; c < kKLive[l]; c++) {
+                const double u = (double)(splitmix(st) >> 11) / 9007199254740992.0;
+                w[(size_t)r * kK[l] + c] = (float)((2.0 * u - 1.0) * bound);
+            }
+        if (cudaMemcpyAsync(n->W[l], w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, n->stream) !=
+            cudaSuccess) {
+            delete n;
+            return nullptr;
+        }
+        cudaStreamSynchronize(n->stream);
+    }
+    if (n->refresh_copies() || cudaStreamSynchronize(n->stream) != cudaSuccess) {
+        delete n;
+        return nullptr;
+    }
+    return n;
+}
+
+void pr_mlp_free(void *net) { delete (Net *)net; }
+
+int pr_mlp_rows(void *net) { return net ? ((Net *)net)->rows : 0; }
+
+namespace {
+int load_inputs(Net *n, const float *ranges, const unsigned long long *boards, const float *scalars, int count) {
+    if (count < 1 || count > n->rows) return 2;
+    assemble_kernel<<<n->rows, 256, 0, n->stream>>>(ranges, boards, scalars, n->X, count);
+    return n->check(cudaGetLastError(), "inputs");
+}
+int finish(Net *n) {
+    int err = 0;
+    cudaError_t e = cudaStreamSynchronize(n->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(&err, n->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return n->check(e, "pass");
+    if (err) {
+        fprintf(stderr, "pokerrust_b200: value network: a GEMM wait timed out (bits %d)\n", err);
+        return 1;
+    }
+    return 0;
+}
+}  // namespace
+
+// Inference: inputs on the device (ranges [count][2][1326], boards [count] (4-card masks),
+// scalars [count][2]); out [count][2652] on the device. count <= rows.
+int pr_mlp_forward(void *net, const float *ranges, const uint64_t *boards, const float *scalars, float *out,
+                   int count) {
+    Net *n = (Net *)net;
+    if (!n || !ranges || !boards || !scalars || !out) return 2;
+    if (int st = load_inputs(n, ranges, (const unsigned long long *)boards, scalars, count)) return st;
+    if (int st = n->forward()) return st;
+    copy_out_kernel<<<count, 256, 0, n->stream>>>(n->Y, out, count);
+    return finish(n);
+}
+
+// One training step on `count` samples (targets [count][2652] on the device): forward, MSE
+// loss, backward, Adam (lr). loss: mean squared error before the update.
+int pr_mlp_train_step(void *net, const float *ranges, const uint64_t *boards, const float *scalars,
+                      const float *targets, int count, float lr, double *loss) {
+    Net *n = (Net *)net;
+    if (!n || !ranges || !boards || !scalars || !targets) return 2;
+    if (int st = load_inputs(n, ranges, (const unsigned long long *)boards, scalars, count)) return st;
+    if (int st = n->forward()) return st;
+    loss_kernel<<<n->rows, 256, 0, n->stream>>>(n->Y, targets, n->dY, n->partial, count, n->rows);
+    if (int st = n->backward()) return st;
+    if (lr > 0.0f)
+        if (int st = n->adam(lr)) return st;
+    if (int st = finish(n)) return st;
+    if (loss) {
+        std::vector<double> p(n->rows);
+        cudaMemcpy(p.data(), n->partial, sizeof(double) * n->rows, cudaMemcpyDeviceToHost);
+        double s = 0;
+        for (int i = 0; i < count; i++) s += p[i];
+        *loss = s / ((double)count * kOut);
+    }
+    return 0;
+}
+
+// Layer l's live parameters (host f32): W [n_live][k_live] (fan-out x fan-in), b [n_live];
+// the gradients of the last training step in the same layout.
+int pr_mlp_layer_shape(int l, int *fan_out, int *fan_in) {
+    if (l < 0 || l >= kLayers) return 2;
+    *fan_out = kNLive[l];
+    *fan_in = kKLive[l];
+    return 0;
+}
+
+namespace {
+int layer_io(Net *n, int l, float *dev_w, float *dev_b, float *W, float *bias, bool to_host) {
+    if (!n || l < 0 || l >= kLayers) return 2;
+    cudaStreamSynchronize(n->stream);
+    const int rows = kNLive[l], cols = kKLive[l];
+    cudaError_t e = cudaSuccess;
+    if (W) {
+        if (to_host)
+            e = cudaMemcpy2D(W, cols * sizeof(float), dev_w, kK[l] * sizeof(float), cols * sizeof(float), rows,
+                             cudaMemcpyDeviceToHost);
+        else
+            e = cudaMemcpy2D(dev_w, kK[l] * sizeof(float), W, cols * sizeof(float), cols * sizeof(float), rows,
+                             cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess && bias)
+        e = to_host ? cudaMemcpy(bias, dev_b, rows * sizeof(float), cudaMemcpyDeviceToHost)
+                    : cudaMemcpy(dev_b, bias, rows * sizeof(float), cudaMemcpyHostToDevice);
+    return n->check(e, "parameter copy");
+}
+}  // namespace
+
+int pr_mlp_get_layer(void *net, int l, float *W, float *bias) {
+    Net *n = (Net *)net;
+    return n ? layer_io(n, l, n->W[l], n->b[l], W, bias, true) : 2;
+}
+
+int pr_mlp_set_layer(void *net, int l, const float *W, const float *bias) {
+    Net *n = (Net *)net;
+    if (!n) return 2;
+    if (int st = layer_io(n, l, n->W[l], n->b[l], const_cast<float *>(W), const_cast<float *>(bias), false))
+        return st;
+    if (int st = n->refresh_copies()) return st;
+    return finish(n);
+}
+
+int pr_mlp_get_grad(void *net, int l, float *dW, float *dbias) {
+    Net *n = (Net *)net;
+    return n ? layer_io(n, l, n->dW[l], n->db[l], dW, dbias, true) : 2;
+}
+
+}  // extern "C"

@@ -1,0 +1,77 @@
+// Host launchers of the tcgen05 BF16 GEMM (mlp_gemm.cuh) and its epilogues.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include "mlp_gemm.cuh"
+#include "mlp_gemm.h"
+
+namespace prb {
+namespace gemm {
+
+// D (f32, leading dimension ldd) = accumulator, rows < rows_live and columns < cols_live.
+struct EpiF32 {
+    float *D;
+    int ldd, rows_live, cols_live;
+    template <class R, class P>
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+#pragma unroll
+        for (int i = 0; i < size(reg); i++) {
+            const int m = m0 + get<0>(pos(i)), n = n0 + get<1>(pos(i));
+            if (m < rows_live && n < cols_live) D[(size_t)m * ldd + n] = reg(i);
+        }
+    }
+};
+
+}  // namespace gemm
+
+cudaError_t gemm_bf16_f32(const void *A, const void *B, float *D, int M, int N, int K, int ldd, int rows_live,
+                          int cols_live, int bn, int *err, cudaStream_t stream) {
+    gemm::EpiF32 epi{D, ldd, rows_live, cols_live};
+    const gemm::bf16 *a = reinterpret_cast<const gemm::bf16 *>(A);
+    const gemm::bf16 *b = reinterpret_cast<const gemm::bf16 *>(B);
+    if (bn == 256) return gemm::run<256>(a, b, M, N, K, epi, err, stream);
+    if (bn == 128) return gemm::run<128>(a, b, M, N, K, epi, err, stream);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace prb
+
+extern "C" {
+
+// D[M][N] (f32) = A[M][K] . B[N][K]^T on the tensor cores, device pointers, synchronous.
+// Returns 0, 2 for bad shapes, or 1 with the kernel's error bits printed on a timed-out wait.
+int pr_gemm_bf16(const void *A, const void *B, float *D, int M, int N, int K, int bn, void *stream) {
+    int *d_err = nullptr;
+    cudaError_t e = cudaMalloc(&d_err, sizeof(int));
+    if (e != cudaSuccess) return 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaMemsetAsync(d_err, 0, sizeof(int), s);
+    e = prb::gemm_bf16_f32(A, B, D, M, N, K, N, M, N, bn, d_err, s);
+    if (e == cudaErrorInvalidValue) {
+        cudaFree(d_err);
+        return 2;
+    }
+    int err = 0;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d_err);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "pokerrust_b200: gemm: %s\n", cudaGetErrorString(e));
+        return 1;
+    }
+    if (err) {
+        fprintf(stderr, "pokerrust_b200: gemm: a wait timed out (error bits %d)\n", err);
+        return 1;
+    }
+    return 0;
+}
+
+// The same product launched asynchronously on `stream`; err: a device int that collects the
+// kernel's error bits (timed-out waits). 0 or 2 (bad shapes) or 1 (launch error).
+int pr_gemm_bf16_async(const void *A, const void *B, float *D, int M, int N, int K, int bn, int *err,
+                       void *stream) {
+    const cudaError_t e = prb::gemm_bf16_f32(A, B, D, M, N, K, N, M, N, bn, err, (cudaStream_t)stream);
+    return e == cudaSuccess ? 0 : (e == cudaErrorInvalidValue ? 2 : 1);
+}
+
+}  // extern "C"

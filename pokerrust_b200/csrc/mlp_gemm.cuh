@@ -1,0 +1,260 @@
+// BF16 GEMM on the 5th-generation tensor cores (tcgen05) for the turn-leaf value network:
+// D[M][N] = A[M][K] . B[N][K]^T with FP32 accumulation in tensor memory, A and B K-major
+// (row-major with K contiguous), fused element-wise epilogues.
+//
+// One CTA computes one 128 x BN tile. Warp 0 (one thread) streams 128 x 64 / BN x 64 tiles
+// of A and B into shared memory with TMA (128-byte swizzle, STAGES-deep ring, no
+// multicast); warp 1 (one thread) issues tcgen05.mma (M = 128, N = BN, K = 16 per
+// instruction) into a TMEM accumulator and frees each stage with tcgen05.commit; then the
+// four warps read the accumulator rows back with tcgen05.ld (warp w owns TMEM lanes
+// 32w..32w+31) and run the epilogue. Every mbarrier wait is bounded: on time-out the kernel
+// records an error, waits (bounded) for its copies and MMAs in flight, frees TMEM and
+// returns.
+//
+// The layouts, descriptors and TMA boxes come from CuTe's sm100 atoms
+// (SM100_MMA_F16BF16_SS, UMMA::Layout_K_SW128_Atom, make_tma_atom_A/B_sm100 with the
+// non-multicast SM90_TMA_LOAD, SM100_TMEM_LOAD_32dp32b*).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cutlass/cutlass.h>
+#include <cute/tensor.hpp>
+#include <cute/arch/tmem_allocator_sm100.hpp>
+#include <cute/atom/copy_atom.hpp>
+#include <cute/atom/mma_atom.hpp>
+#include <cutlass/arch/barrier.h>
+#include <cutlass/numeric_types.h>
+
+namespace prb {
+namespace gemm {
+
+using namespace cute;
+using bf16 = cutlass::bfloat16_t;
+
+constexpr int kBM = 128;
+constexpr int kBK = 64;
+constexpr int kStages = 4;
+constexpr int kThreads = 128;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // give up on an mbarrier after 2 s
+
+template <int BN>
+struct Cfg {
+    using TiledMma = decltype(make_tiled_mma(SM100_MMA_F16BF16_SS<bf16, bf16, float, kBM, BN, UMMA::Major::K,
+                                                                  UMMA::Major::K>{}));
+    using Tiler = Shape<Int<kBM>, Int<BN>, Int<kBK>>;
+    using ShapeA = decltype(partition_shape_A(TiledMma{}, make_shape(Int<kBM>{}, Int<kBK>{})));
+    using ShapeB = decltype(partition_shape_B(TiledMma{}, make_shape(Int<BN>{}, Int<kBK>{})));
+    using SmemA = decltype(UMMA::tile_to_mma_shape(UMMA::Layout_K_SW128_Atom<bf16>{},
+                                                   append(ShapeA{}, Int<kStages>{})));
+    using SmemB = decltype(UMMA::tile_to_mma_shape(UMMA::Layout_K_SW128_Atom<bf16>{},
+                                                   append(ShapeB{}, Int<kStages>{})));
+    static constexpr int kBytesA = kBM * kBK * 2;
+    static constexpr int kBytesB = BN * kBK * 2;
+
+    struct Shared {
+        alignas(1024) cute::ArrayEngine<bf16, cute::cosize_v<SmemA>> A;
+        alignas(1024) cute::ArrayEngine<bf16, cute::cosize_v<SmemB>> B;
+        alignas(8) uint64_t full[kStages];
+        alignas(8) uint64_t empty[kStages];
+        alignas(8) uint64_t acc;
+        uint32_t tmem_base;
+        int failed;
+    };
+    static constexpr size_t kSmem = sizeof(Shared) + 1024;  // room to align the base to 1024
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for the phase with parity `phase` of an mbarrier; false after kWaitNs of wall time.
+// Each try_wait suspends for at most about a microsecond (its time hint), so the bound holds.
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t phase) {
+    const uint32_t a = cute::cast_smem_ptr_to_uint(bar);
+    unsigned long long start = 0;
+    for (unsigned i = 0;; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(phase), "r"(1000u)
+            : "memory");
+        if (ok) return true;
+        const unsigned long long now = global_ns();
+        if (i == 0) start = now;
+        else if (now - start > kWaitNs) return false;
+    }
+}
+
+__device__ __forceinline__ void tmem_fence_after_sync() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_before_sync() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+// Error bits written to `err` (device int) on a timed-out wait.
+enum : int { kErrProducer = 1, kErrMma = 2, kErrEpilogue = 4 };
+
+template <int BN, class TmaA, class TmaB, class Epi>
+__global__ void __launch_bounds__(kThreads, 1)
+    gemm_kernel(CUTE_GRID_CONSTANT TmaA const tma_a, CUTE_GRID_CONSTANT TmaB const tma_b, int M, int N, int K,
+                Epi epi, int *err) {
+    using C = Cfg<BN>;
+    extern __shared__ char smem_raw[];
+    typename C::Shared &ss = *reinterpret_cast<typename C::Shared *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    const int k_tiles = K / kBK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) {
+            cutlass::arch::ClusterTransactionBarrier::init(&ss.full[s], 1);
+            cutlass::arch::ClusterBarrier::init(&ss.empty[s], 1);
+        }
+        cutlass::arch::ClusterBarrier::init(&ss.acc, 1);
+        ss.failed = 0;
+        cutlass::arch::fence_barrier_init();
+    }
+    if (warp == 1) {
+        cute::TMEM::Allocator1Sm alloc;
+        alloc.allocate(BN, &ss.tmem_base);
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+
+    typename C::TiledMma tiled_mma;
+    ThrMMA cta_mma = tiled_mma.get_slice(0);
+    Tensor mA = tma_a.get_tma_tensor(make_shape(M, K));
+    Tensor mB = tma_b.get_tma_tensor(make_shape(N, K));
+    auto coord = make_coord(blockIdx.x, blockIdx.y, _);
+    Tensor gA = local_tile(mA, typename C::Tiler{}, coord, Step<_1, X, _1>{});  // (BM, BK, k)
+    Tensor gB = local_tile(mB, typename C::Tiler{}, coord, Step<X, _1, _1>{});  // (BN, BK, k)
+    Tensor tCgA = cta_mma.partition_A(gA);
+    Tensor tCgB = cta_mma.partition_B(gB);
+    Tensor sA = make_tensor(make_smem_ptr(ss.A.begin()), typename C::SmemA{});
+    Tensor sB = make_tensor(make_smem_ptr(ss.B.begin()), typename C::SmemB{});
+    auto [tAgA, tAsA] = tma_partition(tma_a, Int<0>{}, Layout<_1>{}, group_modes<0, 3>(sA), group_modes<0, 3>(tCgA));
+    auto [tBgB, tBsB] = tma_partition(tma_b, Int<0>{}, Layout<_1>{}, group_modes<0, 3>(sB), group_modes<0, 3>(tCgB));
+    Tensor tCrA = cta_mma.make_fragment_A(sA);
+    Tensor tCrB = cta_mma.make_fragment_B(sB);
+    Tensor cC = make_identity_tensor(make_shape(Int<kBM>{}, Int<BN>{}));
+    Tensor tCcC = cta_mma.partition_C(cC);
+    Tensor tCtAcc = cta_mma.make_fragment_C(tCcC);
+    tCtAcc.data() = ss.tmem_base;
+
+    int issued = 0;
+    if (warp == 0 && lane == 0) {
+        // producer: TMA loads of A and B tiles into the stage ring
+        for (int k = 0; k < k_tiles; k++) {
+            const int s = k % kStages;
+            if (k >= kStages && !bar_wait(&ss.empty[s], ((k / kStages) - 1) & 1)) {
+                atomicOr(err, kErrProducer);
+                ss.failed = 1;
+                break;
+            }
+            cutlass::arch::ClusterTransactionBarrier::arrive_and_expect_tx(&ss.full[s], C::kBytesA + C::kBytesB);
+            copy(tma_a.with(ss.full[s]), tAgA(_, k), tAsA(_, s));
+            copy(tma_b.with(ss.full[s]), tBgB(_, k), tBsB(_, s));
+            issued++;
+        }
+    } else if (warp == 1) {
+        // MMA issuer: one elected thread (inside the atom) per instruction
+        tiled_mma.accumulate_ = UMMA::ScaleOut::Zero;
+        bool ok = true;
+        for (int k = 0; k < k_tiles && ok; k++) {
+            const int s = k % kStages;
+            // warp-uniform decision: the MMA and commit below are warp-collective
+            if (!__all_sync(0xffffffffu, bar_wait(&ss.full[s], (k / kStages) & 1))) {
+                if (lane == 0) atomicOr(err, kErrMma);
+                ok = false;
+                break;
+            }
+            tmem_fence_after_sync();
+#pragma unroll
+            for (int kb = 0; kb < size<2>(tCrA); kb++) {
+                cute::gemm(tiled_mma, tCrA(_, _, kb, s), tCrB(_, _, kb, s), tCtAcc);
+                tiled_mma.accumulate_ = UMMA::ScaleOut::One;
+            }
+            // tcgen05.commit from the lane that issued the MMAs (umma_arrive elects it; the
+            // whole warp calls it)
+            cutlass::arch::umma_arrive(&ss.empty[s]);
+            __syncwarp();
+        }
+        cutlass::arch::umma_arrive(&ss.acc);
+        __syncwarp();
+    }
+
+    __syncwarp();
+
+    // epilogue: all four warps, TMEM rows -> registers -> global, 32 columns at a time
+    const bool acc_ok = __all_sync(0xffffffffu, bar_wait(&ss.acc, 0));  // tcgen05.ld is warp-collective
+    if (!acc_ok && lane == 0) atomicOr(err, kErrEpilogue);
+    tmem_fence_after_sync();
+    if (acc_ok) {
+        Tensor acc = tCtAcc(make_coord(_, _), 0, 0);  // (BM, BN) in TMEM
+        Tensor crd = tCcC(make_coord(_, _), 0, 0);    // (BM, BN) tile coordinates
+        const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
+#pragma unroll 1
+        for (int j = 0; j < BN / 32; j++) {
+            Tensor acc_j = local_tile(acc, Shape<Int<kBM>, _32>{}, make_coord(0, j));
+            Tensor crd_j = local_tile(crd, Shape<Int<kBM>, _32>{}, make_coord(0, j));
+            auto t2r = make_tmem_copy(SM100_TMEM_LOAD_32dp32b32x{}, acc_j);
+            ThrCopy thr = t2r.get_slice(threadIdx.x);
+            Tensor src = thr.partition_S(acc_j);
+            Tensor pos = thr.partition_D(crd_j);
+            Tensor reg = make_tensor<float>(shape(pos));
+            copy(t2r, src, reg);
+            cutlass::arch::fence_view_async_tmem_load();
+            epi(reg, pos, m0, n0);
+        }
+    }
+
+    // teardown: copies and MMAs in flight finish before shared memory and TMEM go away
+    if (warp == 0 && lane == 0 && ss.failed) {
+        // only the last kStages loads can still be in flight (earlier stages were consumed)
+        for (int k = issued > kStages ? issued - kStages : 0; k < issued; k++)
+            bar_wait(&ss.full[k % kStages], (k / kStages) & 1);
+    }
+    if (!acc_ok) bar_wait(&ss.acc, 0);
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 1) {
+        tmem_fence_after_sync();
+        cute::TMEM::Allocator1Sm alloc;
+        alloc.release_allocation_lock();
+        alloc.free(ss.tmem_base, BN);
+    }
+}
+
+// Launches D = A . B^T with epilogue `epi` on `stream` (host side; see gemm_kernel).
+template <int BN, class Epi>
+inline cudaError_t run(const bf16 *A, const bf16 *B, int M, int N, int K, Epi epi, int *err, cudaStream_t stream) {
+    using C = Cfg<BN>;
+    if (M % kBM || N % BN || K % kBK || K <= 0) return cudaErrorInvalidValue;
+    if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) return cudaErrorInvalidValue;
+    Tensor gA = make_tensor(make_gmem_ptr(A), make_shape(M, K), make_stride(K, Int<1>{}));
+    Tensor gB = make_tensor(make_gmem_ptr(B), make_shape(N, K), make_stride(K, Int<1>{}));
+    typename C::TiledMma mma;
+    auto cluster_vmnk = tiled_divide(make_layout(Shape<_1, _1, _1>{}), make_tile(typename C::TiledMma::AtomThrID{}));
+    auto tma_a = make_tma_atom_A_sm100<bf16>(SM90_TMA_LOAD{}, gA, typename C::SmemA{}(_, _, _, 0),
+                                             typename C::Tiler{}, mma, cluster_vmnk);
+    auto tma_b = make_tma_atom_B_sm100<bf16>(SM90_TMA_LOAD{}, gB, typename C::SmemB{}(_, _, _, 0),
+                                             typename C::Tiler{}, mma, cluster_vmnk);
+    auto kernel = gemm_kernel<BN, decltype(tma_a), decltype(tma_b), Epi>;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::kSmem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(M / kBM, N / BN);
+    kernel<<<grid, kThreads, C::kSmem, stream>>>(tma_a, tma_b, M, N, K, epi, err);
+    return cudaGetLastError();
+}
+
+}  // namespace gemm
+}  // namespace prb

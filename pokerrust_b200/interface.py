@@ -123,6 +123,24 @@ def lib():
         L.pr_batch_tune.argtypes = [vp, vp]
         L.pr_batch_iterate_noalloc.restype = i32
         L.pr_batch_iterate_noalloc.argtypes = [vp, i32]
+        L.pr_gemm_bf16.restype = i32
+        L.pr_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, i32, vp]
+        L.pr_gemm_bf16_async.restype = i32
+        L.pr_gemm_bf16_async.argtypes = [vp, vp, vp, i32, i32, i32, i32, vp, vp]
+        L.pr_mlp_new.restype = vp
+        L.pr_mlp_new.argtypes = [i32, u64]
+        L.pr_mlp_free.argtypes = [vp]
+        L.pr_mlp_rows.restype = i32
+        L.pr_mlp_rows.argtypes = [vp]
+        L.pr_mlp_forward.restype = i32
+        L.pr_mlp_forward.argtypes = [vp, vp, vp, vp, vp, i32]
+        L.pr_mlp_train_step.restype = i32
+        L.pr_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, i32, f32, vp]
+        L.pr_mlp_layer_shape.restype = i32
+        L.pr_mlp_layer_shape.argtypes = [i32, vp, vp]
+        for name in ("pr_mlp_get_layer", "pr_mlp_set_layer", "pr_mlp_get_grad"):
+            getattr(L, name).restype = i32
+            getattr(L, name).argtypes = [vp, i32, vp, vp]
         L.pr_batch_value.restype = i32
         L.pr_batch_value.argtypes = [vp, i32, vp]
         L.pr_batch_value_grad.restype = i32
@@ -602,6 +620,73 @@ class Batch:
     def close(self):
         if self.ptr:
             lib().pr_batch_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- turn-leaf value network ----
+
+class ValueNet:
+    """The turn-leaf value network (pr_mlp_*): 2706 inputs (both ranges, the 4 turn cards,
+    pot / 200 and stack / (10 pot)) -> 4 x 1024 GELU -> 2652 outputs (both players'
+    counterfactual values per hand over the pot), BF16 tcgen05 GEMMs with FP32 accumulation,
+    trained with MSE and Adam. Inputs and targets are device tensors (torch)."""
+
+    LAYERS = 5
+
+    def __init__(self, rows=4096, seed=0):
+        self.rows = rows
+        self.ptr = lib().pr_mlp_new(int(rows), int(seed))
+        if not self.ptr:
+            raise PokerLibError("pr_mlp_new failed")
+
+    @staticmethod
+    def layer_shape(l):
+        o, i = ctypes.c_int(), ctypes.c_int()
+        _check(lib().pr_mlp_layer_shape(int(l), ctypes.byref(o), ctypes.byref(i)), "pr_mlp_layer_shape")
+        return o.value, i.value
+
+    def forward(self, ranges, boards, scalars, out):
+        """ranges [n][2][1326] f32, boards [n] int64 (4-card masks), scalars [n][2] f32,
+        out [n][2652] f32: device tensors, n <= rows."""
+        n = int(boards.shape[0])
+        _check(lib().pr_mlp_forward(self.ptr, ranges.data_ptr(), boards.data_ptr(), scalars.data_ptr(),
+                                    out.data_ptr(), n), "pr_mlp_forward")
+
+    def train_step(self, ranges, boards, scalars, targets, lr):
+        loss = ctypes.c_double()
+        n = int(boards.shape[0])
+        _check(lib().pr_mlp_train_step(self.ptr, ranges.data_ptr(), boards.data_ptr(), scalars.data_ptr(),
+                                       targets.data_ptr(), n, float(lr), ctypes.byref(loss)), "pr_mlp_train_step")
+        return loss.value
+
+    def layer(self, l):
+        o, i = self.layer_shape(l)
+        W = np.zeros((o, i), np.float32)
+        b = np.zeros(o, np.float32)
+        _check(lib().pr_mlp_get_layer(self.ptr, int(l), _ptr(W), _ptr(b)), "pr_mlp_get_layer")
+        return W, b
+
+    def set_layer(self, l, W, b):
+        W = np.ascontiguousarray(W, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        _check(lib().pr_mlp_set_layer(self.ptr, int(l), _ptr(W), _ptr(b)), "pr_mlp_set_layer")
+
+    def grad(self, l):
+        o, i = self.layer_shape(l)
+        W = np.zeros((o, i), np.float32)
+        b = np.zeros(o, np.float32)
+        _check(lib().pr_mlp_get_grad(self.ptr, int(l), _ptr(W), _ptr(b)), "pr_mlp_get_grad")
+        return W, b
+
+    def close(self):
+        if self.ptr:
+            lib().pr_mlp_free(self.ptr)
             self.ptr = None
 
     def __del__(self):

@@ -1,0 +1,34 @@
+"""The tcgen05 BF16 GEMM (pr_gemm_bf16) against an FP32 product of the same BF16 operands.
+
+Products of two bf16 values are exact in f32, so the only difference is the order of the
+f32 sums: 1e-5 of the output's scale."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("M,N,K,bn", [(128, 128, 64, 128), (128, 256, 64, 256), (256, 512, 320, 256),
+                                      (384, 384, 1024, 128), (1024, 1024, 2752, 256)])
+def test_gemm_matches_fp32(M, N, K, bn):
+    import torch
+    import pokerrust_b200 as P
+    g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 3 + K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    D = torch.full((M, N), float("nan"), device="cuda", dtype=torch.float32)
+    torch.cuda.synchronize()
+    st = P.lib().pr_gemm_bf16(A.data_ptr(), B.data_ptr(), D.data_ptr(), M, N, K, bn, None)
+    assert st == 0
+    want = A.float() @ B.float().T
+    err = (D - want).abs().max().item()
+    assert err <= 1e-5 * want.abs().max().item(), err
+
+
+def test_gemm_rejects_bad_shapes():
+    import torch
+    import pokerrust_b200 as P
+    A = torch.zeros(100, 64, device="cuda", dtype=torch.bfloat16)
+    B = torch.zeros(128, 64, device="cuda", dtype=torch.bfloat16)
+    D = torch.zeros(100, 128, device="cuda")
+    assert P.lib().pr_gemm_bf16(A.data_ptr(), B.data_ptr(), D.data_ptr(), 100, 128, 64, 128, None) == 2
