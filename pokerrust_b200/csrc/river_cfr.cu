@@ -53,6 +53,10 @@ constexpr int kFoldCol = 12;
 constexpr int kOutPer = 3;             // output phase: hands per lane, in bucket order
 constexpr int kOutWarps = 12;          // 12 * 32 * 3 >= 1081
 constexpr int kRowW = 12;              // group rows: 9 showdown channels padded to 16-byte loads
+// Card sums of the fold channels are kept in 8 copies, 16-byte chunk c of card k of copy p at
+// chunk index (k * chunks + c) * 8 + p: lane position p of a quarter warp reads copy p, which
+// lies in bank group p, so the per-hand card lookups never conflict.
+constexpr int kCfCopies = 8;
 
 // Byte offsets of the shared-memory arrays; computed the same way on host and device.
 struct Layout {
@@ -80,7 +84,7 @@ __host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned gr
     L.r = take(&o, kRangeStride * vb);
     L.own = acc > kNumLeaves ? take(&o, kRangeStride * 4) : 0;
     L.out = take(&o, kRangeStride * vb);
-    L.Cf = take(&o, 52 * kNumFold * vb);
+    L.Cf = take(&o, 52 * kNumFold * vb * kCfCopies);
     L.Tf = take(&o, kNumFold * vb);
     L.Tsd = take(&o, kNumSD * vb);
     L.gwarp = take(&o, 4 * kNumLeaves * vb);
@@ -102,7 +106,7 @@ struct Smem {
     V *r;                        // opponent range of the subgame
     float *own;                  // updater's own range (average strategies only)
     V *out;                      // updater's value, summed over rivers
-    V (*Cf)[kNumFold];           // card sums, fold channels
+    V *Cf;                       // card sums, fold channels (kCfCopies interleaved copies)
     V *Tf;                       // totals, fold channels
     V *Tsd;                      // totals, showdown channels
     V (*gwarp)[kNumLeaves];      // rank-list warp totals
@@ -120,7 +124,7 @@ struct Smem {
           r(reinterpret_cast<V *>(base + L.r)),
           own(reinterpret_cast<float *>(base + L.own)),
           out(reinterpret_cast<V *>(base + L.out)),
-          Cf(reinterpret_cast<V(*)[kNumFold]>(base + L.Cf)),
+          Cf(reinterpret_cast<V *>(base + L.Cf)),
           Tf(reinterpret_cast<V *>(base + L.Tf)),
           Tsd(reinterpret_cast<V *>(base + L.Tsd)),
           gwarp(reinterpret_cast<V(*)[kNumLeaves]>(base + L.gwarp)),
@@ -167,6 +171,16 @@ __device__ __forceinline__ void elem_x(const Smem<V, ACC> &S, uint32_t e, V x[kN
     for (int f = 0; f < kNumFold; f++) x[kNumSD + f] = rh * row[kFoldCol + f];
 }
 
+// The fold-channel card sums of `card` from this lane's copy (see kCfCopies).
+template <typename V>
+__device__ __forceinline__ void cf_row(const V *cf, int card, V out[kNumFold]) {
+    constexpr int kPer = 16 / sizeof(V), kChunks = kNumFold / kPer;
+    const int p = threadIdx.x & 7;
+#pragma unroll
+    for (int c = 0; c < kChunks; c++)
+        load_row(cf + ((size_t)(card * kChunks + c) * kCfCopies + p) * kPer, out + c * kPer, kPer);
+}
+
 // Leaf values (before the leaf's bet/sign scale) of live hand l for all 17 channels:
 // showdowns from the group values of the scans, folds from totals and card sums.
 template <typename V, int ACC>
@@ -187,10 +201,12 @@ __device__ __forceinline__ int hand_values(const Smem<V, ACC> &S, const BoardPac
     const V rh = S.r[h];
     V xf[kNumFold], ca[kNumFold], cb[kNumFold];
     load_row(S.pio[b] + kFoldCol, xf, kNumFold);
-    load_row(S.Cf[c1], ca, kNumFold);
-    load_row(S.Cf[c2], cb, kNumFold);
+    cf_row(S.Cf, c1, ca);
+    cf_row(S.Cf, c2, cb);
+    V tf[kNumFold];
+    load_row(S.Tf, tf, kNumFold);
 #pragma unroll
-    for (int f = 0; f < kNumFold; f++) v[kNumSD + f] = S.Tf[f] - ca[f] - cb[f] + rh * xf[f];
+    for (int f = 0; f < kNumFold; f++) v[kNumSD + f] = tf[f] - ca[f] - cb[f] + rh * xf[f];
     return h;
 }
 
@@ -427,10 +443,22 @@ __global__ void __launch_bounds__(NT, 1)
                     if (sl >= off) inc[c] += t;
                 }
             }
-            if (active && sl == 7) {
-                const int card = pk->list_card[li];
+            {
+                // the list total of each fold channel, written by the list's 8 lanes, lane sl
+                // into copy sl
+                V cf[kNumFold];
 #pragma unroll
-                for (int f = 0; f < kNumFold; f++) S.Cf[card][f] = inc[kNumSD + f];
+                for (int f = 0; f < kNumFold; f++) cf[f] = __shfl_sync(FULL, inc[kNumSD + f], lane | 7);
+                if (active) {
+                    constexpr int kPer = 16 / sizeof(V), kChunks = kNumFold / kPer;
+                    const int card = pk->list_card[li];
+#pragma unroll
+                    for (int c = 0; c < kChunks; c++) {
+                        V *dst = S.Cf + ((size_t)(card * kChunks + c) * kCfCopies + sl) * kPer;
+#pragma unroll
+                        for (int q = 0; q < kPer; q++) dst[q] = cf[c * kPer + q];
+                    }
+                }
             }
             V run[kNumSD], Tc[kNumSD];
 #pragma unroll
