@@ -37,12 +37,70 @@ __device__ __forceinline__ float gelu_grad(float z) {
 }
 
 // ---- GEMM epilogues (called with 32 accumulator values of one row per thread) ----
+// When a thread's 32 values are 32 consecutive columns of one row (the tcgen05.ld
+// 32dp32b32x layout), the epilogues move them with 16-byte loads and stores.
+template <class P>
+__device__ __forceinline__ bool row_run(P const &pos, int *m, int *n) {
+    *m = cute::get<0>(pos(0));
+    *n = cute::get<1>(pos(0));
+    bool ok = true;
+#pragma unroll
+    for (int i = 1; i < 32; i++) ok &= cute::get<0>(pos(i)) == *m && cute::get<1>(pos(i)) == *n + i;
+    return ok;
+}
+
+__device__ __forceinline__ uint4 pack8(const float *v) {
+    uint4 u;
+    uint32_t w[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const bf16 lo(v[2 * k]), hi(v[2 * k + 1]);
+        w[k] = (uint32_t)lo.raw() | ((uint32_t)hi.raw() << 16);
+    }
+    u.x = w[0];
+    u.y = w[1];
+    u.z = w[2];
+    u.w = w[3];
+    return u;
+}
+
+__device__ __forceinline__ void unpack8(uint4 u, float *v) {
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        v[2 * k] = float(bf16::bitcast((uint16_t)(w[k] & 0xFFFF)));
+        v[2 * k + 1] = float(bf16::bitcast((uint16_t)(w[k] >> 16)));
+    }
+}
 struct EpiBiasGelu {  // Z = acc + b, H = gelu(Z), both bf16
     const float *bias;
     bf16 *Z, *H;
     int ld;
     template <class R, class P>
-    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0, int) const {
+        int mr, nr;
+        if (cute::size(reg) == 32 && row_run(pos, &mr, &nr)) {
+            const int m = m0 + mr, n = n0 + nr;
+            float z[32], h[32];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const float4 bq = *reinterpret_cast<const float4 *>(bias + n + 4 * q);
+                z[4 * q] = reg(4 * q) + bq.x;
+                z[4 * q + 1] = reg(4 * q + 1) + bq.y;
+                z[4 * q + 2] = reg(4 * q + 2) + bq.z;
+                z[4 * q + 3] = reg(4 * q + 3) + bq.w;
+            }
+#pragma unroll
+            for (int i = 0; i < 32; i++) h[i] = gelu(z[i]);
+            uint4 *zo = reinterpret_cast<uint4 *>(Z + (size_t)m * ld + n);
+            uint4 *ho = reinterpret_cast<uint4 *>(H + (size_t)m * ld + n);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                zo[q] = pack8(z + 8 * q);
+                ho[q] = pack8(h + 8 * q);
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < cute::size(reg); i++) {
             const int m = m0 + cute::get<0>(pos(i)), n = n0 + cute::get<1>(pos(i));
@@ -57,7 +115,19 @@ struct EpiBiasF32 {  // Y = acc + b (f32)
     float *Y;
     int ld;
     template <class R, class P>
-    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0, int) const {
+        int mr, nr;
+        if (cute::size(reg) == 32 && row_run(pos, &mr, &nr)) {
+            const int m = m0 + mr, n = n0 + nr;
+            float4 *yo = reinterpret_cast<float4 *>(Y + (size_t)m * ld + n);
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const float4 bq = *reinterpret_cast<const float4 *>(bias + n + 4 * q);
+                yo[q] = make_float4(reg(4 * q) + bq.x, reg(4 * q + 1) + bq.y, reg(4 * q + 2) + bq.z,
+                                    reg(4 * q + 3) + bq.w);
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < cute::size(reg); i++) {
             const int m = m0 + cute::get<0>(pos(i)), n = n0 + cute::get<1>(pos(i));
@@ -70,7 +140,22 @@ struct EpiGeluGrad {  // dZ = acc * gelu'(Z), bf16
     bf16 *dZ;
     int ld;
     template <class R, class P>
-    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0, int) const {
+        int mr, nr;
+        if (cute::size(reg) == 32 && row_run(pos, &mr, &nr)) {
+            const size_t at = (size_t)(m0 + mr) * ld + (n0 + nr);
+            const uint4 *zi = reinterpret_cast<const uint4 *>(Z + at);
+            uint4 *dzo = reinterpret_cast<uint4 *>(dZ + at);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                float z[8], g[8];
+                unpack8(zi[q], z);
+#pragma unroll
+                for (int i = 0; i < 8; i++) g[i] = reg(8 * q + i) * gelu_grad(z[i]);
+                dzo[q] = pack8(g);
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < cute::size(reg); i++) {
             const int m = m0 + cute::get<0>(pos(i)), n = n0 + cute::get<1>(pos(i));
@@ -79,11 +164,20 @@ struct EpiGeluGrad {  // dZ = acc * gelu'(Z), bf16
         }
     }
 };
-struct EpiStore {  // D = acc (f32)
+struct EpiStore {  // D = acc (f32); split-K part z goes to D + z * zstride
     float *D;
     int ld;
+    size_t zstride;
     template <class R, class P>
-    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0, int z) const {
+        float *D = this->D + (size_t)z * zstride;
+        int mr, nr;
+        if (cute::size(reg) == 32 && row_run(pos, &mr, &nr)) {
+            float4 *o = reinterpret_cast<float4 *>(D + (size_t)(m0 + mr) * ld + (n0 + nr));
+#pragma unroll
+            for (int q = 0; q < 8; q++) o[q] = make_float4(reg(4 * q), reg(4 * q + 1), reg(4 * q + 2), reg(4 * q + 3));
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < cute::size(reg); i++) {
             const int m = m0 + cute::get<0>(pos(i)), n = n0 + cute::get<1>(pos(i));
@@ -183,6 +277,21 @@ __global__ void adam_kernel(float *__restrict__ w, float *__restrict__ m1, float
     }
 }
 
+// dW = sum of the split-K parts, in part order
+__global__ void split_sum_kernel(const float *__restrict__ parts, float *__restrict__ out, size_t n, int splits) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n / 4; i += (size_t)gridDim.x * blockDim.x) {
+        float4 acc = reinterpret_cast<const float4 *>(parts)[i];
+        for (int z = 1; z < splits; z++) {
+            const float4 v = reinterpret_cast<const float4 *>(parts + (size_t)z * n)[i];
+            acc.x += v.x;
+            acc.y += v.y;
+            acc.z += v.z;
+            acc.w += v.w;
+        }
+        reinterpret_cast<float4 *>(out)[i] = acc;
+    }
+}
+
 __global__ void to_bf16_kernel(const float *__restrict__ w, bf16 *__restrict__ wb, size_t total) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
         wb[i] = bf16(w[i]);
@@ -208,7 +317,10 @@ struct Net {
     float *Y = nullptr;
     bf16 *dY = nullptr, *dYT = nullptr;
     double *partial = nullptr;
+    float *parts = nullptr;  // split-K partial products of the weight gradients
     int step = 0;
+    static constexpr int kSplits = 4;
+    static constexpr size_t kPartsMax = (size_t)kOutPad * kInPad;  // largest weight matrix
     std::vector<void *> owned;
 
     template <class T>
@@ -250,16 +362,24 @@ struct Net {
         transpose_kernel<<<grid, block, 0, stream>>>(in, out, r, c);
     }
 
+    // dW[M][N] = G^T-rows . In^T-rows^T over the batch, as kSplits split-K GEMMs summed in
+    // part order (the weight-gradient GEMMs have few output tiles)
+    cudaError_t weight_grad(const bf16 *GT, const bf16 *InT, int M, int N, float *dWout) {
+        const size_t n = (size_t)M * N;
+        EpiStore epi{parts, N, n};
+        cudaError_t e = gemm::run<256>(GT, InT, M, N, rows, epi, d_err, stream, kSplits);
+        if (e != cudaSuccess) return e;
+        split_sum_kernel<<<592, 256, 0, stream>>>(parts, dWout, n, kSplits);
+        return cudaGetLastError();
+    }
+
     // backward from dY (bf16), gradients into dW / db
     int backward() {
         cudaError_t e = cudaSuccess;
         transpose(dY, dYT, rows, kOutPad);
         // output layer
         transpose(H[3], HT[3], rows, kHid);
-        {
-            EpiStore epi{dW[4], kHid};
-            e = gemm::run<256>(dYT, HT[3], kOutPad, kHid, rows, epi, d_err, stream);
-        }
+        e = weight_grad(dYT, HT[3], kOutPad, kHid, dW[4]);
         bias_grad_kernel<<<(kOutPad * 32 + 255) / 256, 256, 0, stream>>>(dYT, db[4], kOutPad, rows);
         if (e == cudaSuccess) {
             EpiGeluGrad epi{Z[3], dZ[3], kHid};
@@ -270,8 +390,7 @@ struct Net {
             const bf16 *inT = l > 0 ? HT[l - 1] : XT;
             if (l > 0) transpose(H[l - 1], HT[l - 1], rows, kHid);
             else transpose(X, XT, rows, kInPad);
-            EpiStore epi{dW[l], kK[l]};
-            e = gemm::run<256>(dZT[l], inT, kHid, kK[l], rows, epi, d_err, stream);
+            e = weight_grad(dZT[l], inT, kHid, kK[l], dW[l]);
             bias_grad_kernel<<<(kHid * 32 + 255) / 256, 256, 0, stream>>>(dZT[l], db[l], kHid, rows);
             if (e == cudaSuccess && l > 0) {
                 EpiGeluGrad epi2{Z[l - 1], dZ[l - 1], kHid};
@@ -335,7 +454,8 @@ void *pr_mlp_new(int rows, uint64_t seed) {
     }
     ok = ok && n->alloc(&n->X, (size_t)rows * kInPad) && n->alloc(&n->XT, (size_t)rows * kInPad) &&
          n->alloc(&n->Y, (size_t)rows * kOutPad) && n->alloc(&n->dY, (size_t)rows * kOutPad) &&
-         n->alloc(&n->dYT, (size_t)rows * kOutPad) && n->alloc(&n->partial, rows);
+         n->alloc(&n->dYT, (size_t)rows * kOutPad) && n->alloc(&n->partial, rows) &&
+         n->alloc(&n->parts, Net::kSplits * Net::kPartsMax);
     for (int l = 0; l < 4 && ok; l++)
         ok = n->alloc(&n->Z[l], (size_t)rows * kHid) && n->alloc(&n->H[l], (size_t)rows * kHid) &&
              n->alloc(&n->HT[l], (size_t)rows * kHid) && n->alloc(&n->dZ[l], (size_t)rows * kHid) &&

@@ -13,7 +13,7 @@ struct EpiF32 {
     float *D;
     int ldd, rows_live, cols_live;
     template <class R, class P>
-    __device__ void operator()(R const &reg, P const &pos, int m0, int n0) const {
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0, int) const {
 #pragma unroll
         for (int i = 0; i < size(reg); i++) {
             const int m = m0 + get<0>(pos(i)), n = n0 + get<1>(pos(i));

@@ -111,7 +111,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x % 32;
-    const int k_tiles = K / kBK;
+    // split-K: CTA z of gridDim.z covers k tiles [k_begin, k_begin + k_tiles)
+    const int k_all = K / kBK;
+    const int k_begin = (int)(((long long)k_all * blockIdx.z) / gridDim.z);
+    const int k_tiles = (int)(((long long)k_all * (blockIdx.z + 1)) / gridDim.z) - k_begin;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; s++) {
@@ -161,8 +164,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 break;
             }
             cutlass::arch::ClusterTransactionBarrier::arrive_and_expect_tx(&ss.full[s], C::kBytesA + C::kBytesB);
-            copy(tma_a.with(ss.full[s]), tAgA(_, k), tAsA(_, s));
-            copy(tma_b.with(ss.full[s]), tBgB(_, k), tBsB(_, s));
+            copy(tma_a.with(ss.full[s]), tAgA(_, k_begin + k), tAsA(_, s));
+            copy(tma_b.with(ss.full[s]), tBgB(_, k_begin + k), tBsB(_, s));
             issued++;
         }
     } else if (warp == 1) {
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             Tensor reg = make_tensor<float>(shape(pos));
             copy(t2r, src, reg);
             cutlass::arch::fence_view_async_tmem_load();
-            epi(reg, pos, m0, n0);
+            epi(reg, pos, m0, n0, (int)blockIdx.z);
         }
     }
 
@@ -236,9 +239,10 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // Launches D = A . B^T with epilogue `epi` on `stream` (host side; see gemm_kernel).
 template <int BN, class Epi>
-inline cudaError_t run(const bf16 *A, const bf16 *B, int M, int N, int K, Epi epi, int *err, cudaStream_t stream) {
+inline cudaError_t run(const bf16 *A, const bf16 *B, int M, int N, int K, Epi epi, int *err, cudaStream_t stream,
+                       int splits = 1) {
     using C = Cfg<BN>;
-    if (M % kBM || N % BN || K % kBK || K <= 0) return cudaErrorInvalidValue;
+    if (M % kBM || N % BN || K % kBK || K <= 0 || splits < 1 || splits > K / kBK) return cudaErrorInvalidValue;
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) return cudaErrorInvalidValue;
     Tensor gA = make_tensor(make_gmem_ptr(A), make_shape(M, K), make_stride(K, Int<1>{}));
     Tensor gB = make_tensor(make_gmem_ptr(B), make_shape(N, K), make_stride(K, Int<1>{}));
@@ -251,7 +255,7 @@ inline cudaError_t run(const bf16 *A, const bf16 *B, int M, int N, int K, Epi ep
     auto kernel = gemm_kernel<BN, decltype(tma_a), decltype(tma_b), Epi>;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::kSmem);
     if (e != cudaSuccess) return e;
-    dim3 grid(M / kBM, N / BN);
+    dim3 grid(M / kBM, N / BN, splits);
     kernel<<<grid, kThreads, C::kSmem, stream>>>(tma_a, tma_b, M, N, K, epi, err);
     return cudaGetLastError();
 }
