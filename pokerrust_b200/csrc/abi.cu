@@ -5,8 +5,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/pokerrust_b200.h"
@@ -111,6 +113,8 @@ bool river_tree_matches() {
     return true;
 }
 
+constexpr int kPipeChunks = 4;  // chunks of a staged pass (copies overlap the kernel)
+
 struct Builder {
     std::vector<SubgameDesc> desc;
     int capacity = 0;
@@ -131,6 +135,10 @@ struct Builder {
     double *d_results64 = nullptr;
     int cap64 = 0;
     cudaStream_t stream = nullptr;
+    // staged passes are pipelined: ranges of chunk k+1 go up (copy_in) and results of chunk
+    // k-1 come down (copy_out) while the kernel runs chunk k on `stream`
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    cudaEvent_t ev_in[kPipeChunks] = {}, ev_done[kPipeChunks] = {};
     unsigned long long checked_flop = 0;  // boards validated against this flop
     int checked_count = -1;
 };
@@ -287,11 +295,54 @@ int evaluate_impl(Builder *b, EvalTables *t, int player, int exploit, const floa
     const bool avg = (staged || d_own) && b->avg_on && !exploit;
     if (avg) {
         if ((st = sync_average(b))) return st;
-        if (staged) {
+        if (staged && n < 4 * kPipeChunks * 148) {
             e = cudaMemcpyAsync(b->d_own, b->comm_own, (size_t)n * kRangeStride * sizeof(float),
                                 cudaMemcpyHostToDevice, s);
             if (e != cudaSuccess) return fail(kErrCuda, "own range upload", e);
         }
+    }
+    if (staged && n >= 4 * kPipeChunks * 148) {
+        // pipelined: copy-in / kernel / copy-out of kPipeChunks chunks on three streams
+        if (!b->copy_in) {
+            if ((e = cudaStreamCreateWithFlags(&b->copy_in, cudaStreamNonBlocking)) != cudaSuccess ||
+                (e = cudaStreamCreateWithFlags(&b->copy_out, cudaStreamNonBlocking)) != cudaSuccess)
+                return fail(kErrCuda, "stream creation", e);
+            for (int k = 0; k < kPipeChunks; k++)
+                if ((e = cudaEventCreateWithFlags(&b->ev_in[k], cudaEventDisableTiming)) != cudaSuccess ||
+                    (e = cudaEventCreateWithFlags(&b->ev_done[k], cudaEventDisableTiming)) != cudaSuccess)
+                    return fail(kErrCuda, "event creation", e);
+        }
+        // the copies may only start once earlier work on the pass stream is done
+        if ((e = cudaEventRecord(b->ev_done[0], s)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(b->copy_in, b->ev_done[0], 0)) != cudaSuccess)
+            return fail(kErrCuda, "pass ordering", e);
+        for (int k = 0; k < kPipeChunks; k++) {
+            const int lo = (int)((long long)n * k / kPipeChunks), hi = (int)((long long)n * (k + 1) / kPipeChunks);
+            const size_t row0 = (size_t)lo * kRangeStride, rows = (size_t)(hi - lo) * kRangeStride;
+            e = cudaMemcpyAsync(b->d_ranges + row0, b->comm + row0, rows * sizeof(float), cudaMemcpyHostToDevice,
+                                b->copy_in);
+            if (e == cudaSuccess && avg)
+                e = cudaMemcpyAsync(b->d_own + row0, b->comm_own + row0, rows * sizeof(float), cudaMemcpyHostToDevice,
+                                    b->copy_in);
+            if (e == cudaSuccess) e = cudaEventRecord(b->ev_in[k], b->copy_in);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->ev_in[k], 0);
+            if (e != cudaSuccess) return fail(kErrCuda, "range upload", e);
+            e = launch_river(exploit ? kModeBR : kModeCFR, b->d_desc + lo, hi - lo, b->d_ranges + row0,
+                             b->d_results + row0, b->d_regrets + (size_t)lo * kEdges * kBuckets, t->packs, t->flop,
+                             player, t->max_groups, t->max_card_groups, avg ? b->d_own + row0 : nullptr,
+                             avg ? b->d_avg + (size_t)lo * kEdges * kBuckets : nullptr, s);
+            if (e != cudaSuccess) return fail(kErrCuda, "river kernel launch", e);
+            if ((e = cudaEventRecord(b->ev_done[k], s)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(b->copy_out, b->ev_done[k], 0)) != cudaSuccess)
+                return fail(kErrCuda, "pass ordering", e);
+            e = cudaMemcpyAsync(b->comm + row0, b->d_results + row0, rows * sizeof(float), cudaMemcpyDeviceToHost,
+                                b->copy_out);
+            if (e != cudaSuccess) return fail(kErrCuda, "result download", e);
+        }
+        e = cudaStreamSynchronize(b->copy_out);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return fail(kErrCuda, "river pass", e);
+        return kOk;
     }
     if (staged) {
         e = cudaMemcpyAsync(b->d_ranges, b->comm, (size_t)n * kRangeStride * sizeof(float),
@@ -540,12 +591,30 @@ int pr_evaluate_device_own(void *builder, void *eval, int updating_player, const
                          false, d_own);
 }
 
+namespace {
+// Row copies between caller rows of 1326 and staging rows of kRangeStride, split over host
+// threads for large batches (one thread copies ~25 MB/s per row call otherwise idle cores).
+void copy_rows(float *dst, size_t dst_stride, const float *src, size_t src_stride, int count) {
+    auto part = [&](int lo, int hi) {
+        for (int i = lo; i < hi; i++) memcpy(dst + (size_t)i * dst_stride, src + (size_t)i * src_stride, kHands * sizeof(float));
+    };
+    const int threads = count >= 4096 ? (int)std::min<unsigned>(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    if (threads <= 1) {
+        part(0, count);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++)
+        pool.emplace_back(part, (int)((long long)count * t / threads), (int)((long long)count * (t + 1) / threads));
+    for (auto &th : pool) th.join();
+}
+}  // namespace
+
 int pr_upload_batch(void *builder, int first, int count, const float *v) {
     Builder *b = (Builder *)builder;
     if (!b || !v || first < 0 || count < 0 || first + count > (int)b->desc.size())
         return fail(kErrArg, "pr_upload_batch: bad builder or range");
-    for (int i = 0; i < count; i++)
-        memcpy(b->comm + (size_t)(first + i) * kRangeStride, v + (size_t)i * kHands, kHands * sizeof(float));
+    copy_rows(b->comm + (size_t)first * kRangeStride, kRangeStride, v, kHands, count);
     return kOk;
 }
 
@@ -553,8 +622,7 @@ int pr_download_batch(void *builder, int first, int count, float *v) {
     Builder *b = (Builder *)builder;
     if (!b || !v || first < 0 || count < 0 || first + count > (int)b->desc.size())
         return fail(kErrArg, "pr_download_batch: bad builder or range");
-    for (int i = 0; i < count; i++)
-        memcpy(v + (size_t)i * kHands, b->comm + (size_t)(first + i) * kRangeStride, kHands * sizeof(float));
+    copy_rows(v, kHands, b->comm + (size_t)first * kRangeStride, kRangeStride, count);
     return kOk;
 }
 
@@ -648,6 +716,14 @@ void pr_free_builder(void *builder) {
     cudaFree(b->d_avg);
     if (b->comm_own) cudaFreeHost(b->comm_own);
     if (b->comm) cudaFreeHost(b->comm);
+    if (b->copy_in) cudaStreamSynchronize(b->copy_in);
+    if (b->copy_out) cudaStreamSynchronize(b->copy_out);
+    for (int k = 0; k < kPipeChunks; k++) {
+        if (b->ev_in[k]) cudaEventDestroy(b->ev_in[k]);
+        if (b->ev_done[k]) cudaEventDestroy(b->ev_done[k]);
+    }
+    if (b->copy_in) cudaStreamDestroy(b->copy_in);
+    if (b->copy_out) cudaStreamDestroy(b->copy_out);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
