@@ -117,6 +117,13 @@ void *pr_tables_build(uint64_t flop);
  * 2652 collision and 1326 bucket u16 entries); null outputs are skipped. */
 int pr_tables_export(void *eval, uint16_t *eval_out, uint16_t *coll_out, uint16_t *abstr_out);
 
+/* On-disk tables (extension; the reference only sketched a bincode dump, evaluator.rs:43-45,
+ * 148-154): a versioned file with a checksum of the packed eval, collision and bucket
+ * tables. pr_tables_load returns a handle like transfer_flop_eval_cuda's (release with
+ * free_eval_cuda), or null if the file is missing, truncated or corrupted. */
+int pr_tables_save(void *eval, const char *path);
+void *pr_tables_load(const char *path);
+
 /* Status of a table handle: 0, or the bit set of table inconsistencies found on upload. */
 int pr_eval_status(void *eval);
 

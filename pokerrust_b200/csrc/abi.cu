@@ -502,7 +502,8 @@ int build_river_cuda(uint64_t cards, float bet, void *builder) {
 
 void *transfer_flop_eval_cuda(uint64_t flop, const uint64_t *card_order, const uint16_t *card_indexes,
                               const uint16_t *eval, const uint16_t *coll_vec, const uint16_t *abstractions) {
-    (void)coll_vec;  // rebuilt on the device from the sort order
+    // coll_vec is kept for pr_tables_export; the kernels derive the card lists from the
+    // sort order instead of reading it
     EvalTables *t = acquire_tables();
     if (t->status) return t;
     cudaError_t e;
@@ -759,6 +760,83 @@ int pr_tables_export(void *eval, uint16_t *eval_out, uint16_t *coll_out, uint16_
 }
 
 int pr_eval_status(void *eval) { return eval ? ((EvalTables *)eval)->status : -1; }
+
+// ---- table files ---------------------------------------------------------------------
+// Layout (little endian): magic "PRBTABL1" | u32 version (1) | u32 reserved | u64 flop |
+// u64 FNV-1a 64 hash of the three arrays | eval u16[1326 * 1838] | coll u16[1326 * 2652] |
+// buckets u16[1326 * 1326] -- the packed form transfer_flop_eval_cuda takes.
+namespace {
+struct TablesHeader {
+    char magic[8];
+    uint32_t version, reserved;
+    uint64_t flop, hash;
+};
+uint64_t fnv1a64(const void *p, size_t n, uint64_t h) {
+    const unsigned char *c = (const unsigned char *)p;
+    for (size_t i = 0; i < n; i++) h = (h ^ c[i]) * 1099511628211ull;
+    return h;
+}
+}  // namespace
+
+int pr_tables_save(void *eval, const char *path) {
+    EvalTables *t = (EvalTables *)eval;
+    if (!t || t->status || !path) return fail(kErrArg, "pr_tables_save: invalid table handle or path");
+    std::vector<uint16_t> e(kEvalBytes / 2), c(kCollBytes / 2), a(kAbstrBytes / 2);
+    if (int st = pr_tables_export(eval, e.data(), c.data(), a.data())) return st;
+    TablesHeader h{};
+    memcpy(h.magic, "PRBTABL1", 8);
+    h.version = 1;
+    h.flop = t->flop;
+    uint64_t x = 1469598103934665603ull;
+    x = fnv1a64(e.data(), kEvalBytes, x);
+    x = fnv1a64(c.data(), kCollBytes, x);
+    x = fnv1a64(a.data(), kAbstrBytes, x);
+    h.hash = x;
+    FILE *f = fopen(path, "wb");
+    if (!f) return fail(kErrArg, "pr_tables_save: cannot open the file");
+    bool ok = fwrite(&h, sizeof(h), 1, f) == 1 && fwrite(e.data(), 1, kEvalBytes, f) == kEvalBytes &&
+              fwrite(c.data(), 1, kCollBytes, f) == kCollBytes && fwrite(a.data(), 1, kAbstrBytes, f) == kAbstrBytes;
+    ok = (fclose(f) == 0) && ok;
+    return ok ? kOk : fail(kErrArg, "pr_tables_save: write failed");
+}
+
+// Reads a table file and uploads it as transfer_flop_eval_cuda does (the same validation);
+// null if the file is missing, truncated or corrupted.
+void *pr_tables_load(const char *path) {
+    if (!path) return nullptr;
+    FILE *f = fopen(path, "rb");
+    if (!f) {
+        fail(kErrArg, "pr_tables_load: cannot open the file");
+        return nullptr;
+    }
+    TablesHeader h{};
+    std::vector<uint16_t> e(kEvalBytes / 2), c(kCollBytes / 2), a(kAbstrBytes / 2);
+    bool ok = fread(&h, sizeof(h), 1, f) == 1 && memcmp(h.magic, "PRBTABL1", 8) == 0 && h.version == 1 &&
+              fread(e.data(), 1, kEvalBytes, f) == kEvalBytes && fread(c.data(), 1, kCollBytes, f) == kCollBytes &&
+              fread(a.data(), 1, kAbstrBytes, f) == kAbstrBytes;
+    fclose(f);
+    if (ok) {
+        uint64_t x = 1469598103934665603ull;
+        x = fnv1a64(e.data(), kEvalBytes, x);
+        x = fnv1a64(c.data(), kCollBytes, x);
+        x = fnv1a64(a.data(), kAbstrBytes, x);
+        ok = x == h.hash;
+    }
+    if (!ok) {
+        fail(kErrTables, "pr_tables_load: not a table file, truncated or corrupted");
+        return nullptr;
+    }
+    std::vector<uint64_t> order(kHands);
+    std::vector<uint16_t> indexes(52 * 51);
+    int fill[52] = {0};
+    for (int hi = 1, n = 0; hi < 52; hi++)
+        for (int lo = 0; lo < hi; lo++, n++) {
+            order[n] = (1ull << lo) | (1ull << hi);
+            indexes[lo * 51 + fill[lo]++] = (uint16_t)n;
+            indexes[hi * 51 + fill[hi]++] = (uint16_t)n;
+        }
+    return transfer_flop_eval_cuda(h.flop, order.data(), indexes.data(), e.data(), c.data(), a.data());
+}
 
 size_t pr_river_smem_bytes(void *eval, int calc_exploit, int fp64) {
     EvalTables *t = (EvalTables *)eval;

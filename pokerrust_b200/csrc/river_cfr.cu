@@ -48,8 +48,43 @@ namespace {
 constexpr int NT = 512;                // threads per CTA
 constexpr int kGPer = 9;               // warps 0-3: rank list slots per lane (128 * 9 >= 1082)
 constexpr int kCPer = 6;               // card list slots per lane (8 lanes * 6 = 48)
-constexpr int kPioW = 20;              // bucket row: SD channels 0-8, pad, fold channels 12-19
+// Opponent-weight channels. A fold by the updater leaves the opponent's reach where the
+// sibling call (a showdown) leaves it, so that fold shares the showdown's channel: per
+// updater there are 9 showdown channels and 4 channels of folds by the opponent.
+constexpr int kNumCh = kNumSD + kNumFold / 2;
+// Opponent reach row: showdowns 0-8, pad, opponent folds 12-15; rows are 20 wide (80 bytes,
+// an odd number of 16-byte chunks) so that rows of different buckets start in all eight bank
+// groups, and only the first 16 values are loaded.
+constexpr int kPioW = 20;
+constexpr int kPioLoad = 16;
+constexpr int kUFCol = 12;
+constexpr int kWownW = 20;             // updater reach row (CFR): showdowns 0-8, pad, the 8 folds 12-19
 constexpr int kFoldCol = 12;
+// Channel of fold f (0..7) for updater `upd`: fold f is at state kLeaf(kNumSD + f) and its
+// folder is the player to act at its parent. A fold by the updater takes the channel of its
+// sibling call, showdown f + 1; the opponent's folds get channels 9-12 in fold order.
+// (Plain arithmetic, so that it folds to a constant inside unrolled loops; the static_assert
+// below checks it against the tree tables.)
+__host__ __device__ constexpr int folder(int f) { return (f & 1) ^ (f >> 2); }
+__host__ __device__ constexpr int fold_channel(int f, int upd) {
+    return folder(f) == upd ? f + 1 : kNumSD + (f >> 1);
+}
+__host__ __device__ constexpr int leaf_channel(int leaf, int upd) {
+    return leaf < kNumSD ? leaf : fold_channel(leaf - kNumSD, upd);
+}
+__host__ __device__ constexpr int pio_col(int ch) { return ch < kNumSD ? ch : kUFCol + (ch - kNumSD); }
+__host__ __device__ constexpr bool fold_channels_hold() {
+    for (int f = 0; f < kNumFold; f++) {
+        const int st = kLeaf(kNumSD + f), par = kParent(st);
+        if (kActor(par) != folder(f)) return false;                      // who folds
+        if (kChild(par, 0) != st || kChild(par, 1) != kLeaf(f + 1)) return false;  // fold, then call
+        if (kTerm(kLeaf(f + 1)) != kShowdown) return false;
+    }
+    for (int k = 0; k < kNumFold / 2; k++)  // each pair of folds has one fold by each player
+        if (folder(2 * k) == folder(2 * k + 1)) return false;
+    return true;
+}
+static_assert(fold_channels_hold(), "a fold by the updater shares its sibling showdown's opponent reach");
 constexpr int kOutPer = 3;             // output phase: hands per lane, in bucket order
 constexpr int kOutWarps = 12;          // 12 * 32 * 3 >= 1081
 constexpr int kRowW = 12;              // group rows: 9 showdown channels padded to 16-byte loads
@@ -76,7 +111,7 @@ __host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned gr
     Layout L;
     unsigned o = 0;
     L.pio = take(&o, kBuckets * kPioW * vb);
-    L.wown = cfr ? take(&o, kBuckets * kPioW * 4) : 0;
+    L.wown = cfr ? take(&o, kBuckets * kWownW * 4) : 0;
     L.Pg = take(&o, (groups + 1) * kNumSD * vb);
     L.VG = take(&o, groups * kRowW * vb);
     L.VC = take(&o, card_groups * kRowW * vb);
@@ -87,7 +122,7 @@ __host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned gr
     L.Cf = take(&o, 52 * kNumFold * vb * kCfCopies);
     L.Tf = take(&o, kNumFold * vb);
     L.Tsd = take(&o, kNumSD * vb);
-    L.gwarp = take(&o, 4 * kNumLeaves * vb);
+    L.gwarp = take(&o, 4 * kNumCh * vb);
     L.scale = take(&o, kNumLeaves * 4);
     L.stage = cfr ? take(&o, kOutWarps * 2 * acc * 4) : 0;
     L.stage_key = cfr ? take(&o, kOutWarps * 2 * 4) : 0;
@@ -97,8 +132,8 @@ __host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned gr
 
 template <typename V, int ACC = kNumLeaves>
 struct Smem {
-    V (*pio)[kPioW];             // opponent reach per bucket and leaf
-    float (*wown)[kPioW];        // updater reach * leaf scale per bucket and leaf (CFR)
+    V (*pio)[kPioW];             // opponent reach per bucket and channel
+    float (*wown)[kWownW];       // updater reach * leaf scale per bucket and leaf (CFR)
     V (*Pg)[kNumSD];             // rank-list prefix sum at each tie group's start; [G] = total
     V (*VG)[kRowW];              // W - B of each rank-list tie group
     V (*VC)[kRowW];              // W - B of each group of each card list
@@ -109,14 +144,14 @@ struct Smem {
     V *Cf;                       // card sums, fold channels (kCfCopies interleaved copies)
     V *Tf;                       // totals, fold channels
     V *Tsd;                      // totals, showdown channels
-    V (*gwarp)[kNumLeaves];      // rank-list warp totals
+    V (*gwarp)[kNumCh];          // rank-list warp totals
     float *scale;                // leaf scales
     float (*stage)[2][ACC];      // bucket runs touching an output warp's ends (CFR)
     int (*stage_key)[2];
 
     __device__ Smem(unsigned char *base, const Layout &L)
         : pio(reinterpret_cast<V(*)[kPioW]>(base + L.pio)),
-          wown(reinterpret_cast<float(*)[kPioW]>(base + L.wown)),
+          wown(reinterpret_cast<float(*)[kWownW]>(base + L.wown)),
           Pg(reinterpret_cast<V(*)[kNumSD]>(base + L.Pg)),
           VG(reinterpret_cast<V(*)[kRowW]>(base + L.VG)),
           VC(reinterpret_cast<V(*)[kRowW]>(base + L.VC)),
@@ -127,7 +162,7 @@ struct Smem {
           Cf(reinterpret_cast<V *>(base + L.Cf)),
           Tf(reinterpret_cast<V *>(base + L.Tf)),
           Tsd(reinterpret_cast<V *>(base + L.Tsd)),
-          gwarp(reinterpret_cast<V(*)[kNumLeaves]>(base + L.gwarp)),
+          gwarp(reinterpret_cast<V(*)[kNumCh]>(base + L.gwarp)),
           scale(reinterpret_cast<float *>(base + L.scale)),
           stage(reinterpret_cast<float(*)[2][ACC]>(base + L.stage)),
           stage_key(reinterpret_cast<int(*)[2]>(base + L.stage_key)) {}
@@ -157,18 +192,16 @@ __device__ __forceinline__ void load_row(const double *p, double *o, int n) {
     }
 }
 
-// x for all 17 channels of one list element (one bucket-row load).
+// x for all 13 channels of one list element (one bucket-row load).
 template <typename V, int ACC>
-__device__ __forceinline__ void elem_x(const Smem<V, ACC> &S, uint32_t e, V x[kNumLeaves]) {
+__device__ __forceinline__ void elem_x(const Smem<V, ACC> &S, uint32_t e, V x[kNumCh]) {
     const int h = e & 2047;
     const int b = (e >> 11) & 255;
     const V rh = h != (int)kNoHand ? S.r[h] : V(0);
-    V row[kPioW];
-    load_row(S.pio[b], row, kPioW);
+    V row[kPioLoad];
+    load_row(S.pio[b], row, kPioLoad);
 #pragma unroll
-    for (int c = 0; c < kNumSD; c++) x[c] = rh * row[c];
-#pragma unroll
-    for (int f = 0; f < kNumFold; f++) x[kNumSD + f] = rh * row[kFoldCol + f];
+    for (int c = 0; c < kNumCh; c++) x[c] = rh * row[pio_col(c)];
 }
 
 // The fold-channel card sums of `card` from this lane's copy (see kCfCopies).
@@ -183,7 +216,7 @@ __device__ __forceinline__ void cf_row(const V *cf, int card, V out[kNumFold]) {
 
 // Leaf values (before the leaf's bet/sign scale) of live hand l for all 17 channels:
 // showdowns from the group values of the scans, folds from totals and card sums.
-template <typename V, int ACC>
+template <int UPD, typename V, int ACC>
 __device__ __forceinline__ int hand_values(const Smem<V, ACC> &S, const BoardPack *__restrict__ pk, int l,
                                            V v[kNumLeaves]) {
     const uint4 m = __ldg(&pk->meta[l]);
@@ -199,8 +232,10 @@ __device__ __forceinline__ int hand_values(const Smem<V, ACC> &S, const BoardPac
 #pragma unroll
     for (int c = 0; c < kNumSD; c++) v[c] = g[c] - a1[c] - a2[c];  // (W - B): rank list minus card lists
     const V rh = S.r[h];
-    V xf[kNumFold], ca[kNumFold], cb[kNumFold];
-    load_row(S.pio[b] + kFoldCol, xf, kNumFold);
+    V prow[kPioLoad], xf[kNumFold], ca[kNumFold], cb[kNumFold];
+    load_row(S.pio[b], prow, kPioLoad);
+#pragma unroll
+    for (int f = 0; f < kNumFold; f++) xf[f] = prow[pio_col(fold_channel(f, UPD))];
     cf_row(S.Cf, c1, ca);
     cf_row(S.Cf, c2, cb);
     V tf[kNumFold];
@@ -229,7 +264,7 @@ __device__ __forceinline__ V vmax(V a, V b) {
     return a > b ? a : b;
 }
 
-template <int MODE, typename V, bool AVG>
+template <int MODE, typename V, bool AVG, int UPD>
 __global__ void __launch_bounds__(NT, 1)
     river_kernel(const SubgameDesc *__restrict__ desc, const V *__restrict__ ranges, V *__restrict__ results,
                  float *__restrict__ regrets, const BoardPack *__restrict__ packs, unsigned long long flop,
@@ -295,7 +330,9 @@ __global__ void __launch_bounds__(NT, 1)
         for (int Lf = 0; Lf < kNumLeaves; Lf++) {
             const int s = kLeaf(Lf);
             const int col = Lf < kNumSD ? Lf : kFoldCol + (Lf - kNumSD);
-            S.pio[b][col] = updater == 0 ? pbb[s] : psb[s];
+            // showdowns and the opponent's folds; an updater's fold has its showdown's value
+            if (Lf < kNumSD || leaf_channel(Lf, UPD) >= kNumSD)
+                S.pio[b][pio_col(leaf_channel(Lf, UPD))] = UPD == 0 ? pbb[s] : psb[s];
             if constexpr (MODE == kModeCFR) {
                 S.wown[b][col] = float(updater == 0 ? psb[s] : pbb[s]) * leaf_scale(s, updater, bet);
                 S.abar[b][Lf] = 0.0f;
@@ -327,15 +364,15 @@ __global__ void __launch_bounds__(NT, 1)
             // tie-group start (and the total at [G])
             const int g = tid;
             uint32_t ge[kGPer];
-            V tot[kNumLeaves];
+            V tot[kNumCh];
 #pragma unroll
-            for (int c = 0; c < kNumLeaves; c++) tot[c] = V(0);
+            for (int c = 0; c < kNumCh; c++) tot[c] = V(0);
 #pragma unroll
             for (int i = 0; i < kGPer; i++) {
                 const int s = g * kGPer + i;
                 const uint32_t e = s < kLive ? __ldg(&pk->gelem[s]) : kNoHand;
                 ge[i] = e;
-                V x[kNumLeaves];
+                V x[kNumCh];
                 elem_x(S, e, x);
                 if ((e & 2047) != kNoHand && (e & kGroupStart)) {
                     V *dst = S.Pg[e >> 20];
@@ -343,28 +380,28 @@ __global__ void __launch_bounds__(NT, 1)
                     for (int c = 0; c < kNumSD; c++) dst[c] = tot[c];  // lane-local part
                 }
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) tot[c] += x[c];
+                for (int c = 0; c < kNumCh; c++) tot[c] += x[c];
             }
-            V inc[kNumLeaves];
+            V inc[kNumCh];
 #pragma unroll
-            for (int c = 0; c < kNumLeaves; c++) inc[c] = tot[c];
+            for (int c = 0; c < kNumCh; c++) inc[c] = tot[c];
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) {
+                for (int c = 0; c < kNumCh; c++) {
                     const V t = __shfl_up_sync(0xffffffffu, inc[c], off);
                     if (lane >= off) inc[c] += t;
                 }
             }
             if (lane == 31) {
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) S.gwarp[warp][c] = inc[c];
+                for (int c = 0; c < kNumCh; c++) S.gwarp[warp][c] = inc[c];
             }
             bar_rank_list();
             V offs[kNumSD];
-            V total[kNumLeaves];
+            V total[kNumCh];
 #pragma unroll
-            for (int c = 0; c < kNumLeaves; c++) {
+            for (int c = 0; c < kNumCh; c++) {
                 V before = V(0), all = V(0);
 #pragma unroll
                 for (int w = 0; w < 4; w++) {
@@ -392,12 +429,12 @@ __global__ void __launch_bounds__(NT, 1)
                     S.Tsd[c] = total[c];
                 }
 #pragma unroll
-                for (int f = 0; f < kNumFold; f++) S.Tf[f] = total[kNumSD + f];
+                for (int f = 0; f < kNumFold; f++) S.Tf[f] = total[fold_channel(f, UPD)];
                 if constexpr (MODE == kModeCFR) {
                     // blocked hands' contribution to bucket 0 (see the file comment)
 #pragma unroll
                     for (int c = 0; c < kNumLeaves; c++)
-                        S.abar[0][c] += (c < kNumSD ? -235.0f : 235.0f) * total[c];
+                        S.abar[0][c] += (c < kNumSD ? -235.0f : 235.0f) * total[leaf_channel(c, UPD)];
                 }
             }
             // W - B of every tie group: prefix at its start + prefix at its end - total
@@ -417,28 +454,28 @@ __global__ void __launch_bounds__(NT, 1)
             const bool active = li < kNumLists;
             uint32_t ce[kCPer];
             V xs[kCPer][kNumSD];
-            V tot[kNumLeaves];
+            V tot[kNumCh];
 #pragma unroll
-            for (int c = 0; c < kNumLeaves; c++) tot[c] = V(0);
+            for (int c = 0; c < kNumCh; c++) tot[c] = V(0);
 #pragma unroll
             for (int i = 0; i < kCPer; i++) {
                 const int j = sl * kCPer + i;
                 const uint32_t e = (active && j < kListLen) ? __ldg(&pk->celem[li * kLSlots + j]) : kNoHand;
                 ce[i] = e;
-                V x[kNumLeaves];
+                V x[kNumCh];
                 elem_x(S, e, x);
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) tot[c] += x[c];
+                for (int c = 0; c < kNumCh; c++) tot[c] += x[c];
 #pragma unroll
                 for (int c = 0; c < kNumSD; c++) xs[i][c] = x[c];
             }
-            V inc[kNumLeaves];
+            V inc[kNumCh];
 #pragma unroll
-            for (int c = 0; c < kNumLeaves; c++) inc[c] = tot[c];
+            for (int c = 0; c < kNumCh; c++) inc[c] = tot[c];
 #pragma unroll
             for (int off = 1; off < 8; off <<= 1) {
 #pragma unroll
-                for (int c = 0; c < kNumLeaves; c++) {
+                for (int c = 0; c < kNumCh; c++) {
                     const V t = __shfl_up_sync(FULL, inc[c], off);
                     if (sl >= off) inc[c] += t;
                 }
@@ -448,7 +485,7 @@ __global__ void __launch_bounds__(NT, 1)
                 // into copy sl
                 V cf[kNumFold];
 #pragma unroll
-                for (int f = 0; f < kNumFold; f++) cf[f] = __shfl_sync(FULL, inc[kNumSD + f], lane | 7);
+                for (int f = 0; f < kNumFold; f++) cf[f] = __shfl_sync(FULL, inc[fold_channel(f, UPD)], lane | 7);
                 if (active) {
                     constexpr int kPer = 16 / sizeof(V), kChunks = kNumFold / kPer;
                     const int card = pk->list_card[li];
@@ -522,11 +559,11 @@ __global__ void __launch_bounds__(NT, 1)
                 const int key = be >> 16;
                 if (key == (int)kNoBucket) continue;
                 V v[ACC];
-                const int h = hand_values(S, pk, be & 0xffff, v);
+                const int h = hand_values<UPD>(S, pk, be & 0xffff, v);
                 if constexpr (AVG) v[kNumLeaves] = S.own[h];
                 if constexpr (MODE == kModeCFR) {
-                    float w[kPioW];
-                    load_row(S.wown[key], w, kPioW);
+                    float w[kWownW];
+                    load_row(S.wown[key], w, kWownW);
                     float acc = 0.0f;
 #pragma unroll
                     for (int c = 0; c < kNumSD; c++) acc += v[c] * w[c];
@@ -739,6 +776,18 @@ __global__ void __launch_bounds__(NT, 1)
     }
 }
 
+template <int MODE, typename V, bool AVG, int UPD>
+cudaError_t launch_upd(const SubgameDesc *desc, int n, const V *ranges, V *results, float *regrets,
+                       const BoardPack *packs, unsigned long long flop, int max_groups, int max_card_groups,
+                       const float *own, float *avg, size_t smem, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(river_kernel<MODE, V, AVG, UPD>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    river_kernel<MODE, V, AVG, UPD><<<n, NT, smem, stream>>>(desc, ranges, results, regrets, packs, flop, UPD,
+                                                             max_groups, max_card_groups, own, avg);
+    return cudaGetLastError();
+}
+
 template <int MODE, typename V, bool AVG>
 cudaError_t launch_one(const SubgameDesc *desc, int n, const V *ranges, V *results, float *regrets,
                        const BoardPack *packs, unsigned long long flop, int updater, int max_groups,
@@ -746,12 +795,11 @@ cudaError_t launch_one(const SubgameDesc *desc, int n, const V *ranges, V *resul
     const Layout L = make_layout(MODE == kModeCFR, sizeof(V), max_groups, max_card_groups,
                                  kNumLeaves + (AVG ? 1 : 0));
     if (L.total > 227u * 1024u) return cudaErrorInvalidConfiguration;
-    cudaError_t e = cudaFuncSetAttribute(river_kernel<MODE, V, AVG>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
-    if (e != cudaSuccess) return e;
-    river_kernel<MODE, V, AVG><<<n, NT, L.total, stream>>>(desc, ranges, results, regrets, packs, flop,
-                                                           updater, max_groups, max_card_groups, own, avg);
-    return cudaGetLastError();
+    if (updater == 0)
+        return launch_upd<MODE, V, AVG, 0>(desc, n, ranges, results, regrets, packs, flop, max_groups,
+                                           max_card_groups, own, avg, L.total, stream);
+    return launch_upd<MODE, V, AVG, 1>(desc, n, ranges, results, regrets, packs, flop, max_groups, max_card_groups,
+                                       own, avg, L.total, stream);
 }
 
 }  // namespace

@@ -184,6 +184,10 @@ def lib():
         L.pr_tables_build.argtypes = [u64]
         L.pr_tables_export.restype = i32
         L.pr_tables_export.argtypes = [vp, vp, vp, vp]
+        L.pr_tables_save.restype = i32
+        L.pr_tables_save.argtypes = [vp, ctypes.c_char_p]
+        L.pr_tables_load.restype = vp
+        L.pr_tables_load.argtypes = [ctypes.c_char_p]
         _lib = L
     return _lib
 
@@ -276,6 +280,19 @@ def export_tables(ptr):
     a = np.zeros(HANDS * HANDS, np.uint16)
     _check(lib().pr_tables_export(ptr, _ptr(e), _ptr(c), _ptr(a)), "pr_tables_export")
     return e, c, a
+
+
+def save_tables(ptr, path):
+    """Writes a table handle's packed tables to a checksummed file (pr_tables_save)."""
+    _check(lib().pr_tables_save(ptr, os.fsencode(path)), "pr_tables_save")
+
+
+def load_tables(path):
+    """Reads a table file into a device table handle (pr_tables_load)."""
+    ptr = lib().pr_tables_load(os.fsencode(path))
+    if not ptr:
+        raise PokerLibError(f"pr_tables_load failed for {path}")
+    return ptr
 
 
 def free_eval(ptr):

@@ -61,3 +61,21 @@ def test_generated_tables_drive_the_solver(P, flop_tables):
     P.free_eval(gen)
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_table_file_round_trip(tmp_path):
+    import pokerrust_b200 as P
+    from pokerrust_b200 import interface as I
+    t = P.build_flop_tables(0b111)
+    path = str(tmp_path / "flop7.prbt")
+    I.save_tables(t, path)
+    u = I.load_tables(path)
+    for a, b in zip(P.export_tables(t), P.export_tables(u)):
+        assert np.array_equal(a, b)
+    data = bytearray(open(path, "rb").read())
+    data[5000] ^= 0x10
+    open(path, "wb").write(bytes(data))
+    with pytest.raises(P.PokerLibError):
+        I.load_tables(path)
+    P.free_eval(t)
+    P.free_eval(u)
