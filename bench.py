@@ -251,6 +251,20 @@ def batch_cpu_sample(specs, ranges, threads):
             "sample": f"{n} of {len(specs)} subgames, one iteration, {dt:.2f} s, scaled"}
 
 
+def max_over_ranks(x, world, device):
+    """The largest of the ranks' values (the slowest rank's time); the value itself at N = 1."""
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, world, max_seconds):
+    """Whole-job throughput of N replicas: all ranks' units over the slowest rank's time."""
+    return world * units_per_rank / max_seconds
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -394,11 +408,8 @@ def run_gpu(args):
     barrier()
     clk = clocks.stop()
     kernel_ms = ev0.elapsed_time(ev1) / args.steps
-    t = torch.tensor([kernel_ms], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms = float(t.item())
-    value = world * n * NODES_PER_SUBGAME / (ms / 1e3)
+    ms = max_over_ranks(kernel_ms, world, dev)
+    value = replica_rate(n * NODES_PER_SUBGAME, world, ms / 1e3)
 
     if args.profile:
         if rank == 0:
@@ -424,11 +435,7 @@ def run_gpu(args):
         builder.upload_all(host_in)
         P.evaluate_gpu(builder.ptr, tables, i % 2, False)
         out = builder.download_all()
-    e2e_s = (time.perf_counter() - t0) / e_steps
-    t = torch.tensor([e2e_s], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e_steps, world, dev)
     assert np.all(np.isfinite(out))
 
     # whole-game CFR iterations through the library's game driver (game.rs:68-119): the
