@@ -38,6 +38,11 @@ UNIT = "nodes/s"
 WORKLOAD = "fixed-flop limit hold'em, all 27783 river subgames, one CFR pass per step"
 
 
+# DRAM bytes of one full river launch (27,783 subgames), read + write, from a single-pass ncu
+# capture of this program (profiles/launch_list_bench_profile.md)
+TRAFFIC_PER_LAUNCH = 1063193600 + 509289984
+
+
 def algorithmic_bytes(n):
     # ranges in + values out (1326 f32 each), regrets read (26 x 256 f32) and written
     # (the updater's 13 edges), tables once per pass (1176 boards x 11632 B).
@@ -482,7 +487,9 @@ def run_gpu(args):
                     "h2d_bytes_per_step": int(n * 1328 * 4), "d2h_bytes_per_step": int(n * 1328 * 4),
                     "ms_per_step": e2e_s * 1e3},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH if n == SUBGAMES else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full launch "
+                                           "(profiles/launch_list_bench_profile.md)",
                          "peak_source": peak_kind,
                          "note": "algorithmic bytes per pass / kernel time; the pass is bound "
                                  "on-chip (shared memory and issue), not by HBM"},
