@@ -212,13 +212,18 @@ int pr_batch_shape(void *batch, int s, int *num_nodes, int *num_edges, int *num_
 int pr_batch_enable_average(void *batch);
 /* CFR iterations: player 0 update, then player 1. */
 int pr_batch_iterate(void *batch, int iterations);
-/* No counterpart in the reference. pr_batch_iterate without allocation: the iterations are
- * launched eagerly (no graph) and the work-queue scratch (queue heads and order) lives in a
- * fixed device array of the library, so the call runs no cudaMalloc / cudaFree or other
- * allocating routine. Limit: 65536 subgames per batch (status 2 beyond). The queue heads are
- * cleared before every iteration. The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make that first call before any stream capture. Calls that
- * overlap in time share the array and race: issue them one at a time. */
+/* No counterpart in the reference. pr_batch_iterate for callers that may not allocate once
+ * their solve loop runs: a process whose GPU memory is handed out by its own caching
+ * allocator, or a loop on a shared GPU where a cudaMalloc / cudaFree (they synchronise the
+ * device) or building a CUDA graph (pr_batch_iterate does that on its first call) would stall
+ * other work. The passes are launched directly, and the work-queue scratch (queue heads and
+ * queue order) sits in a fixed 256 KB device array of the library, held on every GPU that
+ * loads it, so the call makes no cudaMalloc, cudaFree or other allocating call.
+ * Limit: 65536 subgames per batch (status 2 beyond). The queue heads are cleared before every
+ * pass; the order is rewritten on every call. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress): make that first call before any stream
+ * capture. All calls share the one array, so calls that overlap on the GPU race: issue them
+ * one after another. */
 int pr_batch_iterate_noalloc(void *batch, int iterations);
 /* Per subgame: best-response sums of each player (range-weighted root values) and the
  * exploitability (br0 + br1) / 2 per unit of joint range mass, in chips; against the

@@ -135,11 +135,13 @@ struct Batch {
 
 // ---- no-allocation iteration ----
 // Work-queue scratch of pr_batch_iterate_noalloc: kClasses * 2 queue heads, then the queue
-// order of up to kNoAllocMaxSubgames subgames. A fixed device array of the library, so the
-// call allocates nothing.
+// order of up to kNoAllocMaxSubgames subgames, 256 KB in all. It is a fixed device array of
+// the library, so every GPU that loads the library holds it until the process exits, and
+// the entry point needs no allocation. Host code only sees a stand-in for this name; the
+// device address comes from cudaGetSymbolAddress (noalloc_scratch below).
 constexpr int kNoAllocMaxSubgames = 65536;
 constexpr int kNoAllocHeads = 2 * kClasses;
-__device__ __align__(256) int g_noalloc_scratch[kNoAllocHeads + kNoAllocMaxSubgames];
+static __device__ __align__(256) int g_noalloc_scratch[kNoAllocHeads + kNoAllocMaxSubgames];
 
 std::mutex g_noalloc_mu;
 int *g_noalloc_ptr[64] = {};  // per device, looked up once with that device current
@@ -430,8 +432,12 @@ int pr_batch_root_values(void *batch, int player, int use_average, double *value
     return 0;
 }
 
-// CFR iterations like pr_batch_iterate, launched eagerly, with the work queue (heads and
-// order) in the library's fixed device array instead of the batch's buffers: no allocation.
+// CFR iterations like pr_batch_iterate for callers that may not allocate once their solve
+// loop runs: a process whose GPU memory belongs to its own caching allocator after start-up,
+// or a loop on a shared GPU where a cudaMalloc / cudaFree (which synchronise the device) or
+// building a CUDA graph (pr_batch_iterate does that on its first call) would stall other
+// work. The passes are launched directly, and the work queue (heads and order) lives in the
+// library's fixed device array instead of the batch's buffers.
 int pr_batch_iterate_noalloc(void *batch, int iterations) {
     Batch *b = (Batch *)batch;
     if (!b || iterations < 0) return 2;

@@ -1,6 +1,9 @@
-"""pr_batch_iterate_noalloc against pr_batch_iterate: two calls in a row on identical
-batches give the same regrets and average sums (the tolerance of the batch tests, 1e-4 of
-the largest entry; the kernels are the same, so they agree bit for bit in practice)."""
+"""pr_batch_iterate_noalloc, the entry point for callers that may not allocate while they
+solve (their GPU memory belongs to their own allocator, or a cudaMalloc or graph build would
+stall a shared GPU), against pr_batch_iterate: two calls in a row on identical batches give
+the same regrets and average sums, within the batch tests' tolerance of 1e-4 of the largest
+entry (the kernels are the same, so in practice they agree bit for bit). This file is
+collected last, so a run that stops at the first failure has run every other test first."""
 import numpy as np
 import pytest
 
