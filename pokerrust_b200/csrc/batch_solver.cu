@@ -14,8 +14,8 @@
 //                of p's two cards), W / B = weight of strictly worse / better hands, taken
 //                at the bounds of the hand's tie group (card removal by inclusion-exclusion);
 //      fold      +-stake * (T - C[c1] - C[c2] + x(h)), T the total and C the per-card sums.
-//    Prefix sums use a fixed summation tree (32-wide warp scans of fixed chunks and card
-//    lists), so results do not depend on the CTA size;
+//    Prefix sums use a fixed summation tree (warp scans of fixed 64-hand chunks, two hands
+//    per lane, and of the card lists), so results do not depend on the CTA size;
 //  * bottom-up: values flow to the root; at p's nodes the CFR pass updates regrets
 //    r <- max(r + v(child) - v(node), 0) (the child value is added when the child closes and
 //    the node value subtracted when the node closes, so no per-child storage is needed), the
@@ -306,6 +306,15 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
         const float *Src = src_all + (size_t)sub.edge_off * kBRow;
         const float *rng = a.ranges + (size_t)s * 2 * kBRow;
         const int pos0 = tid * K;
+        // this thread's hands' tie-group and card-list bounds, read once per subgame
+        uint32_t pgrp[K], plist[K], plist2[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int pq = pos0 + k < kBRow ? pos0 + k : kBRow - 1;
+            pgrp[k] = __ldg(&pk->grp[pq]);
+            plist[k] = __ldg(&pk->lists[pq]);
+            plist2[k] = __ldg(&pk->lists2[pq]);
+        }
 
         // walker state, per owned hand: depth-indexed stacks of the open path (indexed at run
         // time, so they live in local memory, cached in L1)
@@ -463,19 +472,25 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                 V *I = S.I + buf * kBRow;
                 V *CT = S.CT + buf * kBChunks;
                 V *SC = S.SC + buf * kBLists * 48;
-                // phase A: chunk scans of the rank order and scans of the card lists
-                for (int u = warp; u < kBChunks + kBLists; u += NW) {
-                    if (u < kBChunks) {
-                        V v = x[u * 32 + lane];
+                // phase A: scans of the rank order in 64-hand chunks (two hands per lane) and
+                // scans of the card lists
+                for (int u = warp; u < kBChunks64 + kBLists; u += NW) {
+                    if (u < kBChunks64) {
+                        const V a0 = x[u * 64 + 2 * lane];
+                        const V a1 = a0 + x[u * 64 + 2 * lane + 1];
+                        V v = a1;
 #pragma unroll
                         for (int off = 1; off < 32; off <<= 1) {
                             const V t = __shfl_up_sync(FULL, v, off);
                             if (lane >= off) v += t;
                         }
-                        I[u * 32 + lane] = v;
+                        V ex = __shfl_up_sync(FULL, v, 1);
+                        if (lane == 0) ex = V(0);
+                        I[u * 64 + 2 * lane] = ex + a0;
+                        I[u * 64 + 2 * lane + 1] = v;
                         if (lane == 31) CT[u] = v;
                     } else {
-                        const int li = u - kBChunks;
+                        const int li = u - kBChunks64;
                         V a0 = V(0), a1 = V(0);
                         if (lane < kBListLen / 2) {
                             a0 = x[pk->clpos[li][2 * lane]];
@@ -496,41 +511,30 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                     }
                 }
                 __syncthreads();
-                // phase C: chunk offsets (every warp, same arithmetic), then values
-                V c0 = V(0), c1 = V(0);
-                if (lane < kBChunks / 2) {
-                    c0 = CT[2 * lane];
-                    c1 = c0 + CT[2 * lane + 1];
-                }
-                V inc = c1;
+                // phase C: chunk offsets (every warp, same arithmetic; lane c holds chunk c's),
+                // then values
+                V inc = lane < kBChunks64 ? CT[lane] : V(0);
 #pragma unroll
                 for (int off = 1; off < 32; off <<= 1) {
                     const V t = __shfl_up_sync(FULL, inc, off);
                     if (lane >= off) inc += t;
                 }
-                V ex = __shfl_up_sync(FULL, inc, 1);
-                if (lane == 0) ex = V(0);
-                const V off_even = ex, off_odd = ex + c0;
-                const V T = __shfl_sync(FULL, inc, kBChunks / 2 - 1);
+                V cofs = __shfl_up_sync(FULL, inc, 1);
+                if (lane == 0) cofs = V(0);
+                const V T = __shfl_sync(FULL, inc, kBChunks64 - 1);
                 const BNode ln = S.tn[S.leaf_node[j]];
                 const V stake = V(ln.stake);
 #pragma unroll
                 for (int k = 0; k < K; k++) {
                     const int pos = pos0 + k;
-                    const int pq = pos < kBRow ? pos : kBRow - 1;
-                    const uint32_t gr = __ldg(&pk->grp[pq]);
-                    const uint32_t l1 = __ldg(&pk->lists[pq]);
-                    const uint32_t l2 = __ldg(&pk->lists2[pq]);
+                    const uint32_t gr = pgrp[k], l1 = plist[k], l2 = plist2[k];
                     const int gs = gr & 0xFFFF, ge = gr >> 16;
                     const int li1 = l1 & 255, li2 = (l1 >> 8) & 255;
                     const int gs1 = (l1 >> 16) & 255, ge1 = l1 >> 24;
                     const int gs2 = l2 & 255, ge2 = (l2 >> 8) & 255;
                     // chunk offsets by shuffle (all lanes take part)
-                    const int ce = ge >> 5, cs = (gs - 1) >> 5;
-                    const V oe_e = __shfl_sync(FULL, off_even, ce >> 1);
-                    const V oe_o = __shfl_sync(FULL, off_odd, ce >> 1);
-                    const V os_e = __shfl_sync(FULL, off_even, (gs > 0 ? cs : 0) >> 1);
-                    const V os_o = __shfl_sync(FULL, off_odd, (gs > 0 ? cs : 0) >> 1);
+                    const V oe = __shfl_sync(FULL, cofs, ge >> 6);
+                    const V os = __shfl_sync(FULL, cofs, gs > 0 ? (gs - 1) >> 6 : 0);
                     if (pos >= kBRow) continue;
                     V val = V(0);
                     if (pos < kBLive) {
@@ -538,8 +542,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                         const V *sc2 = SC + li2 * 48;
                         const V T1 = sc1[kBListLen - 1], T2 = sc2[kBListLen - 1];
                         if (ln.kind == kBShowdown) {
-                            const V Pe = ((ce & 1) ? oe_o : oe_e) + I[ge];
-                            const V Ps = gs > 0 ? ((cs & 1) ? os_o : os_e) + I[gs - 1] : V(0);
+                            const V Pe = oe + I[ge];
+                            const V Ps = gs > 0 ? os + I[gs - 1] : V(0);
                             const V vg = (Pe + Ps) - T;
                             const V v1 = (sc1[ge1] + (gs1 > 0 ? sc1[gs1 - 1] : V(0))) - T1;
                             const V v2 = (sc2[ge2] + (gs2 > 0 ? sc2[gs2 - 1] : V(0))) - T2;

@@ -14,6 +14,7 @@ constexpr int kBRow = 1088;    // per-hand rows, padded to a multiple of 32
 constexpr int kBLists = 47;    // off-board cards
 constexpr int kBListLen = 46;  // live hands holding one off-board card
 constexpr int kBChunks = kBRow / 32;
+constexpr int kBChunks64 = kBRow / 64;  // 64-hand chunks of the rank-order scan
 
 // One subgame as the kernels see it.
 struct BSub {
