@@ -253,6 +253,49 @@ __device__ inline Smem<V> carve(unsigned char *base, int group) {
     return S;
 }
 
+// A thread's K consecutive positions of a row. With K = 2 or 4 (and kBRow a multiple of 4)
+// they are all inside the row or all past it, and move as vector accesses of at most 16 bytes
+// (rows start on 16-byte boundaries); with K = 3 they move one by one. Positions past the row
+// read as zero and are not written.
+static_assert(kBRow % 4 == 0, "vector row accesses");
+template <int K, typename T>
+struct alignas(K == 3 ? sizeof(T) : (K * sizeof(T) > 16 ? 16 : K * sizeof(T))) Lanes {
+    T v[K];
+};
+
+template <int K, typename T, typename U>
+__device__ __forceinline__ void ld_k(const T *row, int pos0, U (&out)[K]) {
+    if constexpr (K == 3) {
+#pragma unroll
+        for (int k = 0; k < K; k++) out[k] = pos0 + k < kBRow ? U(row[pos0 + k]) : U(0);
+    } else {
+        if (pos0 < kBRow) {
+            const Lanes<K, T> t = *reinterpret_cast<const Lanes<K, T> *>(row + pos0);
+#pragma unroll
+            for (int k = 0; k < K; k++) out[k] = U(t.v[k]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; k++) out[k] = U(0);
+        }
+    }
+}
+
+template <int K, typename T, typename U>
+__device__ __forceinline__ void st_k(T *row, int pos0, const U (&in)[K]) {
+    if constexpr (K == 3) {
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            if (pos0 + k < kBRow) row[pos0 + k] = T(in[k]);
+    } else {
+        if (pos0 < kBRow) {
+            Lanes<K, T> t;
+#pragma unroll
+            for (int k = 0; k < K; k++) t.v[k] = T(in[k]);
+            *reinterpret_cast<Lanes<K, T> *>(row + pos0) = t;
+        }
+    }
+}
+
 // Strategy of edge `e` at a node whose out-edges have positive-part sum `S`.
 template <typename V, bool USEAVG>
 __device__ __forceinline__ V sigma(V val, V S, int n) {
@@ -327,6 +370,39 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
 #pragma unroll
         for (int k = 0; k < K; k++) root[k] = V(0);
 
+        // adds the values v of the child behind edge ie to its parent par, open at depth dp
+        auto deliver = [&](int par, int ie, int dp, const V(&v)[K]) {
+            const BNode pq = S.tn[par];
+            if (a.child_out && par == 0) {
+                V *co = reinterpret_cast<V *>(a.child_out) + ((size_t)s * 8 + (ie - pq.edge)) * kBRow;
+                st_k<K>(co, pos0, v);
+            }
+            if (pq.actor != p) {
+#pragma unroll
+                for (int k = 0; k < K; k++) acc[k][dp] = acc[k][dp] + v[k];
+            } else if (MODE == kBModeBR) {
+#pragma unroll
+                for (int k = 0; k < K; k++) acc[k][dp] = acc[k][dp] > v[k] ? acc[k][dp] : v[k];
+            } else {
+                // the edge's strategy from its regret (or average) row; CFR adds the child's
+                // value to the regret, which the parent's close turns into the regret update
+                const size_t ro = (size_t)ie * kBRow;
+                V sv[K];
+                if (MODE == kBModeCFR)
+                    ld_k<K>(R + ro, pos0, sv);
+                else
+                    ld_k<K>(Src + ro, pos0, sv);
+#pragma unroll
+                for (int k = 0; k < K; k++)
+                    acc[k][dp] = acc[k][dp] + mul(sigma<V, USEAVG>(sv[k], Sb[k][dp], pq.nchild), v[k]);
+                if constexpr (MODE == kBModeCFR) {
+                    float r[K];
+#pragma unroll
+                    for (int k = 0; k < K; k++) r[k] = float(sv[k]) + float(v[k]);
+                    st_k<K>(R + ro, pos0, r);
+                }
+            }
+        };
         // closes the open nodes at depth >= d, passing each value to its parent
         auto close_to = [&](int d) {
             while (open_top >= d) {
@@ -336,14 +412,13 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
 #pragma unroll
                 for (int k = 0; k < K; k++) v[k] = acc[k][open_top];
                 if (MODE == kBModeCFR && nm.actor == p) {
+                    for (int e = 0; e < nm.nchild; e++) {
+                        float *row = R + (size_t)(nm.edge + e) * kBRow;
+                        float r[K];
+                        ld_k<K>(row, pos0, r);
 #pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        const int pos = pos0 + k;
-                        if (pos >= kBRow) continue;
-                        for (int e = 0; e < nm.nchild; e++) {
-                            float &r = R[(size_t)(nm.edge + e) * kBRow + pos];
-                            r = fmaxf(r - float(v[k]), 0.0f);
-                        }
+                        for (int k = 0; k < K; k++) r[k] = fmaxf(r[k] - float(v[k]), 0.0f);
+                        st_k<K>(row, pos0, r);
                     }
                 }
                 open_top--;
@@ -351,40 +426,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
 #pragma unroll
                     for (int k = 0; k < K; k++) root[k] = v[k];
                 } else {
-                    // deliver to the parent (open at depth open_top)
-                    const BNode pq = S.tn[nm.parent];
-                    if (a.child_out && nm.parent == 0) {
-                        V *co = reinterpret_cast<V *>(a.child_out) + ((size_t)s * 8 + (nm.in_edge - pq.edge)) * kBRow;
-#pragma unroll
-                        for (int k = 0; k < K; k++)
-                            if (pos0 + k < kBRow) co[pos0 + k] = v[k];
-                    }
-#pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        V ak = acc[k][open_top];
-                        const int pos = pos0 + k;
-                        if (pq.actor == p) {
-                            if (MODE == kBModeBR) {
-                                ak = ak > v[k] ? ak : v[k];
-                            } else {
-                                const V sb = Sb[k][open_top];
-                                V val = V(0);
-                                if (pos < kBRow) {
-                                    if (MODE == kBModeCFR) {
-                                        float &r = R[(size_t)nm.in_edge * kBRow + pos];
-                                        val = V(r);
-                                        r = r + float(v[k]);
-                                    } else {
-                                        val = V(Src[(size_t)nm.in_edge * kBRow + pos]);
-                                    }
-                                }
-                                ak = ak + mul(sigma<V, USEAVG>(val, sb, pq.nchild), v[k]);
-                            }
-                        } else {
-                            ak = ak + v[k];
-                        }
-                        acc[k][open_top] = ak;
-                    }
+                    deliver(nm.parent, nm.in_edge, open_top, v);
                 }
             }
         };
@@ -397,39 +439,31 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                 const int d = nd.depth;
                 V npo[K], npp[K];
                 if (td == 0) {
+                    ld_k<K>(rng + o * kBRow, pos0, npo);
 #pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        const int pos = pos0 + k;
-                        npo[k] = pos < kBRow ? V(rng[o * kBRow + pos]) : V(0);
-                        npp[k] = V(1);
-                    }
+                    for (int k = 0; k < K; k++) npp[k] = V(1);
                 } else {
                     const BNode pm = S.tn[nd.parent];
                     const bool own = pm.actor == p;
                     const bool need = !own || AVG;
+                    const size_t ro = (size_t)nd.in_edge * kBRow;
+                    V sv[K];
+                    if (need) ld_k<K>(Src + ro, pos0, sv);
 #pragma unroll
                     for (int k = 0; k < K; k++) {
                         const V po_par = po[k][d - 1];
                         const V pp_par = pp[k][d - 1];
-                        V sg = V(1);
-                        if (need) {
-                            const int pos = pos0 + k;
-                            const V val = pos < kBRow ? V(Src[(size_t)nd.in_edge * kBRow + pos]) : V(0);
-                            sg = sigma<V, USEAVG>(val, St[k][d - 1], pm.nchild);
-                        }
+                        const V sg = need ? sigma<V, USEAVG>(sv[k], St[k][d - 1], pm.nchild) : V(1);
+                        npo[k] = own ? po_par : mul(po_par, sg);
+                        npp[k] = own ? mul(pp_par, sg) : pp_par;
+                    }
+                    if constexpr (AVG) {
                         if (own) {
-                            npo[k] = po_par;
-                            npp[k] = mul(pp_par, sg);
-                            if constexpr (AVG) {
-                                const int pos = pos0 + k;
-                                if (pos < kBRow) {
-                                    float &av = A[(size_t)nd.in_edge * kBRow + pos];
-                                    av += float(mul(pp_par, sg));
-                                }
-                            }
-                        } else {
-                            npo[k] = mul(po_par, sg);
-                            npp[k] = pp_par;
+                            float av[K];
+                            ld_k<K>(A + ro, pos0, av);
+#pragma unroll
+                            for (int k = 0; k < K; k++) av[k] += float(npp[k]);
+                            st_k<K>(A + ro, pos0, av);
                         }
                     }
                 }
@@ -441,26 +475,24 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                 if (nd.kind == kBDecision) {
                     // strategy sums of the node, for its children
                     const bool own = nd.actor == p;
-                    const bool need = !own || AVG;
+                    V sum[K];
 #pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        V sum = V(0);
-                        if (need) {
-                            const int pos = pos0 + k;
-                            for (int e = 0; e < nd.nchild; e++) {
-                                const V val = pos < kBRow ? V(Src[(size_t)(nd.edge + e) * kBRow + pos]) : V(0);
-                                sum += val > V(0) ? val : V(0);
-                            }
+                    for (int k = 0; k < K; k++) sum[k] = V(0);
+                    if (!own || AVG) {
+                        for (int e = 0; e < nd.nchild; e++) {
+                            V sv[K];
+                            ld_k<K>(Src + (size_t)(nd.edge + e) * kBRow, pos0, sv);
+#pragma unroll
+                            for (int k = 0; k < K; k++) sum[k] += sv[k] > V(0) ? sv[k] : V(0);
                         }
-                        St[k][d] = sum;
                     }
-                } else {
-                    V *x = S.X + (size_t)(nd.edge - g0) * kBRow;
 #pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        const int pos = pos0 + k;
-                        if (pos < kBRow) x[pos] = pos < kBLive ? npo[k] : V(0);
-                    }
+                    for (int k = 0; k < K; k++) St[k][d] = sum[k];
+                } else {
+                    V xv[K];
+#pragma unroll
+                    for (int k = 0; k < K; k++) xv[k] = pos0 + k < kBLive ? npo[k] : V(0);
+                    st_k<K>(S.X + (size_t)(nd.edge - g0) * kBRow, pos0, xv);
                 }
             }
             __syncthreads();
@@ -524,6 +556,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                 const V T = __shfl_sync(FULL, inc, kBChunks64 - 1);
                 const BNode ln = S.tn[S.leaf_node[j]];
                 const V stake = V(ln.stake);
+                V xv[K];
+                ld_k<K>(x, pos0, xv);
 #pragma unroll
                 for (int k = 0; k < K; k++) {
                     const int pos = pos0 + k;
@@ -535,7 +569,6 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                     // chunk offsets by shuffle (all lanes take part)
                     const V oe = __shfl_sync(FULL, cofs, ge >> 6);
                     const V os = __shfl_sync(FULL, cofs, gs > 0 ? (gs - 1) >> 6 : 0);
-                    if (pos >= kBRow) continue;
                     V val = V(0);
                     if (pos < kBLive) {
                         const V *sc1 = SC + li1 * 48;
@@ -549,12 +582,13 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                             const V v2 = (sc2[ge2] + (gs2 > 0 ? sc2[gs2 - 1] : V(0))) - T2;
                             val = mul(stake, (vg - v1) - v2);
                         } else {
-                            const V free = ((T - T1) - T2) + x[pos];
+                            const V free = ((T - T1) - T2) + xv[k];
                             val = mul(ln.actor == p ? -stake : stake, free);
                         }
                     }
-                    x[pos] = val;
+                    xv[k] = val;
                 }
+                st_k<K>(x, pos0, xv);
             }
             __syncthreads();
 
@@ -567,56 +601,27 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                     open_top = d;
                     open_id[d] = bu;
                     const bool own = nd.actor == p;
+                    V sum[K];
 #pragma unroll
                     for (int k = 0; k < K; k++) {
                         acc[k][d] = (own && MODE == kBModeBR) ? neg_inf<V>() : V(0);
-                        V sum = V(0);
-                        if (own && MODE != kBModeBR) {
-                            const int pos = pos0 + k;
-                            for (int e = 0; e < nd.nchild; e++) {
-                                const V val = pos < kBRow ? V(Src[(size_t)(nd.edge + e) * kBRow + pos]) : V(0);
-                                sum += val > V(0) ? val : V(0);
-                            }
-                        }
-                        Sb[k][d] = sum;
+                        sum[k] = V(0);
                     }
+                    if (own && MODE != kBModeBR) {
+                        for (int e = 0; e < nd.nchild; e++) {
+                            V sv[K];
+                            ld_k<K>(Src + (size_t)(nd.edge + e) * kBRow, pos0, sv);
+#pragma unroll
+                            for (int k = 0; k < K; k++) sum[k] += sv[k] > V(0) ? sv[k] : V(0);
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < K; k++) Sb[k][d] = sum[k];
                 } else {
                     // a leaf: its value goes straight to the parent (open at depth d - 1)
-                    const V *x = S.X + (size_t)(nd.edge - g0) * kBRow;
-                    const BNode pq = S.tn[nd.parent];
-                    if (a.child_out && nd.parent == 0) {
-                        V *co = reinterpret_cast<V *>(a.child_out) + ((size_t)s * 8 + (nd.in_edge - pq.edge)) * kBRow;
-#pragma unroll
-                        for (int k = 0; k < K; k++)
-                            if (pos0 + k < kBRow) co[pos0 + k] = x[pos0 + k];
-                    }
-#pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        const int pos = pos0 + k;
-                        const V v = pos < kBRow ? x[pos] : V(0);
-                        V ak = acc[k][d - 1];
-                        if (pq.actor == p) {
-                            if (MODE == kBModeBR) {
-                                ak = ak > v ? ak : v;
-                            } else {
-                                const V sb = Sb[k][d - 1];
-                                V val = V(0);
-                                if (pos < kBRow) {
-                                    if (MODE == kBModeCFR) {
-                                        float &r = R[(size_t)nd.in_edge * kBRow + pos];
-                                        val = V(r);
-                                        r = r + float(v);
-                                    } else {
-                                        val = V(Src[(size_t)nd.in_edge * kBRow + pos]);
-                                    }
-                                }
-                                ak = ak + mul(sigma<V, USEAVG>(val, sb, pq.nchild), v);
-                            }
-                        } else {
-                            ak = ak + v;
-                        }
-                        acc[k][d - 1] = ak;
-                    }
+                    V xv[K];
+                    ld_k<K>(S.X + (size_t)(nd.edge - g0) * kBRow, pos0, xv);
+                    deliver(nd.parent, nd.in_edge, d - 1, xv);
                 }
             }
             __syncthreads();  // X is rewritten by the next group
@@ -625,18 +630,15 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
 
         // ---- outputs: root values and their range-weighted sum ----
         if (a.root_out) {
-            V *ro = reinterpret_cast<V *>(a.root_out) + (size_t)s * kBRow;
-#pragma unroll
-            for (int k = 0; k < K; k++)
-                if (pos0 + k < kBRow) ro[pos0 + k] = root[k];
+            st_k<K>(reinterpret_cast<V *>(a.root_out) + (size_t)s * kBRow, pos0, root);
         }
         if (a.sum_out) {
             V part = V(0);
+            V rv[K];
+            ld_k<K>(rng + p * kBRow, pos0, rv);
 #pragma unroll
-            for (int k = 0; k < K; k++) {
-                const int pos = pos0 + k;
-                if (pos < kBRow) part += mul(V(rng[p * kBRow + pos]), root[k]);
-            }
+            for (int k = 0; k < K; k++)
+                if (pos0 + k < kBRow) part += mul(rv[k], root[k]);
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(FULL, part, off);
             if (lane == 0) S.wsum[warp] = part;
