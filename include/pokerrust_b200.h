@@ -287,6 +287,66 @@ int pr_mlp_get_layer(void *net, int l, float *W, float *b);
 int pr_mlp_set_layer(void *net, int l, const float *W, const float *b);
 int pr_mlp_get_grad(void *net, int l, float *dW, float *db);
 
+/* ---- full fixed-flop game with general bets (extension; no reference counterpart) ----
+ * Flop and turn streets with pot-fraction bets (rules in the source of pr_full_tree), a
+ * chance node dealing the 49 turn cards, and at the end of the turn a river chance node whose
+ * 48 river subgames (pr_subgame trees with the leaf's pot and stack) are solved by the batched
+ * river solver in the same pass. CFR with regrets clipped at zero, alternating players; the
+ * average strategy is the reach-weighted sum. Net-leaf mode answers the leaves with chips
+ * behind by the value network instead. */
+typedef struct {
+    float fracs[4];     /* bet and raise sizes as pot fractions */
+    int32_t nfrac;      /* 0..4 */
+    int32_t allin;      /* all-in is an option */
+    int32_t max_raises; /* bets + raises on the street, 0..4 */
+} pr_street;
+typedef struct {
+    uint64_t flop;          /* 3 cards */
+    float pot;              /* chips in the pot before the flop, pot/2 from each player */
+    float stack;            /* chips behind each player */
+    pr_street street[2];    /* flop, turn */
+    uint32_t river_sizes;   /* river subgames: pr_subgame.sizes */
+    int32_t river_raises;   /* river subgames: pr_subgame.max_raises */
+} pr_full_spec;
+
+/* The flop and turn nodes on the host: 48-byte nodes in pre-order and the child list (see
+ * full_tree.h for the layout); null outputs are skipped. 2 if the spec is bad or the
+ * outputs are too small. */
+int pr_full_tree(const pr_full_spec *spec, void *nodes_out, int max_nodes, int *num_nodes, int *num_edges,
+                 int *num_leaves, int *kids_out, int max_kids);
+/* ranges: [2][1326] floats (hands touching the flop are ignored). Null on failure. */
+void *pr_full_new(const pr_full_spec *spec, const float *ranges);
+void pr_full_free(void *game);
+int pr_full_shape(void *game, int *num_nodes, int *num_edges, int *num_leaves, int *bet_subgames,
+                  int *allin_subgames);
+/* Net-leaf mode on (a pr_mlp_new network) or off (null). */
+int pr_full_set_net(void *game, void *net);
+/* Average sums weighted by the iteration number (1, the default) or uniformly (0). */
+int pr_full_set_linear_average(void *game, int on);
+/* One CFR half-iteration for `player`; pr_full_iterate: whole iterations (one CUDA graph each
+ * without a network). */
+int pr_full_pass(void *game, int player);
+int pr_full_iterate(void *game, int iterations);
+/* FP64 best responses to the average strategies over the whole game and the exploitability
+ * (br0 + br1) / 2 per unit of joint range mass, in chips. resolve_iterations > 0 first
+ * re-solves the river subgames of the leaves with chips behind from zero under the current
+ * average flop and turn strategies (for net-leaf strategies, which stop at the turn). */
+int pr_full_exploitability(void *game, int resolve_iterations, double *br0, double *br1, double *expl);
+/* Device state: which 0 regrets / 1 average sums [edges][1326] f32; 2 reach [nodes][2][1326],
+ * 3 leaf values [leaves][1326], 4 node values [nodes][1326] (f32, last CFR pass); 5, 6, 7
+ * the same in f64 from the last best response; 8 network inputs [net leaves][2][1326] and
+ * 9 reach masses [net leaves][2] (f32, last net-leaf pass). pr_full_write: which 0 or 1. */
+int pr_full_read(void *game, int which, void *out);
+/* Zeroes every regret and average sum (flop, turn and river subgames). */
+int pr_full_reset(void *game);
+int pr_full_write(void *game, int which, const void *in);
+/* River subgame batches (0: leaves with chips behind, 1: all-in leaves; subgame j * 48 + k is
+ * river card k, in card order, of the batch's j-th leaf), their leaf node ids, and the joint
+ * mass of the initial ranges. */
+void *pr_full_batch(void *game, int which);
+int pr_full_batch_leaves(void *game, int which, int *nodes_out);
+double pr_full_joint(void *game);
+
 #ifdef __cplusplus
 }
 #endif

@@ -135,7 +135,7 @@ int flatten(const Node *n, int parent, int in_edge, int depth, Flat &f) {
 }
 
 bool make_tree(float pot, float stack, uint32_t sizes, int max_raises, Flat &f) {
-    if (!(pot > 0) || !(stack > 0) || !(sizes & 7) || max_raises < 1) return false;
+    if (!(pot > 0) || !(stack >= 0) || !(sizes & 7) || max_raises < 1) return false;
     Spec sp{pot, stack, sizes & 7u, max_raises};
     auto root = grow(sp, 0.0f, 0.0f, 0, 0);
     flatten(root.get(), -1, -1, 0, f);

@@ -10,6 +10,7 @@ from .interface import (  # noqa: F401
     SPEC_DTYPE,
     Batch,
     Builder,
+    FullGame,
     Game,
     PokerLibError,
     ValueNet,
@@ -18,6 +19,8 @@ from .interface import (  # noqa: F401
     build_flop_tables,
     build_river,
     card_order,
+    full_spec,
+    full_tree,
     download_gpu,
     evaluate_gpu,
     export_tables,

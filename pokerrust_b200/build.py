@@ -10,7 +10,7 @@ LIB_DIR = os.path.join(HERE, "_lib")
 SO_PATH = os.path.join(LIB_DIR, "libpokerrust_b200.so")
 A_PATH = os.path.join(LIB_DIR, "libpoker.a")
 SOURCES = ["abi.cu", "river_cfr.cu", "pack_boards.cu", "gen_tables.cu", "game.cu", "upper_tree.cu",
-           "batch_solver.cu", "batch_api.cu", "mlp_gemm.cu", "mlp.cu"]
+           "batch_solver.cu", "batch_api.cu", "mlp_gemm.cu", "mlp.cu", "full_game.cu"]
 # sources built on CuTe's sm100 atoms (tcgen05 MMA, TMA, TMEM): they need the CUTLASS headers
 CUTE_SOURCES = {"mlp_gemm.cu", "mlp.cu"}
 NVCC_FLAGS = [

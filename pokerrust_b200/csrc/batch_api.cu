@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/pokerrust_b200.h"
+#include "batch_internal.h"
 #include "batch_solver.h"
 #include "device_common.cuh"
 
@@ -53,6 +54,9 @@ struct Batch {
     BNode *d_nodes = nullptr;
     BPack *d_packs = nullptr;
     float *d_ranges = nullptr;
+    double *d_ranges64 = nullptr;  // [count][2][kBRow] double ranges of best responses inside a larger game
+    bool own_weight = false;       // CFR average sums weighted by the updater's range
+    const float *avg_weight = nullptr;  // device scalar weighting CFR average-sum terms (null: 1)
     float *d_regrets = nullptr, *d_avg = nullptr;
     int *d_order = nullptr, *d_head = nullptr, *d_err = nullptr;
     void *d_sum = nullptr;   // [count] doubles
@@ -65,8 +69,9 @@ struct Batch {
     ~Batch() {
         if (graph) cudaGraphExecDestroy(graph);
         if (stream) cudaStreamSynchronize(stream);
-        for (void *p : {(void *)d_subs, (void *)d_nodes, (void *)d_packs, (void *)d_ranges, (void *)d_regrets,
-                        (void *)d_avg, (void *)d_order, (void *)d_head, (void *)d_err, d_sum, d_root, d_child})
+        for (void *p : {(void *)d_subs, (void *)d_nodes, (void *)d_packs, (void *)d_ranges, (void *)d_ranges64,
+                        (void *)d_regrets, (void *)d_avg, (void *)d_order, (void *)d_head, (void *)d_err, d_sum,
+                        d_root, d_child})
             cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -97,7 +102,7 @@ struct Batch {
 
     // one pass of `mode` for `player` over every class; heads [slot*kClasses + c] must be zero
     int pass(int mode, int player, int fp64, int use_average, void *root_out, void *sum_out, int slot,
-             void *child_out = nullptr) {
+             void *child_out = nullptr, cudaStream_t on = nullptr) {
         for (int c = 0; c < kClasses; c++) {
             const ClassCfg &k = cls[c];
             if (!k.count) continue;
@@ -116,9 +121,13 @@ struct Batch {
             a.root_out = root_out;
             a.sum_out = sum_out;
             a.child_out = child_out;
+            a.ranges64 = fp64 ? d_ranges64 : nullptr;
+            a.own_reach = own_weight;
+            a.avg_weight = avg_weight;
             const int ctas = std::min(k.count, std::max(1, k.per_sm) * sms);
             const int group = batch_group_leaves(fp64);
-            cudaError_t e = launch_batch_pass(mode, k.K, fp64, mode == kBModeCFR && avg_on, a, ctas, group, stream);
+            cudaError_t e = launch_batch_pass(mode, k.K, fp64, mode == kBModeCFR && avg_on, a, ctas, group,
+                                              on ? on : stream);
             if (e != cudaSuccess) return bfail("pass launch", e);
         }
         return 0;
@@ -163,6 +172,65 @@ int *noalloc_scratch() {
 }
 
 }  // namespace
+
+int batch_view(void *batch, BatchView *v, bool need64) {
+    Batch *b = (Batch *)batch;
+    if (!b || !v) return 2;
+    if (need64 && !b->d_ranges64) {
+        const size_t bytes = sizeof(double) * 2 * kBRow * b->count;
+        cudaError_t e = cudaMalloc(&b->d_ranges64, bytes);
+        if (e == cudaSuccess) e = cudaMemset(b->d_ranges64, 0, bytes);
+        if (e != cudaSuccess) return bfail("double range allocation", e);
+    }
+    v->packs = b->d_packs;
+    v->ranges = b->d_ranges;
+    v->ranges64 = b->d_ranges64;
+    v->count = b->count;
+    v->stream = b->stream;
+    return 0;
+}
+
+int batch_set_own_weight(void *batch, bool on) {
+    Batch *b = (Batch *)batch;
+    if (!b) return 2;
+    if (b->own_weight != on && b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->own_weight = on;
+    return 0;
+}
+
+int batch_set_avg_weight(void *batch, const float *weight) {
+    Batch *b = (Batch *)batch;
+    if (!b) return 2;
+    if (b->avg_weight != weight && b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->avg_weight = weight;
+    return 0;
+}
+
+int batch_run_pass(void *batch, int mode, int player, int fp64, int use_average, void *root_out,
+                   cudaStream_t on) {
+    Batch *b = (Batch *)batch;
+    if (!b || (use_average && !b->avg_on) || (mode == kBModeCFR && fp64)) return 2;
+    const int slot = 3;  // heads of this slot are reset here, on the caller's stream
+    cudaError_t e = cudaMemsetAsync(b->d_head + slot * kClasses, 0, sizeof(int) * kClasses, on);
+    if (e != cudaSuccess) return bfail("queue reset", e);
+    return b->pass(mode, player, fp64, use_average, root_out, nullptr, slot, nullptr, on);
+}
+
+int batch_clear(void *batch, cudaStream_t on) {
+    Batch *b = (Batch *)batch;
+    if (!b) return 2;
+    const size_t rows = (size_t)b->total_edges * kBRow * sizeof(float);
+    cudaError_t e = cudaMemsetAsync(b->d_regrets, 0, rows, on);
+    if (e == cudaSuccess && b->d_avg) e = cudaMemsetAsync(b->d_avg, 0, rows, on);
+    return e == cudaSuccess ? 0 : bfail("clear", e);
+}
+
 }  // namespace prb
 
 using namespace prb;

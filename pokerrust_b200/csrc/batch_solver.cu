@@ -318,6 +318,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
     const unsigned FULL = 0xffffffffu;
     const int p = a.player, o = 1 - p;
     const float *src_all = USEAVG ? a.avg : a.regrets;
+    // weight of this pass's average-sum terms (1 unless the caller weights iterations)
+    const float wavg = AVG && a.avg_weight ? *a.avg_weight : 1.0f;
 
     // The next queue entry is taken (and its rows prefetched into L2) while the current one
     // is solved.
@@ -439,9 +441,16 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                 const int d = nd.depth;
                 V npo[K], npp[K];
                 if (td == 0) {
-                    ld_k<K>(rng + o * kBRow, pos0, npo);
+                    if (sizeof(V) == 8 && a.ranges64)
+                        ld_k<K>(a.ranges64 + ((size_t)s * 2 + o) * kBRow, pos0, npo);
+                    else
+                        ld_k<K>(rng + o * kBRow, pos0, npo);
+                    if (MODE == kBModeCFR && a.own_reach) {
+                        ld_k<K>(rng + p * kBRow, pos0, npp);
+                    } else {
 #pragma unroll
-                    for (int k = 0; k < K; k++) npp[k] = V(1);
+                        for (int k = 0; k < K; k++) npp[k] = V(1);
+                    }
                 } else {
                     const BNode pm = S.tn[nd.parent];
                     const bool own = pm.actor == p;
@@ -462,7 +471,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                             float av[K];
                             ld_k<K>(A + ro, pos0, av);
 #pragma unroll
-                            for (int k = 0; k < K; k++) av[k] += float(npp[k]);
+                            for (int k = 0; k < K; k++) av[k] += wavg * float(npp[k]);
                             st_k<K>(A + ro, pos0, av);
                         }
                     }

@@ -55,6 +55,10 @@ struct BLaunch {
     void *root_out;       // [subgame][kBRow] root values of `player` (V), or null
     void *sum_out;        // [subgame] sum over hands of range x root value (V), or null
     void *child_out;      // [subgame][8][kBRow] values of the root's children (V), or null
+    const double *ranges64;  // double passes: [subgame][2][kBRow] opponent weights, or null (use ranges)
+    int own_reach;        // CFR: average sums weighted by the updater's range (subgames inside a larger
+                          // game, whose ranges change between iterations), not by 1
+    const float *avg_weight;  // CFR: device scalar multiplying this pass's average-sum terms, or null (1)
 };
 
 // Builds the packs and position-order ranges of `count` subgames: ranges_in holds

@@ -3,8 +3,9 @@
 // its C ABI.
 //
 // Rules. Player 0 acts first. Both players have put pot/2 into the pot before the river
-// and have `stack` chips behind. `sizes` enables bets of 0.5 pot (bit 0), 1 pot (bit 1) and
-// all-in (bit 2); at most `max_raises` bets and raises happen on the river.
+// and have `stack` chips behind (0 after an all-in: both check to the showdown). `sizes`
+// enables bets of 0.5 pot (bit 0), 1 pot (bit 1) and all-in (bit 2); at most `max_raises`
+// bets and raises happen on the river.
 //  * Not facing a bet: check, or bet each enabled size. A fractional bet is
 //    frac x (pot + both players' river chips), capped at the player's remaining stack;
 //    all-in is the remaining stack. Amounts that coincide with an earlier option are dropped.
@@ -53,7 +54,7 @@ inline bool build_bet_tree(float pot, float stack, uint32_t sizes, int max_raise
     t->nodes.clear();
     t->edge_owner.clear();
     t->num_edges = t->num_leaves = t->depth = 0;
-    if (!(pot > 0.0f) || !(stack > 0.0f) || (sizes & 7u) == 0 || max_raises < 1) return false;
+    if (!(pot > 0.0f) || !(stack >= 0.0f) || (sizes & 7u) == 0 || max_raises < 1) return false;
     struct St {
         float c[2];    // river chips of each player
         int actor, raises;

@@ -1,0 +1,158 @@
+"""Full fixed-flop solve with general bets: the plain river traversal against value-network
+leaves, on one GPU.
+
+    python -m pokerrust_b200.full_solve --config small --iterations 400 --check 50
+
+Both forms run CFR on the same game: flop and turn streets on the device, and at the end of
+the turn either the 48 river subgames of each leaf (plain, the batched river solver) or the
+turn-leaf value network (net-leaf; all-in leaves keep their betting-free river subgames).
+Every `check` iterations the FP64 exploitability of the average strategies is measured: for
+the net-leaf form after re-solving the river subgames under its flop and turn strategies
+(`--resolve` iterations), since its strategy stops at the turn. The network is trained first
+on turn-leaf states of this game (the leaves' boards, pots and stacks with random ranges),
+valued by the batched river solver and the adjoint. Prints one JSON line: the game's size,
+both trajectories (iterations, solver seconds, exploitability in % of the starting pot),
+when each first reached the target, and the network's data and training cost.
+"""
+import argparse
+import json
+import sys
+import time
+
+import numpy as np
+
+from . import interface as P
+from . import train_value_net as T
+from . import value_data as D
+
+CONFIGS = {
+    # 0.75-pot bets and all-in, one bet or raise per street, stacks 10x the pot
+    "small": dict(pot=10.0, stack=100.0, fracs=(0.75,), allin=True, raises=1),
+    # the large game's sizes (0.33, 0.75, 1.5 pot, all-in) and 50x stacks, one bet or raise per street
+    "large": dict(pot=10.0, stack=500.0, fracs=(0.33, 0.75, 1.5), allin=True, raises=1),
+}
+
+
+def seeded_game(config, seed):
+    """(spec, ranges): a seeded flop and both ranges U(0,1) with 30 % of the hands zeroed
+    (hands on the flop zeroed), each normalised to sum 1."""
+    c = CONFIGS[config]
+    rng = np.random.default_rng(seed)
+    flop = 0
+    for card in rng.choice(52, 3, replace=False):
+        flop |= 1 << int(card)
+    order = P.card_order()
+    ranges = rng.random((2, P.HANDS)).astype(np.float32)
+    ranges[rng.random(ranges.shape) < 0.3] = 0.0
+    ranges[:, (order & np.uint64(flop)) != 0] = 0.0
+    ranges /= ranges.sum(axis=1, keepdims=True)
+    spec = P.full_spec(flop, c["pot"], c["stack"], flop_fracs=c["fracs"], flop_allin=c["allin"],
+                       flop_raises=c["raises"], turn_fracs=c["fracs"], turn_allin=c["allin"],
+                       turn_raises=c["raises"], river_sizes=D.RIVER_SIZES, river_raises=D.RIVER_RAISES)
+    return spec, ranges
+
+
+def trajectory(game, iterations, check, pot, target_pct, resolve=0):
+    """CFR in steps of `check` iterations; after each step the FP64 exploitability (solver
+    seconds exclude the measurement)."""
+    points, reached = [], None
+    done, solver_s = 0, 0.0
+    while done < iterations:
+        n = min(check, iterations - done)
+        t0 = time.perf_counter()
+        game.iterate(n)
+        solver_s += time.perf_counter() - t0
+        done += n
+        t0 = time.perf_counter()
+        _, _, ex = game.exploitability(resolve_iterations=resolve)
+        pct = 100.0 * ex / pot
+        points.append({"iterations": done, "solver_s": solver_s, "pct_pot": pct,
+                       "measure_s": time.perf_counter() - t0})
+        if reached is None and pct <= target_pct:
+            reached = {"iterations": done, "solver_s": solver_s}
+    return points, reached
+
+
+def leaf_dataset(spec, n, seed, iterations):
+    """n turn-leaf states of the game: a random leaf with chips behind (its 4-card board, pot
+    and stack) and random ranges (U(0,1), 25 % zeroed, board hands zeroed, normalised), valued
+    over the 48 rivers by the batched solver (pot-normalised counterfactual values)."""
+    nodes, _, _, _ = P.full_tree(spec)
+    leaves = nodes[(nodes["kind"] == 3) & (nodes["stack"] > 0)]
+    rng = np.random.default_rng(seed)
+    pick = leaves[rng.integers(0, len(leaves), n)]
+    boards = pick["board"].astype(np.uint64)
+    pots = pick["stake"].astype(np.float32)
+    stacks = pick["stack"].astype(np.float32)
+    order = P.card_order()
+    ranges = np.zeros((n, 2, P.HANDS), np.float32)
+    for i in range(n):
+        live = (order & boards[i]) == 0
+        for p in range(2):
+            r = rng.random(P.HANDS, dtype=np.float32)
+            r[rng.random(P.HANDS) < 0.25] = 0.0
+            r[~live] = 0.0
+            ranges[i, p] = r / r.sum()
+    values = np.zeros((n, 2, P.HANDS), np.float32)
+    solve_s = 0.0
+    for s in range(0, n, 256):
+        e = min(n, s + 256)
+        values[s:e], dt = D.river_values(boards[s:e], ranges[s:e], pots[s:e], stacks[s:e], iterations)
+        solve_s += dt
+    scalars = np.stack([pots / 200.0, stacks / (10.0 * pots)], axis=1).astype(np.float32)
+    return dict(boards=boards, ranges=ranges, scalars=scalars, values=values, pots=pots, stacks=stacks,
+                solve_s=solve_s)
+
+
+def run(config, seed, iterations, check, target_pct, samples, river_iterations, epochs, resolve, net_iterations):
+    import torch
+    spec, ranges = seeded_game(config, seed)
+    pot = CONFIGS[config]["pot"]
+    out = {"config": config, "seed": seed, "target_pct_pot": target_pct}
+    t0 = time.perf_counter()
+    g = P.FullGame(spec, ranges)
+    out["game"] = {"nodes": g.nodes, "edges": g.edges, "leaves": g.leaves, "river_subgames": g.bet_subgames,
+                   "allin_subgames": g.allin_subgames, "setup_s": time.perf_counter() - t0}
+    pts, reached = trajectory(g, iterations, check, pot, target_pct)
+    out["plain"] = {"trajectory": pts, "reached": reached}
+    # the network: data from this game's leaves, then training
+    t0 = time.perf_counter()
+    data = leaf_dataset(spec, samples, seed + 1, river_iterations)
+    gen_s = time.perf_counter() - t0
+    net = P.ValueNet(rows=256, seed=seed)
+    t0 = time.perf_counter()
+    curve = T.train(net, data, np.arange(samples), epochs, 256, 1e-3, seed)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    out["network"] = {"samples": samples, "river_iterations": river_iterations, "generation_s": gen_s,
+                      "epochs": epochs, "train_s": train_s, "final_loss": curve[-1] if curve else None}
+    g.reset()
+    g.set_net(net)
+    pts, reached = trajectory(g, net_iterations, check, pot, target_pct, resolve=resolve)
+    out["net_leaf"] = {"trajectory": pts, "reached": reached, "resolve_iterations": resolve}
+    g.set_net(None)
+    g.close()
+    net.close()
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", default="small", choices=sorted(CONFIGS))
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--iterations", type=int, default=400)
+    ap.add_argument("--net-iterations", type=int, default=400)
+    ap.add_argument("--check", type=int, default=50)
+    ap.add_argument("--target", type=float, default=0.5, help="exploitability target, % of the starting pot")
+    ap.add_argument("--samples", type=int, default=2048)
+    ap.add_argument("--river-iterations", type=int, default=200)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--resolve", type=int, default=200)
+    a = ap.parse_args(argv)
+    print(json.dumps(run(a.config, a.seed, a.iterations, a.check, a.target, a.samples, a.river_iterations,
+                         a.epochs, a.resolve, a.net_iterations)), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

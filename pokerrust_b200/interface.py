@@ -32,6 +32,26 @@ SPEC_DTYPE = np.dtype([("board", "<u8"), ("pot", "<f4"), ("stack", "<f4"), ("siz
                        ("max_raises", "<i4")])
 
 
+class StreetRules(ctypes.Structure):
+    """pr_street: bet sizes of one street (pot fractions, all-in, raise cap)."""
+    _fields_ = [("fracs", ctypes.c_float * 4), ("nfrac", ctypes.c_int32), ("allin", ctypes.c_int32),
+                ("max_raises", ctypes.c_int32)]
+
+
+class FullSpec(ctypes.Structure):
+    """pr_full_spec: a fixed-flop game with general bets on the flop and turn and river
+    subgames at the end of the turn."""
+    _fields_ = [("flop", ctypes.c_uint64), ("pot", ctypes.c_float), ("stack", ctypes.c_float),
+                ("street", StreetRules * 2), ("river_sizes", ctypes.c_uint32), ("river_raises", ctypes.c_int32)]
+
+
+# the host tree's 48-byte nodes (full_tree.h: FNode)
+FNODE_DTYPE = np.dtype([("kind", "u1"), ("actor", "u1"), ("nchild", "u1"), ("street", "u1"), ("parent", "<i4"),
+                        ("in_edge", "<i4"), ("edge", "<i4"), ("kids", "<i4"), ("level", "<i4"),
+                        ("stake", "<f4"), ("stack", "<f4"), ("pad", "<u4"), ("board", "<u8")], align=True)
+assert FNODE_DTYPE.itemsize == 48
+
+
 class PokerLibError(RuntimeError):
     pass
 
@@ -188,6 +208,36 @@ def lib():
         L.pr_tables_save.argtypes = [vp, ctypes.c_char_p]
         L.pr_tables_load.restype = vp
         L.pr_tables_load.argtypes = [ctypes.c_char_p]
+        fs = ctypes.POINTER(FullSpec)
+        L.pr_full_tree.restype = i32
+        L.pr_full_tree.argtypes = [fs, vp, i32, vp, vp, vp, vp, i32]
+        L.pr_full_new.restype = vp
+        L.pr_full_new.argtypes = [fs, vp]
+        L.pr_full_free.argtypes = [vp]
+        L.pr_full_shape.restype = i32
+        L.pr_full_shape.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.pr_full_set_net.restype = i32
+        L.pr_full_set_net.argtypes = [vp, vp]
+        L.pr_full_pass.restype = i32
+        L.pr_full_pass.argtypes = [vp, i32]
+        L.pr_full_iterate.restype = i32
+        L.pr_full_iterate.argtypes = [vp, i32]
+        L.pr_full_exploitability.restype = i32
+        L.pr_full_exploitability.argtypes = [vp, i32, vp, vp, vp]
+        L.pr_full_read.restype = i32
+        L.pr_full_read.argtypes = [vp, i32, vp]
+        L.pr_full_set_linear_average.restype = i32
+        L.pr_full_set_linear_average.argtypes = [vp, i32]
+        L.pr_full_reset.restype = i32
+        L.pr_full_reset.argtypes = [vp]
+        L.pr_full_write.restype = i32
+        L.pr_full_write.argtypes = [vp, i32, vp]
+        L.pr_full_batch.restype = vp
+        L.pr_full_batch.argtypes = [vp, i32]
+        L.pr_full_batch_leaves.restype = i32
+        L.pr_full_batch_leaves.argtypes = [vp, i32, vp]
+        L.pr_full_joint.restype = ctypes.c_double
+        L.pr_full_joint.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -634,10 +684,21 @@ class Batch:
     def iteration_bytes(self):
         return lib().pr_batch_iteration_bytes(self.ptr)
 
+    @classmethod
+    def _borrow(cls, ptr):
+        """A view of a batch owned by another object (not freed by close())."""
+        b = cls.__new__(cls)
+        b.ptr = ptr
+        b.count = lib().pr_batch_count(ptr)
+        b.specs = None
+        b.ranges = None
+        b._borrowed = True
+        return b
+
     def close(self):
-        if self.ptr:
+        if self.ptr and not getattr(self, "_borrowed", False):
             lib().pr_batch_free(self.ptr)
-            self.ptr = None
+        self.ptr = None
 
     def __del__(self):
         try:
@@ -704,6 +765,148 @@ class ValueNet:
     def close(self):
         if self.ptr:
             lib().pr_mlp_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- full fixed-flop game with general bets ----
+
+def full_spec(flop, pot, stack, flop_fracs=(0.75,), flop_allin=True, flop_raises=1, turn_fracs=(0.75,),
+              turn_allin=True, turn_raises=1, river_sizes=0b011, river_raises=2):
+    """A FullSpec: 3-card flop mask, pot before the flop, chips behind, per-street sizes."""
+    sp = FullSpec()
+    sp.flop = int(flop)
+    sp.pot = float(pot)
+    sp.stack = float(stack)
+    for i, (fr, ai, rz) in enumerate(((flop_fracs, flop_allin, flop_raises), (turn_fracs, turn_allin, turn_raises))):
+        fr = list(fr)
+        assert len(fr) <= 4
+        for k, f in enumerate(fr):
+            sp.street[i].fracs[k] = float(f)
+        sp.street[i].nfrac = len(fr)
+        sp.street[i].allin = int(bool(ai))
+        sp.street[i].max_raises = int(rz)
+    sp.river_sizes = int(river_sizes)
+    sp.river_raises = int(river_raises)
+    return sp
+
+
+def full_tree(spec):
+    """The flop and turn nodes (FNODE_DTYPE array in pre-order), the child list, edge and
+    leaf counts."""
+    n, e, l = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().pr_full_tree(ctypes.byref(spec), None, 0, ctypes.byref(n), ctypes.byref(e), ctypes.byref(l),
+                              None, 0), "pr_full_tree")
+    nodes = np.zeros(n.value, FNODE_DTYPE)
+    kids = np.zeros(max(1, 64 * n.value), np.int32)
+    _check(lib().pr_full_tree(ctypes.byref(spec), nodes.ctypes.data_as(ctypes.c_void_p), n.value, None, None,
+                              None, kids.ctypes.data_as(ctypes.c_void_p), len(kids)), "pr_full_tree")
+    used = 0
+    for nd in nodes:
+        if nd["kind"] in (0, 2):
+            used = max(used, int(nd["kids"]) + int(nd["nchild"]))
+    return nodes, kids[:used], e.value, l.value
+
+
+class FullGame:
+    """A fixed-flop game with general bets on every street, solved on the device: flop and
+    turn by level-synchronous sweeps, the river by the batched river solver (pr_full_*)."""
+
+    def __init__(self, spec, ranges):
+        self.spec = spec
+        ranges = np.ascontiguousarray(ranges, np.float32).reshape(2, HANDS)
+        self.ptr = lib().pr_full_new(ctypes.byref(spec), _ptr(ranges))
+        if not self.ptr:
+            raise PokerLibError("pr_full_new failed (bad spec or allocation; see stderr)")
+        n, e, l, b, a = (ctypes.c_int() for _ in range(5))
+        _check(lib().pr_full_shape(self.ptr, ctypes.byref(n), ctypes.byref(e), ctypes.byref(l), ctypes.byref(b),
+                                   ctypes.byref(a)), "pr_full_shape")
+        self.nodes, self.edges, self.leaves = n.value, e.value, l.value
+        self.bet_subgames, self.allin_subgames = b.value, a.value
+        self.joint = lib().pr_full_joint(self.ptr)
+        self._net = None
+
+    def set_net(self, net):
+        """Net-leaf mode with a ValueNet, or plain river subgames (None)."""
+        self._net = net
+        _check(lib().pr_full_set_net(self.ptr, net.ptr if net is not None else None), "pr_full_set_net")
+
+    def set_linear_average(self, on):
+        """Average sums weighted by the iteration number (True, the default) or by 1."""
+        _check(lib().pr_full_set_linear_average(self.ptr, int(bool(on))), "pr_full_set_linear_average")
+
+    def half_iteration(self, player):
+        _check(lib().pr_full_pass(self.ptr, int(player)), "pr_full_pass")
+
+    def iterate(self, iterations=1):
+        _check(lib().pr_full_iterate(self.ptr, int(iterations)), "pr_full_iterate")
+
+    def exploitability(self, resolve_iterations=0):
+        """(BR0, BR1, exploitability per unit of joint mass in chips), FP64."""
+        b0, b1, ex = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(lib().pr_full_exploitability(self.ptr, int(resolve_iterations), ctypes.byref(b0), ctypes.byref(b1),
+                                            ctypes.byref(ex)), "pr_full_exploitability")
+        return b0.value, b1.value, ex.value
+
+    def _read(self, which, shape, dtype):
+        out = np.zeros(shape, dtype)
+        _check(lib().pr_full_read(self.ptr, int(which), out.ctypes.data_as(ctypes.c_void_p)), "pr_full_read")
+        return out
+
+    def regrets(self):
+        return self._read(0, (self.edges, HANDS), np.float32)
+
+    def average(self):
+        return self._read(1, (self.edges, HANDS), np.float32)
+
+    def reach(self, fp64=False):
+        return self._read(5 if fp64 else 2, (self.nodes, 2, HANDS), np.float64 if fp64 else np.float32)
+
+    def leaf_values(self, fp64=False):
+        return self._read(6 if fp64 else 3, (self.leaves, HANDS), np.float64 if fp64 else np.float32)
+
+    def node_values(self, fp64=False):
+        return self._read(7 if fp64 else 4, (self.nodes, HANDS), np.float64 if fp64 else np.float32)
+
+    def net_inputs(self):
+        """Normalised ranges [net leaves][2][1326] and reach masses [net leaves][2] of the last
+        net-leaf pass (leaves in batch_leaves(0) order)."""
+        n = self.bet_subgames // 48
+        return self._read(8, (n, 2, HANDS), np.float32), self._read(9, (n, 2), np.float32)
+
+    def _write(self, which, data):
+        data = np.ascontiguousarray(data, np.float32).reshape(self.edges, HANDS)
+        _check(lib().pr_full_write(self.ptr, int(which), _ptr(data)), "pr_full_write")
+
+    def set_regrets(self, data):
+        self._write(0, data)
+
+    def reset(self):
+        """Zero regrets and average sums everywhere (flop, turn, river subgames)."""
+        _check(lib().pr_full_reset(self.ptr), "pr_full_reset")
+
+    def set_average(self, data):
+        self._write(1, data)
+
+    def batch(self, which):
+        """The river subgames of the leaves with chips behind (0) or all-in (1), or None."""
+        p = lib().pr_full_batch(self.ptr, int(which))
+        return Batch._borrow(p) if p else None
+
+    def batch_leaves(self, which):
+        n = lib().pr_full_batch_leaves(self.ptr, int(which), None)
+        out = np.zeros(max(1, n), np.int32)
+        lib().pr_full_batch_leaves(self.ptr, int(which), out.ctypes.data_as(ctypes.c_void_p))
+        return out[:n]
+
+    def close(self):
+        if self.ptr:
+            lib().pr_full_free(self.ptr)
             self.ptr = None
 
     def __del__(self):
