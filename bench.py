@@ -198,6 +198,45 @@ def batch_section(P, rank, peak, cpu_threads, with_cpu):
     return out
 
 
+def full_game_section(P):
+    """The full fixed-flop game with general bets (flop and turn sweeps over batched river
+    subgames): CFR iteration time, river subgames solved per second, iterations / solver
+    seconds until the FP64 exploitability of the average strategies is at most 0.5 % of the
+    starting pot, and the iteration time with value-network leaves (untrained network: the
+    time does not depend on the weights)."""
+    from pokerrust_b200 import full_solve as FS
+    spec, ranges = FS.seeded_game("small", 7)
+    pot = FS.CONFIGS["small"]["pot"]
+    g = P.FullGame(spec, ranges)
+    g.iterate(3)  # the first iteration runs eagerly, then one iteration is captured as a graph
+    steps = 20
+    t0 = time.perf_counter()
+    g.iterate(steps)
+    it_s = (time.perf_counter() - t0) / steps
+    out = {
+        "workload": "fixed flop (seed 7), pot 10, stacks 100, flop and turn bets 0.75 pot / all-in with one "
+                    "bet or raise per street, river subgames with 0.5 / 1 pot bets and two raises; ranges "
+                    "U(0,1) with 30 % zeroed",
+        "nodes": g.nodes, "leaves": g.leaves, "river_subgames": g.bet_subgames + g.allin_subgames,
+        "iteration_ms": it_s * 1e3,
+        "river_subgame_solves_per_s": 2 * (g.bet_subgames + g.allin_subgames) / it_s,
+    }
+    g.reset()
+    pts, reached = FS.trajectory(g, 300, 50, pot, 0.5)
+    out["exploitability_pct_pot"] = [(p["iterations"], round(p["pct_pot"], 4)) for p in pts]
+    out["time_to_0.5pct_pot"] = reached
+    net = P.ValueNet(rows=512, seed=1)
+    g.set_net(net)
+    g.iterate(2)
+    t0 = time.perf_counter()
+    g.iterate(steps)
+    out["net_leaf_iteration_ms"] = (time.perf_counter() - t0) / steps * 1e3
+    g.set_net(None)
+    net.close()
+    g.close()
+    return out
+
+
 def value_net_section(P, peak_tflops, peak_sustained):
     """The turn-leaf value network: tensor-core throughput of training steps at batch 4096
     (random inputs; 6 x 8.64 M x 4096 FLOP per step), and a small train / held-out run on
@@ -464,6 +503,7 @@ def run_gpu(args):
     batch = batch_section(P, rank, measured_peaks()[0], os.cpu_count() or 1, rank == 0)
     tp = tensor_peaks()
     vnet = value_net_section(P, tp[0], tp[1])
+    full = full_game_section(P)
 
     line = None
     if rank == 0:
@@ -500,6 +540,7 @@ def run_gpu(args):
             "clocks": clk,
             "batch_subgames": batch,
             "value_network": vnet,
+            "full_game": full,
             "game_iteration": {"ms": dev_iter_s * 1e3,
                                "note": "one full CFR iteration of the fixed-flop game (both players): "
                                        "upper tree and river passes on the device, one CUDA graph",

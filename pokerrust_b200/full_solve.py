@@ -9,8 +9,9 @@ turn-leaf value network (net-leaf; all-in leaves keep their betting-free river s
 Every `check` iterations the FP64 exploitability of the average strategies is measured: for
 the net-leaf form after re-solving the river subgames under its flop and turn strategies
 (`--resolve` iterations), since its strategy stops at the turn. The network is trained first
-on turn-leaf states of this game (the leaves' boards, pots and stacks with random ranges),
-valued by the batched river solver and the adjoint. Prints one JSON line: the game's size,
+on turn-leaf states of this game (the leaves' boards, pots and stacks; ranges from random
+strategy profiles of the game and random ranges), valued by the batched river solver and
+the adjoint. Prints one JSON line: the game's size,
 both trajectories (iterations, solver seconds, exploitability in % of the starting pot),
 when each first reached the target, and the network's data and training cost.
 """
@@ -73,20 +74,54 @@ def trajectory(game, iterations, check, pot, target_pct, resolve=0):
     return points, reached
 
 
-def leaf_dataset(spec, n, seed, iterations):
-    """n turn-leaf states of the game: a random leaf with chips behind (its 4-card board, pot
-    and stack) and random ranges (U(0,1), 25 % zeroed, board hands zeroed, normalised), valued
-    over the 48 rivers by the batched solver (pot-normalised counterfactual values)."""
+def leaf_ranges(game, n, rng, per_draw=64):
+    """Ranges at the game's leaves with chips behind under random flop and turn strategies:
+    each draw sets random regrets (uniform values raised to a random power, 30 % zeroed), runs
+    one pass and takes the reach of `per_draw` random leaves, normalised. Returns the leaf
+    node ids and ranges [n][2][1326]."""
+    nodes = game.batch_leaves(0)
+    saved = game.regrets()
+    ids, out = [], []
+    while len(ids) < n:
+        reg = rng.random((game.edges, P.HANDS), dtype=np.float32) ** rng.uniform(1.0, 8.0)
+        reg[rng.random(reg.shape) < 0.3] = 0.0
+        game.set_regrets(reg.astype(np.float32))
+        game.half_iteration(0)
+        R = game.reach()
+        for v in rng.choice(nodes, min(per_draw, len(nodes)), replace=False):
+            m = R[v].astype(np.float64).sum(axis=1)
+            if np.all(m > 1e-12) and len(ids) < n:
+                ids.append(int(v))
+                out.append((R[v] / m[:, None]).astype(np.float32))
+    game.reset()
+    game.set_regrets(saved)
+    return np.array(ids), np.stack(out)
+
+
+def leaf_dataset(spec, n, seed, iterations, game=None):
+    """n turn-leaf states of the game, valued over the 48 rivers by the batched solver
+    (pot-normalised counterfactual values). Each state is a leaf with chips behind (its 4-card
+    board, pot and stack). Its ranges are either the reach of random strategy profiles
+    (half the states, when `game` is given; see leaf_ranges) or random (U(0,1), 25 % zeroed,
+    board hands zeroed, normalised)."""
     nodes, _, _, _ = P.full_tree(spec)
-    leaves = nodes[(nodes["kind"] == 3) & (nodes["stack"] > 0)]
     rng = np.random.default_rng(seed)
-    pick = leaves[rng.integers(0, len(leaves), n)]
+    order = P.card_order()
+    n_game = n // 2 if game is not None else 0
+    if n_game:
+        ids, game_ranges = leaf_ranges(game, n_game, rng)
+        pick_game = nodes[ids]
+    leaves = nodes[(nodes["kind"] == 3) & (nodes["stack"] > 0)]
+    pick = leaves[rng.integers(0, len(leaves), n - n_game)]
+    if n_game:
+        pick = np.concatenate([pick_game, pick])
     boards = pick["board"].astype(np.uint64)
     pots = pick["stake"].astype(np.float32)
     stacks = pick["stack"].astype(np.float32)
-    order = P.card_order()
     ranges = np.zeros((n, 2, P.HANDS), np.float32)
-    for i in range(n):
+    if n_game:
+        ranges[:n_game] = game_ranges
+    for i in range(n_game, n):
         live = (order & boards[i]) == 0
         for p in range(2):
             r = rng.random(P.HANDS, dtype=np.float32)
@@ -104,7 +139,8 @@ def leaf_dataset(spec, n, seed, iterations):
                 solve_s=solve_s)
 
 
-def run(config, seed, iterations, check, target_pct, samples, river_iterations, epochs, resolve, net_iterations):
+def run(config, seed, iterations, check, target_pct, samples, river_iterations, epochs, resolve, net_iterations,
+        plain_only=False):
     import torch
     spec, ranges = seeded_game(config, seed)
     pot = CONFIGS[config]["pot"]
@@ -115,17 +151,35 @@ def run(config, seed, iterations, check, target_pct, samples, river_iterations, 
                    "allin_subgames": g.allin_subgames, "setup_s": time.perf_counter() - t0}
     pts, reached = trajectory(g, iterations, check, pot, target_pct)
     out["plain"] = {"trajectory": pts, "reached": reached}
+    # the same strategies measured the net-leaf way (rivers re-solved under the flop and
+    # turn strategies), to calibrate that measurement
+    _, _, ex = g.exploitability(resolve_iterations=resolve)
+    out["plain"]["resolved_pct_pot"] = 100.0 * ex / pot
+    if plain_only:
+        g.close()
+        return out
     # the network: data from this game's leaves, then training
+    g.reset()
     t0 = time.perf_counter()
-    data = leaf_dataset(spec, samples, seed + 1, river_iterations)
+    data = leaf_dataset(spec, samples, seed + 1, river_iterations, game=g)
     gen_s = time.perf_counter() - t0
     net = P.ValueNet(rows=256, seed=seed)
+    # every tenth state held out, from both halves (game reach and random ranges)
+    held = np.arange(samples) % 10 == 9
     t0 = time.perf_counter()
-    curve = T.train(net, data, np.arange(samples), epochs, 256, 1e-3, seed)
+    curve = T.train(net, data, np.flatnonzero(~held), epochs, 256, 1e-3, seed)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
+    te = np.flatnonzero(held)
+    pred = T.predict(net, data, te)
+    want = data["values"][te]
+    game_half = te < samples // 2
     out["network"] = {"samples": samples, "river_iterations": river_iterations, "generation_s": gen_s,
-                      "epochs": epochs, "train_s": train_s, "final_loss": curve[-1] if curve else None}
+                      "epochs": epochs, "train_s": train_s, "final_loss": curve[-1] if curve else None,
+                      "held_out_mse": {"network_game_ranges": T.mse(pred[game_half], want[game_half]),
+                                       "zero_game_ranges": T.mse(0 * want[game_half], want[game_half]),
+                                       "network_random_ranges": T.mse(pred[~game_half], want[~game_half]),
+                                       "zero_random_ranges": T.mse(0 * want[~game_half], want[~game_half])}}
     g.reset()
     g.set_net(net)
     pts, reached = trajectory(g, net_iterations, check, pot, target_pct, resolve=resolve)
@@ -144,13 +198,14 @@ def main(argv=None):
     ap.add_argument("--net-iterations", type=int, default=400)
     ap.add_argument("--check", type=int, default=50)
     ap.add_argument("--target", type=float, default=0.5, help="exploitability target, % of the starting pot")
-    ap.add_argument("--samples", type=int, default=2048)
+    ap.add_argument("--samples", type=int, default=4096)
     ap.add_argument("--river-iterations", type=int, default=200)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--resolve", type=int, default=200)
+    ap.add_argument("--plain-only", action="store_true", help="skip the network and the net-leaf solve")
     a = ap.parse_args(argv)
     print(json.dumps(run(a.config, a.seed, a.iterations, a.check, a.target, a.samples, a.river_iterations,
-                         a.epochs, a.resolve, a.net_iterations)), flush=True)
+                         a.epochs, a.resolve, a.net_iterations, a.plain_only)), flush=True)
     return 0
 
 
