@@ -208,6 +208,7 @@ def full_game_section(P):
     spec, ranges = FS.seeded_game("small", 7)
     pot = FS.CONFIGS["small"]["pot"]
     g = P.FullGame(spec, ranges)
+    g.tune()
     g.iterate(3)  # the first iteration runs eagerly, then one iteration is captured as a graph
     steps = 20
     t0 = time.perf_counter()
@@ -370,6 +371,27 @@ def run_batch_profile(args):
     print(json.dumps({"batch_profile": True, "subgames": args.batch_profile, "iteration_ms": dt * 1e3,
                       "achieved_gbs": nbytes / dt / 1e9, "bytes_per_iteration": nbytes}), flush=True)
     b.close()
+    return 0
+
+
+def run_full_profile(args):
+    """The full fixed-flop game alone (for profiling): the bench's full game, warm-up and
+    timed CFR iterations (one CUDA graph each), one JSON line."""
+    import torch
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    import pokerrust_b200 as P
+    from pokerrust_b200 import full_solve as FS
+    spec, ranges = FS.seeded_game("small", 7)
+    g = P.FullGame(spec, ranges)
+    g.tune()
+    g.iterate(max(2, args.warmup))
+    t0 = time.perf_counter()
+    g.iterate(args.steps)
+    dt = (time.perf_counter() - t0) / max(1, args.steps)
+    print(json.dumps({"full_profile": True, "nodes": g.nodes, "river_subgames": g.bet_subgames + g.allin_subgames,
+                      "iteration_ms": dt * 1e3}), flush=True)
+    g.close()
     return 0
 
 
@@ -569,6 +591,8 @@ def main():
                     help="only the batched general subgames: this many, a few timed iterations")
     ap.add_argument("--net-profile", action="store_true",
                     help="only the value network: warm-up and timed training steps at batch 4096")
+    ap.add_argument("--full-profile", action="store_true",
+                    help="only the full fixed-flop game with general bets: warm-up and timed CFR iterations")
     ap.add_argument("--subgames", type=int, default=0,
                     help="use the first N river roots only (profiling runs); 0 = all 27783")
     ap.add_argument("--profile", action="store_true",
@@ -580,6 +604,8 @@ def main():
         return run_batch_profile(args)
     if args.net_profile:
         return run_net_profile(args)
+    if args.full_profile:
+        return run_full_profile(args)
     return run_gpu(args)
 
 

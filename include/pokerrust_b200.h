@@ -321,6 +321,9 @@ int pr_full_shape(void *game, int *num_nodes, int *num_edges, int *num_leaves, i
                   int *allin_subgames);
 /* Net-leaf mode on (a pr_mlp_new network) or off (null). */
 int pr_full_set_net(void *game, void *net);
+/* The batched solver's autotuner on both river-subgame batches; ms_out[4] (or null): the
+ * chosen per-pass times of each batch's two shape classes. */
+int pr_full_tune(void *game, double *ms_out);
 /* Average sums weighted by the iteration number (1, the default) or uniformly (0). */
 int pr_full_set_linear_average(void *game, int on);
 /* One CFR half-iteration for `player`; pr_full_iterate: whole iterations (one CUDA graph each

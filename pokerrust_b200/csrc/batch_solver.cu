@@ -507,9 +507,24 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
             __syncthreads();
 
             // ---- leaves of the group: opponent weights -> p's values ----
-            for (int j = g0; j < g1; j++) {
-                const int buf = (j - g0) & 1;
-                V *x = S.X + (size_t)(j - g0) * kBRow;
+            // A fold by p followed by its sibling call (a showdown) sees the same opponent
+            // weights (p's actions leave them unchanged): one scan serves both leaves.
+            int phase = 0;  // scans done in this group; their parity picks the buffers
+            for (int j = g0; j < g1;) {
+                const int buf = phase & 1;
+                phase++;
+                const BNode ln = S.tn[S.leaf_node[j]];
+                bool pair = false;
+                BNode lsd = ln;  // the leaf whose kind and stake give the main value
+                if (ln.kind == kBFold && ln.actor == p && j + 1 < g1) {
+                    const BNode nx = S.tn[S.leaf_node[j + 1]];
+                    if (nx.kind == kBShowdown && nx.parent == ln.parent) {
+                        pair = true;
+                        lsd = nx;
+                    }
+                }
+                V *xf = S.X + (size_t)(j - g0) * kBRow;  // the fold's row when paired
+                V *x = pair ? xf + kBRow : xf;           // the scanned leaf's row
                 V *I = S.I + buf * kBRow;
                 V *CT = S.CT + buf * kBChunks;
                 V *SC = S.SC + buf * kBLists * 48;
@@ -563,9 +578,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                 V cofs = __shfl_up_sync(FULL, inc, 1);
                 if (lane == 0) cofs = V(0);
                 const V T = __shfl_sync(FULL, inc, kBChunks64 - 1);
-                const BNode ln = S.tn[S.leaf_node[j]];
-                const V stake = V(ln.stake);
-                V xv[K];
+                const V stake = V(lsd.stake);
+                V xv[K], fv[K];
                 ld_k<K>(x, pos0, xv);
 #pragma unroll
                 for (int k = 0; k < K; k++) {
@@ -578,12 +592,13 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                     // chunk offsets by shuffle (all lanes take part)
                     const V oe = __shfl_sync(FULL, cofs, ge >> 6);
                     const V os = __shfl_sync(FULL, cofs, gs > 0 ? (gs - 1) >> 6 : 0);
-                    V val = V(0);
+                    V val = V(0), fval = V(0);
                     if (pos < kBLive) {
                         const V *sc1 = SC + li1 * 48;
                         const V *sc2 = SC + li2 * 48;
                         const V T1 = sc1[kBListLen - 1], T2 = sc2[kBListLen - 1];
-                        if (ln.kind == kBShowdown) {
+                        const V free = ((T - T1) - T2) + xv[k];
+                        if (lsd.kind == kBShowdown) {
                             const V Pe = oe + I[ge];
                             const V Ps = gs > 0 ? os + I[gs - 1] : V(0);
                             const V vg = (Pe + Ps) - T;
@@ -591,13 +606,16 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                             const V v2 = (sc2[ge2] + (gs2 > 0 ? sc2[gs2 - 1] : V(0))) - T2;
                             val = mul(stake, (vg - v1) - v2);
                         } else {
-                            const V free = ((T - T1) - T2) + xv[k];
-                            val = mul(ln.actor == p ? -stake : stake, free);
+                            val = mul(lsd.actor == p ? -stake : stake, free);
                         }
+                        if (pair) fval = mul(-V(ln.stake), free);
                     }
                     xv[k] = val;
+                    fv[k] = fval;
                 }
                 st_k<K>(x, pos0, xv);
+                if (pair) st_k<K>(xf, pos0, fv);
+                j += pair ? 2 : 1;
             }
             __syncthreads();
 

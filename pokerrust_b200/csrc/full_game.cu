@@ -127,18 +127,43 @@ __global__ void __launch_bounds__(FT) down_kernel(FView v, const int *__restrict
                 c[kH + h] = nd.actor == 1 ? mul(b, p[k]) : b;
             }
         }
-    } else if (nd.kind == kFDeal) {
-        for (int k = 0; k < nd.nchild; k++) {
-            const int ci = v.kids[nd.kids + k];
-            const unsigned long long dealt = v.nodes[ci].board & ~nd.board;
-            T *c = R + (size_t)ci * 2 * kH;
-            for (int h = threadIdx.x; h < kH; h += FT) {
-                const bool blocked = (hand_bits(h) & dealt) != 0;
-                c[h] = blocked ? T(0) : r0[h];
-                c[kH + h] = blocked ? T(0) : r1[h];
-            }
-        }
     }
+}
+
+// deal nodes, top-down: one CTA per (deal node, card); the card's hands are masked
+template <typename T>
+__global__ void __launch_bounds__(FT) deal_down_kernel(FView v, const int *__restrict__ deals, T *__restrict__ R) {
+    const int n = deals[blockIdx.x];
+    const FNode nd = v.nodes[n];
+    const int k = blockIdx.y;
+    if (k >= nd.nchild) return;
+    const int ci = v.kids[nd.kids + k];
+    const unsigned long long dealt = v.nodes[ci].board & ~nd.board;
+    const T *r = R + (size_t)n * 2 * kH;
+    T *c = R + (size_t)ci * 2 * kH;
+    for (int h = threadIdx.x; h < kH; h += FT) {
+        const bool blocked = (hand_bits(h) & dealt) != 0;
+        c[h] = blocked ? T(0) : r[h];
+        c[kH + h] = blocked ? T(0) : r[kH + h];
+    }
+}
+
+// deal nodes, bottom-up: the mean over the cards of the children's values (hands holding the
+// card count 0); one CTA per (deal node, FT hands)
+template <typename T>
+__global__ void __launch_bounds__(FT) deal_up_kernel(FView v, const int *__restrict__ deals, T *__restrict__ V) {
+    const int n = deals[blockIdx.x];
+    const FNode nd = v.nodes[n];
+    const int h = blockIdx.y * FT + threadIdx.x;
+    if (h >= kH) return;
+    const unsigned long long hb = hand_bits(h);
+    T s = T(0);
+    for (int k = 0; k < nd.nchild; k++) {
+        const int ci = v.kids[nd.kids + k];
+        if (hb & (v.nodes[ci].board & ~nd.board)) continue;
+        s += V[(size_t)ci * kH + h];
+    }
+    V[(size_t)n * kH + h] = s / T(nd.nchild);
 }
 
 enum { kUpCFR = 0, kUpBR = 1, kUpEval = 2 };
@@ -181,19 +206,6 @@ __global__ void __launch_bounds__(FT) up_kernel(FView v, const int *__restrict__
                 hand_cards(h, &c1, &c2);
                 const T x = ((total - csum[c1]) - csum[c2]) + opp[h];
                 out[h] = mul(m, x);
-            }
-            return;
-        }
-        case kFDeal: {
-            for (int h = threadIdx.x; h < kH; h += FT) {
-                const unsigned long long hb = hand_bits(h);
-                T s = T(0);
-                for (int k = 0; k < nd.nchild; k++) {
-                    const int ci = v.kids[nd.kids + k];
-                    if (hb & (v.nodes[ci].board & ~nd.board)) continue;
-                    s += V[(size_t)ci * kH + h];
-                }
-                out[h] = s / T(nd.nchild);
             }
             return;
         }
@@ -316,8 +328,8 @@ __global__ void root_sum_kernel(const double *__restrict__ V, const float *__res
 struct Game {
     pr_full_spec spec{};
     FullTree tree;
-    std::vector<std::vector<int>> levels;
-    std::vector<int> level_off;
+    std::vector<std::vector<int>> levels, deals;  // per level: deal nodes / all other nodes
+    std::vector<int> level_off, deal_off;
     std::vector<float> init;  // [2][kH]
     double joint = 0;
     int N = 0, E = 0, L = 0;
@@ -362,12 +374,14 @@ struct Game {
     FView fview() const { return FView{d_nodes, d_kids}; }
     const int *level_ptr(int l) const { return d_levels + level_off[l]; }
     int level_size(int l) const { return (int)levels[l].size(); }
+    const int *deal_ptr(int l) const { return d_levels + deal_off[l]; }
+    int deal_size(int l) const { return (int)deals[l].size(); }
 
     template <typename T>
     int down(T *R, const float *src, int average) {
         for (int l = 0; l + 1 < (int)levels.size(); l++) {
-            if (!level_size(l)) continue;
-            down_kernel<T><<<level_size(l), FT, 0, stream>>>(fview(), level_ptr(l), R, src, average);
+            if (level_size(l)) down_kernel<T><<<level_size(l), FT, 0, stream>>>(fview(), level_ptr(l), R, src, average);
+            if (deal_size(l)) deal_down_kernel<T><<<dim3(deal_size(l), 52), FT, 0, stream>>>(fview(), deal_ptr(l), R);
         }
         cudaError_t e = cudaGetLastError();
         return e == cudaSuccess ? 0 : ffail("down sweep", e);
@@ -376,6 +390,8 @@ struct Game {
     template <typename T, int MODE>
     int up(int upd, const T *R, T *V, const T *leafV, const float *src, int average) {
         for (int l = (int)levels.size() - 1; l >= 0; l--) {
+            if (deal_size(l))
+                deal_up_kernel<T><<<dim3(deal_size(l), (kH + FT - 1) / FT), FT, 0, stream>>>(fview(), deal_ptr(l), V);
             if (!level_size(l)) continue;
             up_kernel<T, MODE><<<level_size(l), FT, 0, stream>>>(fview(), level_ptr(l), upd, R, V, leafV,
                                                                  MODE == kUpCFR ? d_reg : nullptr,
@@ -510,11 +526,14 @@ void *pr_full_new(const pr_full_spec *spec, const float *ranges) {
     g->E = t.num_edges;
     g->L = (int)t.leaves.size();
     g->levels.assign(t.levels, {});
-    for (int i = 0; i < g->N; i++) g->levels[t.nodes[i].level].push_back(i);
+    g->deals.assign(t.levels, {});
+    for (int i = 0; i < g->N; i++) (t.nodes[i].kind == kFDeal ? g->deals : g->levels)[t.nodes[i].level].push_back(i);
     std::vector<int> flat;
-    for (auto &l : g->levels) {
+    for (int l = 0; l < t.levels; l++) {
         g->level_off.push_back((int)flat.size());
-        flat.insert(flat.end(), l.begin(), l.end());
+        flat.insert(flat.end(), g->levels[l].begin(), g->levels[l].end());
+        g->deal_off.push_back((int)flat.size());
+        flat.insert(flat.end(), g->deals[l].begin(), g->deals[l].end());
     }
     // initial ranges, hands on the flop removed; joint mass of clash-free pairs
     g->init.assign(2 * kH, 0.0f);
@@ -677,6 +696,31 @@ int pr_full_set_net(void *game, void *net) {
             (e = cudaMalloc(&g->d_nboard, sizeof(unsigned long long) * n)) != cudaSuccess)
             return ffail("net buffers", e);
     }
+    return 0;
+}
+
+// Runs the batched solver's autotuner on both river-subgame batches (launch configuration
+// per tree-shape class; their solver state is restored). ms_out[4]: the chosen per-pass
+// times of batch 0's and batch 1's two classes, or null.
+int pr_full_tune(void *game, double *ms_out) {
+    Game *g = (Game *)game;
+    if (!g) return 2;
+    cudaError_t e = cudaStreamSynchronize(g->stream);
+    if (e != cudaSuccess) return ffail("tune", e);
+    for (int b = 0; b < 2; b++) {
+        double ms[2] = {0.0, 0.0};
+        if (g->batch[b])
+            if (int st = pr_batch_tune(g->batch[b], ms)) return st;
+        if (ms_out) {
+            ms_out[2 * b] = ms[0];
+            ms_out[2 * b + 1] = ms[1];
+        }
+    }
+    if (g->graph) {
+        cudaGraphExecDestroy(g->graph);
+        g->graph = nullptr;
+    }
+    g->graph_failed = false;
     return 0;
 }
 

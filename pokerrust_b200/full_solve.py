@@ -147,8 +147,11 @@ def run(config, seed, iterations, check, target_pct, samples, river_iterations, 
     out = {"config": config, "seed": seed, "target_pct_pot": target_pct}
     t0 = time.perf_counter()
     g = P.FullGame(spec, ranges)
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    g.tune()
     out["game"] = {"nodes": g.nodes, "edges": g.edges, "leaves": g.leaves, "river_subgames": g.bet_subgames,
-                   "allin_subgames": g.allin_subgames, "setup_s": time.perf_counter() - t0}
+                   "allin_subgames": g.allin_subgames, "setup_s": setup_s, "tune_s": time.perf_counter() - t0}
     pts, reached = trajectory(g, iterations, check, pot, target_pct)
     out["plain"] = {"trajectory": pts, "reached": reached}
     # the same strategies measured the net-leaf way (rivers re-solved under the flop and

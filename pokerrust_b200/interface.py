@@ -226,6 +226,8 @@ def lib():
         L.pr_full_exploitability.argtypes = [vp, i32, vp, vp, vp]
         L.pr_full_read.restype = i32
         L.pr_full_read.argtypes = [vp, i32, vp]
+        L.pr_full_tune.restype = i32
+        L.pr_full_tune.argtypes = [vp, vp]
         L.pr_full_set_linear_average.restype = i32
         L.pr_full_set_linear_average.argtypes = [vp, i32]
         L.pr_full_reset.restype = i32
@@ -835,6 +837,12 @@ class FullGame:
         """Net-leaf mode with a ValueNet, or plain river subgames (None)."""
         self._net = net
         _check(lib().pr_full_set_net(self.ptr, net.ptr if net is not None else None), "pr_full_set_net")
+
+    def tune(self):
+        """Autotunes the river-subgame batches; per-pass ms of each batch's two classes."""
+        ms = np.zeros(4)
+        _check(lib().pr_full_tune(self.ptr, _ptr(ms)), "pr_full_tune")
+        return ms
 
     def set_linear_average(self, on):
         """Average sums weighted by the iteration number (True, the default) or by 1."""
