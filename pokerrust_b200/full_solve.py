@@ -98,6 +98,49 @@ def leaf_ranges(game, n, rng, per_draw=64):
     return np.array(ids), np.stack(out)
 
 
+def river_values(boards, ranges, pots, stacks, iterations, chunk=1024):
+    """Leaf values [n][2][1326] (pot-normalised, mean over the 48 rivers) of the states, by
+    the batched solver in batches of `chunk` states (48 subgames each), the launch
+    configuration tuned on the first batch and reused; and the seconds spent."""
+    n = len(boards)
+    order = P.card_order()
+    values = np.zeros((n, 2, P.HANDS), np.float32)
+    cfg = None
+    t0 = time.perf_counter()
+    for s0 in range(0, n, chunk):
+        s1 = min(n, s0 + chunk)
+        m = s1 - s0
+        specs = np.zeros(m * 48, P.SPEC_DTYPE)
+        rr = np.zeros((m * 48, 2, P.HANDS), np.float32)
+        k = 0
+        for i in range(s0, s1):
+            for c in range(52):
+                if (int(boards[i]) >> c) & 1:
+                    continue
+                specs[k] = (int(boards[i]) | (1 << c), pots[i], stacks[i], D.RIVER_SIZES, D.RIVER_RAISES)
+                rr[k] = ranges[i]
+                rr[k][:, (order & np.uint64(1 << c)) != 0] = 0.0
+                k += 1
+        b = P.Batch(specs, rr)
+        b.enable_average()
+        b.iterate(1)
+        if cfg is None:
+            b.tune()
+            cfg = [b.config(c) for c in range(2)]
+        else:
+            for c in range(2):
+                if cfg[c]["count"]:
+                    b.set_config(c, cfg[c]["K"], cfg[c]["per_sm"], cfg[c]["order"])
+        b.iterate(iterations - 1)
+        # each player's counterfactual values at the root: the adjoint's dV/dr0 and -dV/dr1
+        c0, _ = b.root_values(0, use_average=True)
+        c1, _ = b.root_values(1, use_average=True)
+        b.close()
+        v = np.stack([c0, c1], axis=1).reshape(m, 48, 2, P.HANDS).mean(axis=1)
+        values[s0:s1] = v / pots[s0:s1, None, None]
+    return values, time.perf_counter() - t0
+
+
 def leaf_dataset(spec, n, seed, iterations, game=None):
     """n turn-leaf states of the game, valued over the 48 rivers by the batched solver
     (pot-normalised counterfactual values). Each state is a leaf with chips behind (its 4-card
@@ -128,12 +171,7 @@ def leaf_dataset(spec, n, seed, iterations, game=None):
             r[rng.random(P.HANDS) < 0.25] = 0.0
             r[~live] = 0.0
             ranges[i, p] = r / r.sum()
-    values = np.zeros((n, 2, P.HANDS), np.float32)
-    solve_s = 0.0
-    for s in range(0, n, 256):
-        e = min(n, s + 256)
-        values[s:e], dt = D.river_values(boards[s:e], ranges[s:e], pots[s:e], stacks[s:e], iterations)
-        solve_s += dt
+    values, solve_s = river_values(boards, ranges, pots, stacks, iterations)
     scalars = np.stack([pots / 200.0, stacks / (10.0 * pots)], axis=1).astype(np.float32)
     return dict(boards=boards, ranges=ranges, scalars=scalars, values=values, pots=pots, stacks=stacks,
                 solve_s=solve_s)
@@ -201,8 +239,8 @@ def main(argv=None):
     ap.add_argument("--net-iterations", type=int, default=400)
     ap.add_argument("--check", type=int, default=50)
     ap.add_argument("--target", type=float, default=0.5, help="exploitability target, % of the starting pot")
-    ap.add_argument("--samples", type=int, default=4096)
-    ap.add_argument("--river-iterations", type=int, default=200)
+    ap.add_argument("--samples", type=int, default=32768)
+    ap.add_argument("--river-iterations", type=int, default=100)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--resolve", type=int, default=200)
     ap.add_argument("--plain-only", action="store_true", help="skip the network and the net-leaf solve")
