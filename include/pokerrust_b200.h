@@ -261,6 +261,10 @@ double pr_batch_iteration_bytes(void *batch);
  * D[M][N] (f32) = A[M][K] . B[N][K]^T for bf16 A, B on the tcgen05 tensor cores (device
  * pointers; M % 128 == 0, N % bn == 0, K % 64 == 0, bn 128 or 256). Synchronous. */
 int pr_gemm_bf16(const void *A, const void *B, float *D, int M, int N, int K, int bn, void *stream);
+/* The same product with either operand stored MN-major: a_mn = 1 reads A from a [K][M]
+ * array, b_mn = 1 reads B from a [K][N] array (the tensor cores take either layout). */
+int pr_gemm_bf16_major(const void *A, const void *B, float *D, int M, int N, int K, int bn, int a_mn, int b_mn,
+                       void *stream);
 /* Asynchronous form; err is a device int that collects error bits of timed-out waits. */
 int pr_gemm_bf16_async(const void *A, const void *B, float *D, int M, int N, int K, int bn, int *err,
                        void *stream);

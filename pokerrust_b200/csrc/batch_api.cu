@@ -359,15 +359,14 @@ void *pr_batch_new(const pr_subgame *specs, int count, const float *ranges) {
         delete b;
         return nullptr;
     }
+    // the hand of every position, one strided copy out of the packs
     b->hand.resize((size_t)count * kBRow);
-    for (int s = 0; s < count; s++) {
-        e = cudaMemcpy(b->hand.data() + (size_t)s * kBRow, (const char *)(b->d_packs + s) + offsetof(BPack, hand),
-                       sizeof(uint16_t) * kBRow, cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) {
-            bfail("pack download", e);
-            delete b;
-            return nullptr;
-        }
+    e = cudaMemcpy2D(b->hand.data(), sizeof(uint16_t) * kBRow, (const char *)b->d_packs + offsetof(BPack, hand),
+                     sizeof(BPack), sizeof(uint16_t) * kBRow, count, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        bfail("pack download", e);
+        delete b;
+        return nullptr;
     }
     if (b->upload_order()) {
         delete b;

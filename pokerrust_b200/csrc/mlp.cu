@@ -1,7 +1,9 @@
 // Turn-leaf value network: a 5-layer MLP (2706 -> 4 x 1024 GELU -> 2652) trained and run on
 // the device with the tcgen05 GEMM of mlp_gemm.cuh (BF16 operands, FP32 accumulation),
-// fused epilogues (bias + GELU, bias, GELU derivative), BF16 transposes, an MSE loss
-// kernel, bias-gradient reductions and Adam on FP32 master weights.
+// fused epilogues (bias + GELU, bias, GELU derivative), an MSE loss kernel, bias-gradient
+// reductions and Adam on FP32 master weights. The backward GEMMs read transposed operands
+// (activations for the weight gradients, weights for the input gradients) MN-major, straight
+// from their row-major arrays.
 //
 // Input per sample: both players' ranges over the 1326 hands, the 4 turn-board cards as a
 // 52-wide 0/1 vector, pot and stack scaled to [0, 1] (pot / 200, stack / (10 pot)).
@@ -187,20 +189,6 @@ struct EpiStore {  // D = acc (f32); split-K part z goes to D + z * zstride
 };
 
 // ---- element-wise kernels ----
-__global__ void transpose_kernel(const bf16 *__restrict__ in, bf16 *__restrict__ out, int rows, int cols) {
-    __shared__ bf16 tile[32][33];
-    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
-        const int r = r0 + i, c = c0 + threadIdx.x;
-        tile[i][threadIdx.x] = (r < rows && c < cols) ? in[(size_t)r * cols + c] : bf16(0.0f);
-    }
-    __syncthreads();
-    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
-        const int c = c0 + i, r = r0 + threadIdx.x;
-        if (c < cols && r < rows) out[(size_t)c * rows + r] = tile[threadIdx.x][i];
-    }
-}
-
 // inputs: ranges [n][2][1326], boards (4 cards) [n], scalars [n][2] -> X [rows][kInPad] bf16
 __global__ void assemble_kernel(const float *__restrict__ ranges, const unsigned long long *__restrict__ boards,
                                 const float *__restrict__ scalars, bf16 *__restrict__ X, int n) {
@@ -243,15 +231,43 @@ __global__ void loss_kernel(const float *__restrict__ Y, const float *__restrict
     (void)rows;
 }
 
-// db[j] = sum over rows of G^T[j][:]  (G^T: [cols][rows] bf16, one warp per column)
-__global__ void bias_grad_kernel(const bf16 *__restrict__ GT, float *__restrict__ db, int cols, int rows) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x % 32;
-    if (warp >= cols) return;
-    float acc = 0.0f;
-    for (int m = lane; m < rows; m += 32) acc += float(GT[(size_t)warp * rows + m]);
+// Bias gradients db[c] = sum over rows of G[r][c] (G: [rows][cols] bf16), in two fixed-order
+// steps: kBiasChunks row chunks per column (a CTA of 64 columns, two per thread, x 8 row
+// phases per chunk), then the chunks in order.
+constexpr int kBiasChunks = 16;
+
+__global__ void bias_part_kernel(const bf16 *__restrict__ G, float *__restrict__ part, int cols, int rows) {
+    __shared__ float red[8][2][33];
+    const int c = blockIdx.x * 64 + 2 * threadIdx.x;
+    const int per = rows / kBiasChunks;
+    const int r0 = blockIdx.y * per;
+    float a0 = 0.0f, a1 = 0.0f;
+    for (int r = r0 + threadIdx.y; r < r0 + per; r += 8) {
+        const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162 *>(G + (size_t)r * cols + c);
+        a0 += __low2float(v);
+        a1 += __high2float(v);
+    }
+    red[threadIdx.y][0][threadIdx.x] = a0;
+    red[threadIdx.y][1][threadIdx.x] = a1;
+    __syncthreads();
+    if (threadIdx.y == 0) {
+        float t0 = 0.0f, t1 = 0.0f;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-    if (lane == 0) db[warp] = acc;
+        for (int i = 0; i < 8; i++) {
+            t0 += red[i][0][threadIdx.x];
+            t1 += red[i][1][threadIdx.x];
+        }
+        part[(size_t)blockIdx.y * cols + c] = t0;
+        part[(size_t)blockIdx.y * cols + c + 1] = t1;
+    }
+}
+
+__global__ void bias_sum_kernel(const float *__restrict__ part, float *__restrict__ db, int cols) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float t = 0.0f;
+    for (int k = 0; k < kBiasChunks; k++) t += part[(size_t)k * cols + c];
+    db[c] = t;
 }
 
 // Adam on f32 master weights; padding (rows >= n_live or columns >= k_live) stays zero.
@@ -307,17 +323,18 @@ struct Net {
     int rows = 0;  // batch rows (multiple of 256)
     cudaStream_t stream = nullptr;
     int *d_err = nullptr;
-    // parameters (f32 master, bf16 copy, bf16 transpose), gradients, Adam moments
+    // parameters (f32 master, bf16 copy), gradients, Adam moments
     float *W[kLayers] = {}, *b[kLayers] = {}, *dW[kLayers] = {}, *db[kLayers] = {};
     float *mW[kLayers] = {}, *vW[kLayers] = {}, *mb[kLayers] = {}, *vb[kLayers] = {};
-    bf16 *Wb[kLayers] = {}, *WT[kLayers] = {};
+    bf16 *Wb[kLayers] = {};
     // activations
-    bf16 *X = nullptr, *XT = nullptr;
-    bf16 *Z[4] = {}, *H[4] = {}, *HT[4] = {}, *dZ[4] = {}, *dZT[4] = {};
+    bf16 *X = nullptr;
+    bf16 *Z[4] = {}, *H[4] = {}, *dZ[4] = {};
     float *Y = nullptr;
-    bf16 *dY = nullptr, *dYT = nullptr;
+    bf16 *dY = nullptr;
     double *partial = nullptr;
     float *parts = nullptr;  // split-K partial products of the weight gradients
+    float *bias_parts = nullptr;  // [kBiasChunks][cols] partial bias gradients
     int step = 0;
     static constexpr int kSplits = 4;
     static constexpr size_t kPartsMax = (size_t)kOutPad * kInPad;  // largest weight matrix
@@ -357,44 +374,40 @@ struct Net {
         return check(e, "forward");
     }
 
-    void transpose(const bf16 *in, bf16 *out, int r, int c) {
-        dim3 grid((c + 31) / 32, (r + 31) / 32), block(32, 8);
-        transpose_kernel<<<grid, block, 0, stream>>>(in, out, r, c);
-    }
-
-    // dW[M][N] = G^T-rows . In^T-rows^T over the batch, as kSplits split-K GEMMs summed in
-    // part order (the weight-gradient GEMMs have few output tiles)
-    cudaError_t weight_grad(const bf16 *GT, const bf16 *InT, int M, int N, float *dWout) {
+    // dW[M][N] = G^T . In over the batch (G: [rows][M], In: [rows][N], both read MN-major), as
+    // kSplits split-K GEMMs summed in part order (the weight-gradient GEMMs have few output
+    // tiles)
+    cudaError_t weight_grad(const bf16 *G, const bf16 *In, int M, int N, float *dWout) {
         const size_t n = (size_t)M * N;
         EpiStore epi{parts, N, n};
-        cudaError_t e = gemm::run<256>(GT, InT, M, N, rows, epi, d_err, stream, kSplits);
+        cudaError_t e =
+            gemm::run<256, gemm::kMNMajor, gemm::kMNMajor>(G, In, M, N, rows, epi, d_err, stream, kSplits);
         if (e != cudaSuccess) return e;
         split_sum_kernel<<<592, 256, 0, stream>>>(parts, dWout, n, kSplits);
         return cudaGetLastError();
     }
 
-    // backward from dY (bf16), gradients into dW / db
+    void bias_grad(const bf16 *G, float *dbout, int cols) {
+        bias_part_kernel<<<dim3(cols / 64, kBiasChunks), dim3(32, 8), 0, stream>>>(G, bias_parts, cols, rows);
+        bias_sum_kernel<<<(cols + 255) / 256, 256, 0, stream>>>(bias_parts, dbout, cols);
+    }
+
+    // backward from dY (bf16), gradients into dW / db; the input gradients dZ . W read the
+    // weights [out][in] MN-major
     int backward() {
-        cudaError_t e = cudaSuccess;
-        transpose(dY, dYT, rows, kOutPad);
-        // output layer
-        transpose(H[3], HT[3], rows, kHid);
-        e = weight_grad(dYT, HT[3], kOutPad, kHid, dW[4]);
-        bias_grad_kernel<<<(kOutPad * 32 + 255) / 256, 256, 0, stream>>>(dYT, db[4], kOutPad, rows);
+        cudaError_t e = weight_grad(dY, H[3], kOutPad, kHid, dW[4]);
+        bias_grad(dY, db[4], kOutPad);
         if (e == cudaSuccess) {
             EpiGeluGrad epi{Z[3], dZ[3], kHid};
-            e = gemm::run<256>(dY, WT[4], rows, kHid, kOutPad, epi, d_err, stream);
+            e = gemm::run<256, gemm::kKMajor, gemm::kMNMajor>(dY, Wb[4], rows, kHid, kOutPad, epi, d_err, stream);
         }
         for (int l = 3; l >= 0 && e == cudaSuccess; l--) {
-            transpose(dZ[l], dZT[l], rows, kHid);
-            const bf16 *inT = l > 0 ? HT[l - 1] : XT;
-            if (l > 0) transpose(H[l - 1], HT[l - 1], rows, kHid);
-            else transpose(X, XT, rows, kInPad);
-            e = weight_grad(dZT[l], inT, kHid, kK[l], dW[l]);
-            bias_grad_kernel<<<(kHid * 32 + 255) / 256, 256, 0, stream>>>(dZT[l], db[l], kHid, rows);
+            e = weight_grad(dZ[l], l > 0 ? H[l - 1] : X, kHid, kK[l], dW[l]);
+            bias_grad(dZ[l], db[l], kHid);
             if (e == cudaSuccess && l > 0) {
                 EpiGeluGrad epi2{Z[l - 1], dZ[l - 1], kHid};
-                e = gemm::run<256>(dZ[l], WT[l], rows, kHid, kHid, epi2, d_err, stream);
+                e = gemm::run<256, gemm::kKMajor, gemm::kMNMajor>(dZ[l], Wb[l], rows, kHid, kHid, epi2, d_err,
+                                                                 stream);
             }
         }
         if (e == cudaSuccess) e = cudaGetLastError();
@@ -410,16 +423,12 @@ struct Net {
                                                  kKLive[l], lr, b1, b2, c1, c2, eps);
             adam_kernel<<<8, 256, 0, stream>>>(b[l], mb[l], vb[l], db[l], nullptr, 1, kN[l], 1, kNLive[l], lr, b1,
                                                b2, c1, c2, eps);
-            transpose(Wb[l], WT[l], kN[l], kK[l]);
         }
         return check(cudaGetLastError(), "adam");
     }
 
     int refresh_copies() {
-        for (int l = 0; l < kLayers; l++) {
-            to_bf16_kernel<<<592, 256, 0, stream>>>(W[l], Wb[l], (size_t)kN[l] * kK[l]);
-            transpose(Wb[l], WT[l], kN[l], kK[l]);
-        }
+        for (int l = 0; l < kLayers; l++) to_bf16_kernel<<<592, 256, 0, stream>>>(W[l], Wb[l], (size_t)kN[l] * kK[l]);
         return check(cudaGetLastError(), "weights");
     }
 };
@@ -449,17 +458,15 @@ void *pr_mlp_new(int rows, uint64_t seed) {
     for (int l = 0; l < kLayers && ok; l++) {
         const size_t sz = (size_t)kN[l] * kK[l];
         ok = n->alloc(&n->W[l], sz) && n->alloc(&n->dW[l], sz) && n->alloc(&n->mW[l], sz) && n->alloc(&n->vW[l], sz) &&
-             n->alloc(&n->Wb[l], sz) && n->alloc(&n->WT[l], sz) && n->alloc(&n->b[l], kN[l]) &&
+             n->alloc(&n->Wb[l], sz) && n->alloc(&n->b[l], kN[l]) &&
              n->alloc(&n->db[l], kN[l]) && n->alloc(&n->mb[l], kN[l]) && n->alloc(&n->vb[l], kN[l]);
     }
-    ok = ok && n->alloc(&n->X, (size_t)rows * kInPad) && n->alloc(&n->XT, (size_t)rows * kInPad) &&
-         n->alloc(&n->Y, (size_t)rows * kOutPad) && n->alloc(&n->dY, (size_t)rows * kOutPad) &&
-         n->alloc(&n->dYT, (size_t)rows * kOutPad) && n->alloc(&n->partial, rows) &&
-         n->alloc(&n->parts, Net::kSplits * Net::kPartsMax);
+    ok = ok && n->alloc(&n->X, (size_t)rows * kInPad) && n->alloc(&n->Y, (size_t)rows * kOutPad) &&
+         n->alloc(&n->dY, (size_t)rows * kOutPad) && n->alloc(&n->partial, rows) &&
+         n->alloc(&n->parts, Net::kSplits * Net::kPartsMax) && n->alloc(&n->bias_parts, (size_t)kBiasChunks * kOutPad);
     for (int l = 0; l < 4 && ok; l++)
         ok = n->alloc(&n->Z[l], (size_t)rows * kHid) && n->alloc(&n->H[l], (size_t)rows * kHid) &&
-             n->alloc(&n->HT[l], (size_t)rows * kHid) && n->alloc(&n->dZ[l], (size_t)rows * kHid) &&
-             n->alloc(&n->dZT[l], (size_t)rows * kHid);
+             n->alloc(&n->dZ[l], (size_t)rows * kHid);
     if (!ok) {
         fprintf(stderr, "pokerrust_b200: value network: allocation failed\n");
         delete n;

@@ -24,13 +24,26 @@ struct EpiF32 {
 
 }  // namespace gemm
 
+namespace {
+template <int BN>
+cudaError_t run_majors(const gemm::bf16 *a, const gemm::bf16 *b, int M, int N, int K, gemm::EpiF32 epi, bool a_mn,
+                       bool b_mn, int *err, cudaStream_t stream) {
+    using gemm::kKMajor;
+    using gemm::kMNMajor;
+    if (!a_mn && !b_mn) return gemm::run<BN, kKMajor, kKMajor>(a, b, M, N, K, epi, err, stream);
+    if (!a_mn && b_mn) return gemm::run<BN, kKMajor, kMNMajor>(a, b, M, N, K, epi, err, stream);
+    if (a_mn && !b_mn) return gemm::run<BN, kMNMajor, kKMajor>(a, b, M, N, K, epi, err, stream);
+    return gemm::run<BN, kMNMajor, kMNMajor>(a, b, M, N, K, epi, err, stream);
+}
+}  // namespace
+
 cudaError_t gemm_bf16_f32(const void *A, const void *B, float *D, int M, int N, int K, int ldd, int rows_live,
-                          int cols_live, int bn, int *err, cudaStream_t stream) {
+                          int cols_live, int bn, int *err, cudaStream_t stream, bool a_mn, bool b_mn) {
     gemm::EpiF32 epi{D, ldd, rows_live, cols_live};
     const gemm::bf16 *a = reinterpret_cast<const gemm::bf16 *>(A);
     const gemm::bf16 *b = reinterpret_cast<const gemm::bf16 *>(B);
-    if (bn == 256) return gemm::run<256>(a, b, M, N, K, epi, err, stream);
-    if (bn == 128) return gemm::run<128>(a, b, M, N, K, epi, err, stream);
+    if (bn == 256) return run_majors<256>(a, b, M, N, K, epi, a_mn, b_mn, err, stream);
+    if (bn == 128) return run_majors<128>(a, b, M, N, K, epi, a_mn, b_mn, err, stream);
     return cudaErrorInvalidValue;
 }
 
@@ -38,15 +51,15 @@ cudaError_t gemm_bf16_f32(const void *A, const void *B, float *D, int M, int N, 
 
 extern "C" {
 
-// D[M][N] (f32) = A[M][K] . B[N][K]^T on the tensor cores, device pointers, synchronous.
-// Returns 0, 2 for bad shapes, or 1 with the kernel's error bits printed on a timed-out wait.
-int pr_gemm_bf16(const void *A, const void *B, float *D, int M, int N, int K, int bn, void *stream) {
+namespace {
+int gemm_sync(const void *A, const void *B, float *D, int M, int N, int K, int bn, void *stream, bool a_mn,
+              bool b_mn) {
     int *d_err = nullptr;
     cudaError_t e = cudaMalloc(&d_err, sizeof(int));
     if (e != cudaSuccess) return 1;
     cudaStream_t s = (cudaStream_t)stream;
     cudaMemsetAsync(d_err, 0, sizeof(int), s);
-    e = prb::gemm_bf16_f32(A, B, D, M, N, K, N, M, N, bn, d_err, s);
+    e = prb::gemm_bf16_f32(A, B, D, M, N, K, N, M, N, bn, d_err, s, a_mn, b_mn);
     if (e == cudaErrorInvalidValue) {
         cudaFree(d_err);
         return 2;
@@ -66,11 +79,27 @@ int pr_gemm_bf16(const void *A, const void *B, float *D, int M, int N, int K, in
     return 0;
 }
 
-// The same product launched asynchronously on `stream`; err: a device int that collects the
-// kernel's error bits (timed-out waits). 0 or 2 (bad shapes) or 1 (launch error).
+}  // namespace
+
+// D[M][N] (f32) = A[M][K] . B[N][K]^T on the tensor cores, device pointers, synchronous.
+// Returns 0, 2 for bad shapes, or 1 with the kernel's error bits printed on a timed-out wait.
+int pr_gemm_bf16(const void *A, const void *B, float *D, int M, int N, int K, int bn, void *stream) {
+    return gemm_sync(A, B, D, M, N, K, bn, stream, false, false);
+}
+
+// The same product with either operand MN-major: a_mn = 1 reads A from [K][M] storage
+// (D = A^T-stored . B^T), b_mn = 1 reads B from [K][N] storage.
+int pr_gemm_bf16_major(const void *A, const void *B, float *D, int M, int N, int K, int bn, int a_mn, int b_mn,
+                       void *stream) {
+    return gemm_sync(A, B, D, M, N, K, bn, stream, a_mn != 0, b_mn != 0);
+}
+
+// The K-major product launched asynchronously on `stream`; err: a device int that collects
+// the kernel's error bits (timed-out waits). 0 or 2 (bad shapes) or 1 (launch error).
 int pr_gemm_bf16_async(const void *A, const void *B, float *D, int M, int N, int K, int bn, int *err,
                        void *stream) {
-    const cudaError_t e = prb::gemm_bf16_f32(A, B, D, M, N, K, N, M, N, bn, err, (cudaStream_t)stream);
+    const cudaError_t e =
+        prb::gemm_bf16_f32(A, B, D, M, N, K, N, M, N, bn, err, (cudaStream_t)stream, false, false);
     return e == cudaSuccess ? 0 : (e == cudaErrorInvalidValue ? 2 : 1);
 }
 

@@ -1,6 +1,8 @@
 // BF16 GEMM on the 5th-generation tensor cores (tcgen05) for the turn-leaf value network:
-// D[M][N] = A[M][K] . B[N][K]^T with FP32 accumulation in tensor memory, A and B K-major
-// (row-major with K contiguous), fused element-wise epilogues.
+// D[M][N] = A[M][K] . B[N][K]^T with FP32 accumulation in tensor memory and fused
+// element-wise epilogues. Each operand is K-major (stored [M][K] / [N][K], K contiguous) or
+// MN-major (stored [K][M] / [K][N], M or N contiguous): the tensor cores read either
+// shared-memory layout, so transposed operands need no transpose in memory.
 //
 // One CTA computes one 128 x BN tile. Warp 0 (one thread) streams 128 x 64 / BN x 64 tiles
 // of A and B into shared memory with TMA (128-byte swizzle, STAGES-deep ring, no
@@ -12,11 +14,13 @@
 // returns.
 //
 // The layouts, descriptors and TMA boxes come from CuTe's sm100 atoms
-// (SM100_MMA_F16BF16_SS, UMMA::Layout_K_SW128_Atom, make_tma_atom_A/B_sm100 with the
-// non-multicast SM90_TMA_LOAD, SM100_TMEM_LOAD_32dp32b*).
+// (SM100_MMA_F16BF16_SS, UMMA::Layout_K_SW128_Atom / Layout_MN_SW128_Atom,
+// make_tma_atom_A/B_sm100 with the non-multicast SM90_TMA_LOAD, SM100_TMEM_LOAD_32dp32b*).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 #include <cutlass/cutlass.h>
 #include <cute/tensor.hpp>
@@ -38,17 +42,29 @@ constexpr int kStages = 4;
 constexpr int kThreads = 128;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // give up on an mbarrier after 2 s
 
-template <int BN>
+constexpr UMMA::Major kKMajor = UMMA::Major::K;
+constexpr UMMA::Major kMNMajor = UMMA::Major::MN;
+
+// 128-byte-swizzled shared-memory atom of an operand with the given major mode, and the order
+// its copies tile a (rows, K, stage) buffer: K-major atoms along the rows first; MN-major
+// atoms (64 rows x 8 K) along K first, so that each 64-row block holds all 64 K values of a
+// stage contiguously and one TMA box of 64 x 64 fills it
+template <UMMA::Major MJ>
+using SwAtom = std::conditional_t<MJ == UMMA::Major::K, UMMA::Layout_K_SW128_Atom<bf16>,
+                                  UMMA::Layout_MN_SW128_Atom<bf16>>;
+template <UMMA::Major MJ>
+using TileOrder = std::conditional_t<MJ == UMMA::Major::K, GenColMajor, Step<_2, _1, _3>>;
+
+template <int BN, UMMA::Major MA = kKMajor, UMMA::Major MB = kKMajor>
 struct Cfg {
-    using TiledMma = decltype(make_tiled_mma(SM100_MMA_F16BF16_SS<bf16, bf16, float, kBM, BN, UMMA::Major::K,
-                                                                  UMMA::Major::K>{}));
+    using TiledMma = decltype(make_tiled_mma(SM100_MMA_F16BF16_SS<bf16, bf16, float, kBM, BN, MA, MB>{}));
     using Tiler = Shape<Int<kBM>, Int<BN>, Int<kBK>>;
     using ShapeA = decltype(partition_shape_A(TiledMma{}, make_shape(Int<kBM>{}, Int<kBK>{})));
     using ShapeB = decltype(partition_shape_B(TiledMma{}, make_shape(Int<BN>{}, Int<kBK>{})));
-    using SmemA = decltype(UMMA::tile_to_mma_shape(UMMA::Layout_K_SW128_Atom<bf16>{},
-                                                   append(ShapeA{}, Int<kStages>{})));
-    using SmemB = decltype(UMMA::tile_to_mma_shape(UMMA::Layout_K_SW128_Atom<bf16>{},
-                                                   append(ShapeB{}, Int<kStages>{})));
+    using SmemA =
+        decltype(UMMA::tile_to_mma_shape(SwAtom<MA>{}, append(ShapeA{}, Int<kStages>{}), TileOrder<MA>{}));
+    using SmemB =
+        decltype(UMMA::tile_to_mma_shape(SwAtom<MB>{}, append(ShapeB{}, Int<kStages>{}), TileOrder<MB>{}));
     static constexpr int kBytesA = kBM * kBK * 2;
     static constexpr int kBytesB = BN * kBK * 2;
 
@@ -101,11 +117,11 @@ __device__ __forceinline__ void tmem_fence_before_sync() {
 // Error bits written to `err` (device int) on a timed-out wait.
 enum : int { kErrProducer = 1, kErrMma = 2, kErrEpilogue = 4 };
 
-template <int BN, class TmaA, class TmaB, class Epi>
+template <int BN, UMMA::Major MA, UMMA::Major MB, class TmaA, class TmaB, class Epi>
 __global__ void __launch_bounds__(kThreads, 1)
     gemm_kernel(CUTE_GRID_CONSTANT TmaA const tma_a, CUTE_GRID_CONSTANT TmaB const tma_b, int M, int N, int K,
                 Epi epi, int *err) {
-    using C = Cfg<BN>;
+    using C = Cfg<BN, MA, MB>;
     extern __shared__ char smem_raw[];
     typename C::Shared &ss = *reinterpret_cast<typename C::Shared *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -237,22 +253,32 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-// Launches D = A . B^T with epilogue `epi` on `stream` (host side; see gemm_kernel).
-template <int BN, class Epi>
+// The (rows x K) view of an operand: K-major [rows][K] or MN-major [K][rows] in memory.
+template <UMMA::Major MJ>
+inline auto operand_view(const bf16 *p, int rows, int K) {
+    if constexpr (MJ == UMMA::Major::K)
+        return make_tensor(make_gmem_ptr(p), make_shape(rows, K), make_stride(K, Int<1>{}));
+    else
+        return make_tensor(make_gmem_ptr(p), make_shape(rows, K), make_stride(Int<1>{}, rows));
+}
+
+// Launches D = A . B^T with epilogue `epi` on `stream` (host side; see gemm_kernel). MA / MB:
+// the major mode of A ([M][K] or [K][M] in memory) and B ([N][K] or [K][N]).
+template <int BN, UMMA::Major MA = kKMajor, UMMA::Major MB = kKMajor, class Epi>
 inline cudaError_t run(const bf16 *A, const bf16 *B, int M, int N, int K, Epi epi, int *err, cudaStream_t stream,
                        int splits = 1) {
-    using C = Cfg<BN>;
+    using C = Cfg<BN, MA, MB>;
     if (M % kBM || N % BN || K % kBK || K <= 0 || splits < 1 || splits > K / kBK) return cudaErrorInvalidValue;
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) return cudaErrorInvalidValue;
-    Tensor gA = make_tensor(make_gmem_ptr(A), make_shape(M, K), make_stride(K, Int<1>{}));
-    Tensor gB = make_tensor(make_gmem_ptr(B), make_shape(N, K), make_stride(K, Int<1>{}));
+    Tensor gA = operand_view<MA>(A, M, K);
+    Tensor gB = operand_view<MB>(B, N, K);
     typename C::TiledMma mma;
     auto cluster_vmnk = tiled_divide(make_layout(Shape<_1, _1, _1>{}), make_tile(typename C::TiledMma::AtomThrID{}));
     auto tma_a = make_tma_atom_A_sm100<bf16>(SM90_TMA_LOAD{}, gA, typename C::SmemA{}(_, _, _, 0),
                                              typename C::Tiler{}, mma, cluster_vmnk);
     auto tma_b = make_tma_atom_B_sm100<bf16>(SM90_TMA_LOAD{}, gB, typename C::SmemB{}(_, _, _, 0),
                                              typename C::Tiler{}, mma, cluster_vmnk);
-    auto kernel = gemm_kernel<BN, decltype(tma_a), decltype(tma_b), Epi>;
+    auto kernel = gemm_kernel<BN, MA, MB, decltype(tma_a), decltype(tma_b), Epi>;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::kSmem);
     if (e != cudaSuccess) return e;
     dim3 grid(M / kBM, N / BN, splits);

@@ -104,23 +104,24 @@ def river_values(boards, ranges, pots, stacks, iterations, chunk=1024):
     configuration tuned on the first batch and reused; and the seconds spent."""
     n = len(boards)
     order = P.card_order()
+    holds = ((order[None, :] >> np.arange(52, dtype=np.uint64)[:, None]) & np.uint64(1)) != 0  # [card][hand]
     values = np.zeros((n, 2, P.HANDS), np.float32)
     cfg = None
     t0 = time.perf_counter()
     for s0 in range(0, n, chunk):
         s1 = min(n, s0 + chunk)
         m = s1 - s0
+        b4 = np.asarray(boards[s0:s1], np.uint64)
+        off = ((b4[:, None] >> np.arange(52, dtype=np.uint64)[None, :]) & np.uint64(1)) == 0
+        river = np.nonzero(off)[1].reshape(m, 48)  # the 48 river cards of each state, in card order
         specs = np.zeros(m * 48, P.SPEC_DTYPE)
-        rr = np.zeros((m * 48, 2, P.HANDS), np.float32)
-        k = 0
-        for i in range(s0, s1):
-            for c in range(52):
-                if (int(boards[i]) >> c) & 1:
-                    continue
-                specs[k] = (int(boards[i]) | (1 << c), pots[i], stacks[i], D.RIVER_SIZES, D.RIVER_RAISES)
-                rr[k] = ranges[i]
-                rr[k][:, (order & np.uint64(1 << c)) != 0] = 0.0
-                k += 1
+        specs["board"] = (b4[:, None] | (np.uint64(1) << river.astype(np.uint64))).ravel()
+        specs["pot"] = np.repeat(np.asarray(pots[s0:s1], np.float32), 48)
+        specs["stack"] = np.repeat(np.asarray(stacks[s0:s1], np.float32), 48)
+        specs["sizes"] = D.RIVER_SIZES
+        specs["max_raises"] = D.RIVER_RAISES
+        rr = np.repeat(np.asarray(ranges[s0:s1], np.float32), 48, axis=0)
+        rr *= ~holds[river.ravel()][:, None, :]  # hands holding the river card
         b = P.Batch(specs, rr)
         b.enable_average()
         b.iterate(1)

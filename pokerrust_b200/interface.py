@@ -145,6 +145,8 @@ def lib():
         L.pr_batch_iterate_noalloc.argtypes = [vp, i32]
         L.pr_gemm_bf16.restype = i32
         L.pr_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, i32, vp]
+        L.pr_gemm_bf16_major.restype = i32
+        L.pr_gemm_bf16_major.argtypes = [vp, vp, vp, i32, i32, i32, i32, i32, i32, vp]
         L.pr_gemm_bf16_async.restype = i32
         L.pr_gemm_bf16_async.argtypes = [vp, vp, vp, i32, i32, i32, i32, vp, vp]
         L.pr_mlp_new.restype = vp

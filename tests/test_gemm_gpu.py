@@ -25,6 +25,28 @@ def test_gemm_matches_fp32(M, N, K, bn):
     assert err <= 1e-5 * want.abs().max().item(), err
 
 
+@pytest.mark.parametrize("a_mn,b_mn", [(0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K,bn", [(128, 256, 64, 256), (256, 512, 320, 256), (1024, 2816, 4096, 256),
+                                      (384, 384, 1024, 128)])
+def test_gemm_mn_major_operands(M, N, K, bn, a_mn, b_mn):
+    """Operands stored MN-major ([K][M] for A, [K][N] for B), read by the tensor cores without
+    a transpose in memory: the same product."""
+    import torch
+    import pokerrust_b200 as P
+    g = torch.Generator(device="cuda").manual_seed(M * 5 + N + K + 7 * a_mn + 3 * b_mn)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    As = A.T.contiguous() if a_mn else A
+    Bs = B.T.contiguous() if b_mn else B
+    D = torch.full((M, N), float("nan"), device="cuda", dtype=torch.float32)
+    torch.cuda.synchronize()
+    st = P.lib().pr_gemm_bf16_major(As.data_ptr(), Bs.data_ptr(), D.data_ptr(), M, N, K, bn, a_mn, b_mn, None)
+    assert st == 0
+    want = A.float() @ B.float().T
+    err = (D - want).abs().max().item()
+    assert err <= 1e-5 * want.abs().max().item(), err
+
+
 def test_gemm_rejects_bad_shapes():
     import torch
     import pokerrust_b200 as P
