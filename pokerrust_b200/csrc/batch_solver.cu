@@ -52,7 +52,6 @@ __global__ void __launch_bounds__(kSetupThreads) batch_setup_kernel(const BSub *
     __shared__ uint16_t first[kBRow], last[kBRow];
     __shared__ uint8_t lo_li[kBRow], hi_li[kBRow], lo_gs[kBRow], lo_ge[kBRow], hi_gs[kBRow], hi_ge[kBRow];
     __shared__ uint8_t list_card[48];
-    __shared__ int8_t list_of_card[52];
 
     if (__popcll(board) != 5 || (board >> 52)) {
         if (tid == 0) atomicOr(err, 1);
@@ -88,13 +87,8 @@ __global__ void __launch_bounds__(kSetupThreads) batch_setup_kernel(const BSub *
     for (int p = tid; p < kBRow; p += kSetupThreads) hand_at[p] = p < kBLive ? (uint16_t)(key[p] & 2047) : 0xFFFF;
     if (tid == 0) {
         int n = 0;
-        for (int c = 0; c < 52; c++) {
-            list_of_card[c] = -1;
-            if (!((board >> c) & 1)) {
-                list_of_card[c] = (int8_t)n;
-                list_card[n++] = (uint8_t)c;
-            }
-        }
+        for (int c = 0; c < 52; c++)
+            if (!((board >> c) & 1)) list_card[n++] = (uint8_t)c;
         list_card[47] = 0;
         // tie groups: equal hand values
         int f = 0;
@@ -296,6 +290,23 @@ __device__ __forceinline__ void st_k(T *row, int pos0, const U (&in)[K]) {
     }
 }
 
+// Rows read by the walks come in edge order (edges are numbered in pre-order): a node's
+// strategy sums read rows [edge, edge + nchild), and the next nodes read the rows after them.
+// This asks L1 for the 128-byte lines that a warp's positions of rows [first, first + n)
+// occupy (rows from `rows` on, past the subgame's last edge, are skipped), one line per lane.
+constexpr int kPfRows = 4;  // rows of lookahead
+template <int K>
+__device__ __forceinline__ void prefetch_rows(const float *base, int first, int n, int rows, int warp, int lane) {
+    constexpr int kSpan = 32 * K;                  // floats of a row that one warp covers
+    constexpr int kLines = (kSpan + 31) / 32 + 1;  // 128-byte lines the span can touch
+    static_assert(kPfRows * kLines <= 32, "one prefetch per lane");
+    if (lane < n * kLines) {
+        const int row = first + lane / kLines;
+        const int f = warp * kSpan + (lane % kLines) * 32;
+        if (row < rows && f < kBRow) asm volatile("prefetch.global.L1 [%0];" ::"l"(base + (size_t)row * kBRow + f));
+    }
+}
+
 // Strategy of edge `e` at a node whose out-edges have positive-part sum `S`.
 template <typename V, bool USEAVG>
 __device__ __forceinline__ V sigma(V val, V S, int n) {
@@ -494,7 +505,9 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
 #pragma unroll
                             for (int k = 0; k < K; k++) sum[k] += sv[k] > V(0) ? sv[k] : V(0);
                         }
+                        prefetch_rows<K>(Src, nd.edge + nd.nchild, kPfRows, sub.num_edges, warp, lane);
                     }
+                    if (AVG && own) prefetch_rows<K>(A, nd.edge, min(nd.nchild, kPfRows), sub.num_edges, warp, lane);
 #pragma unroll
                     for (int k = 0; k < K; k++) St[k][d] = sum[k];
                 } else {
@@ -641,6 +654,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
 #pragma unroll
                             for (int k = 0; k < K; k++) sum[k] += sv[k] > V(0) ? sv[k] : V(0);
                         }
+                        prefetch_rows<K>(Src, nd.edge + nd.nchild, kPfRows, sub.num_edges, warp, lane);
                     }
 #pragma unroll
                     for (int k = 0; k < K; k++) Sb[k][d] = sum[k];

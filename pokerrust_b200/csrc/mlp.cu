@@ -270,26 +270,66 @@ __global__ void bias_sum_kernel(const float *__restrict__ part, float *__restric
     db[c] = t;
 }
 
-// Adam on f32 master weights; padding (rows >= n_live or columns >= k_live) stays zero.
-__global__ void adam_kernel(float *__restrict__ w, float *__restrict__ m1, float *__restrict__ m2,
-                            const float *__restrict__ g, bf16 *__restrict__ wb, int rows, int cols, int n_live,
-                            int k_live, float lr, float b1, float b2, float c1, float c2, float eps) {
-    const size_t total = (size_t)rows * cols;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        const int r = (int)(i / cols), c = (int)(i % cols);
-        if (r >= n_live || c >= k_live) {
-            w[i] = 0.0f;
-            if (wb) wb[i] = bf16(0.0f);
-            continue;
+// Adam over every layer's weights and biases in one launch. Each entry is one parameter
+// array; its gradient is the sum of `splits` split-K parts in part order (the weights) or
+// one array (the biases). Padding (rows >= n_live or columns >= k_live) stays zero.
+struct AdamEntry {
+    float *w, *m1, *m2;
+    const float *grad;  // [splits][rows][cols]
+    bf16 *wb;           // bf16 copy, or null
+    int rows, cols, n_live, k_live, splits;
+};
+struct AdamArgs {
+    AdamEntry e[2 * kLayers];
+    int count;
+    float lr, b1, b2, c1, c2, eps;
+};
+
+// blockIdx.y picks the entry; CTAs stride over its rows, threads over 4-column groups
+// (every padded width is a multiple of 4), so no index needs a division.
+__global__ void adam_all_kernel(const __grid_constant__ AdamArgs a) {
+    const AdamEntry &E = a.e[blockIdx.y];
+    const size_t n = (size_t)E.rows * E.cols;
+    const int cols4 = E.cols / 4;
+    for (int r = blockIdx.x; r < E.rows; r += gridDim.x) {
+        for (int q = threadIdx.x; q < cols4; q += blockDim.x) {
+            const size_t li = (size_t)r * E.cols + 4 * q;
+            float4 w = *reinterpret_cast<const float4 *>(E.w + li);
+            float4 m1 = *reinterpret_cast<const float4 *>(E.m1 + li);
+            float4 m2 = *reinterpret_cast<const float4 *>(E.m2 + li);
+            float4 g = *reinterpret_cast<const float4 *>(E.grad + li);
+            for (int z = 1; z < E.splits; z++) {
+                const float4 v = *reinterpret_cast<const float4 *>(E.grad + (size_t)z * n + li);
+                g.x += v.x;
+                g.y += v.y;
+                g.z += v.z;
+                g.w += v.w;
+            }
+            float *wv = &w.x, *av = &m1.x, *bv = &m2.x;
+            const float *gv = &g.x;
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                if (r >= E.n_live || 4 * q + t >= E.k_live) {
+                    wv[t] = 0.0f;
+                    continue;
+                }
+                const float m = a.b1 * av[t] + (1.0f - a.b1) * gv[t];
+                const float v = a.b2 * bv[t] + (1.0f - a.b2) * gv[t] * gv[t];
+                av[t] = m;
+                bv[t] = v;
+                wv[t] -= a.lr * ((m / a.c1) / (sqrtf(v / a.c2) + a.eps));
+            }
+            *reinterpret_cast<float4 *>(E.w + li) = w;
+            *reinterpret_cast<float4 *>(E.m1 + li) = m1;
+            *reinterpret_cast<float4 *>(E.m2 + li) = m2;
+            if (E.wb) {
+                const bf16 h[4] = {bf16(w.x), bf16(w.y), bf16(w.z), bf16(w.w)};
+                uint2 u;
+                u.x = (uint32_t)h[0].raw() | ((uint32_t)h[1].raw() << 16);
+                u.y = (uint32_t)h[2].raw() | ((uint32_t)h[3].raw() << 16);
+                *reinterpret_cast<uint2 *>(E.wb + li) = u;
+            }
         }
-        const float gi = g[i];
-        const float a = b1 * m1[i] + (1.0f - b1) * gi;
-        const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
-        m1[i] = a;
-        m2[i] = b;
-        const float upd = (a / c1) / (sqrtf(b / c2) + eps);
-        w[i] -= lr * upd;
-        if (wb) wb[i] = bf16(w[i]);
     }
 }
 
@@ -333,11 +373,10 @@ struct Net {
     float *Y = nullptr;
     bf16 *dY = nullptr;
     double *partial = nullptr;
-    float *parts = nullptr;  // split-K partial products of the weight gradients
+    float *parts[kLayers] = {};  // per layer: split-K partial products of the weight gradients
     float *bias_parts = nullptr;  // [kBiasChunks][cols] partial bias gradients
     int step = 0;
     static constexpr int kSplits = 4;
-    static constexpr size_t kPartsMax = (size_t)kOutPad * kInPad;  // largest weight matrix
     std::vector<void *> owned;
 
     template <class T>
@@ -374,17 +413,18 @@ struct Net {
         return check(e, "forward");
     }
 
-    // dW[M][N] = G^T . In over the batch (G: [rows][M], In: [rows][N], both read MN-major), as
-    // kSplits split-K GEMMs summed in part order (the weight-gradient GEMMs have few output
-    // tiles)
-    cudaError_t weight_grad(const bf16 *G, const bf16 *In, int M, int N, float *dWout) {
-        const size_t n = (size_t)M * N;
-        EpiStore epi{parts, N, n};
-        cudaError_t e =
-            gemm::run<256, gemm::kMNMajor, gemm::kMNMajor>(G, In, M, N, rows, epi, d_err, stream, kSplits);
-        if (e != cudaSuccess) return e;
-        split_sum_kernel<<<592, 256, 0, stream>>>(parts, dWout, n, kSplits);
-        return cudaGetLastError();
+    // dW[M][N] of layer l = G^T . In over the batch (G: [rows][M], In: [rows][N], both read
+    // MN-major), as kSplits split-K GEMMs (the weight-gradient GEMMs have few output tiles)
+    // whose parts stay apart: Adam sums them in part order
+    cudaError_t weight_grad(const bf16 *G, const bf16 *In, int M, int N, int l) {
+        EpiStore epi{parts[l], N, (size_t)M * N};
+        return gemm::run<256, gemm::kMNMajor, gemm::kMNMajor>(G, In, M, N, rows, epi, d_err, stream, kSplits);
+    }
+
+    // the gradient of layer l's weights as one array (dW[l]), from its split-K parts
+    int materialize_grad(int l) {
+        split_sum_kernel<<<592, 256, 0, stream>>>(parts[l], dW[l], (size_t)kN[l] * kK[l], kSplits);
+        return check(cudaGetLastError(), "gradient sum");
     }
 
     void bias_grad(const bf16 *G, float *dbout, int cols) {
@@ -395,14 +435,14 @@ struct Net {
     // backward from dY (bf16), gradients into dW / db; the input gradients dZ . W read the
     // weights [out][in] MN-major
     int backward() {
-        cudaError_t e = weight_grad(dY, H[3], kOutPad, kHid, dW[4]);
+        cudaError_t e = weight_grad(dY, H[3], kOutPad, kHid, 4);
         bias_grad(dY, db[4], kOutPad);
         if (e == cudaSuccess) {
             EpiGeluGrad epi{Z[3], dZ[3], kHid};
             e = gemm::run<256, gemm::kKMajor, gemm::kMNMajor>(dY, Wb[4], rows, kHid, kOutPad, epi, d_err, stream);
         }
         for (int l = 3; l >= 0 && e == cudaSuccess; l--) {
-            e = weight_grad(dZ[l], l > 0 ? H[l - 1] : X, kHid, kK[l], dW[l]);
+            e = weight_grad(dZ[l], l > 0 ? H[l - 1] : X, kHid, kK[l], l);
             bias_grad(dZ[l], db[l], kHid);
             if (e == cudaSuccess && l > 0) {
                 EpiGeluGrad epi2{Z[l - 1], dZ[l - 1], kHid};
@@ -416,14 +456,18 @@ struct Net {
 
     int adam(float lr) {
         step++;
-        const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-        const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+        AdamArgs a{};
+        a.lr = lr;
+        a.b1 = 0.9f;
+        a.b2 = 0.999f;
+        a.eps = 1e-8f;
+        a.c1 = 1.0f - powf(a.b1, (float)step);
+        a.c2 = 1.0f - powf(a.b2, (float)step);
         for (int l = 0; l < kLayers; l++) {
-            adam_kernel<<<1184, 256, 0, stream>>>(W[l], mW[l], vW[l], dW[l], Wb[l], kN[l], kK[l], kNLive[l],
-                                                 kKLive[l], lr, b1, b2, c1, c2, eps);
-            adam_kernel<<<8, 256, 0, stream>>>(b[l], mb[l], vb[l], db[l], nullptr, 1, kN[l], 1, kNLive[l], lr, b1,
-                                               b2, c1, c2, eps);
+            a.e[a.count++] = AdamEntry{W[l], mW[l], vW[l], parts[l], Wb[l], kN[l], kK[l], kNLive[l], kKLive[l], kSplits};
+            a.e[a.count++] = AdamEntry{b[l], mb[l], vb[l], db[l], nullptr, 1, kN[l], 1, kNLive[l], 1};
         }
+        adam_all_kernel<<<dim3(296, a.count), 256, 0, stream>>>(a);
         return check(cudaGetLastError(), "adam");
     }
 
@@ -463,7 +507,8 @@ void *pr_mlp_new(int rows, uint64_t seed) {
     }
     ok = ok && n->alloc(&n->X, (size_t)rows * kInPad) && n->alloc(&n->Y, (size_t)rows * kOutPad) &&
          n->alloc(&n->dY, (size_t)rows * kOutPad) && n->alloc(&n->partial, rows) &&
-         n->alloc(&n->parts, Net::kSplits * Net::kPartsMax) && n->alloc(&n->bias_parts, (size_t)kBiasChunks * kOutPad);
+         n->alloc(&n->bias_parts, (size_t)kBiasChunks * kOutPad);
+    for (int l = 0; l < kLayers && ok; l++) ok = n->alloc(&n->parts[l], (size_t)Net::kSplits * kN[l] * kK[l]);
     for (int l = 0; l < 4 && ok; l++)
         ok = n->alloc(&n->Z[l], (size_t)rows * kHid) && n->alloc(&n->H[l], (size_t)rows * kHid) &&
              n->alloc(&n->dZ[l], (size_t)rows * kHid);
@@ -600,7 +645,9 @@ int pr_mlp_set_layer(void *net, int l, const float *W, const float *bias) {
 
 int pr_mlp_get_grad(void *net, int l, float *dW, float *dbias) {
     Net *n = (Net *)net;
-    return n ? layer_io(n, l, n->dW[l], n->db[l], dW, dbias, true) : 2;
+    if (!n || l < 0 || l >= kLayers) return 2;
+    if (int st = n->materialize_grad(l)) return st;
+    return layer_io(n, l, n->dW[l], n->db[l], dW, dbias, true);
 }
 
 }  // extern "C"
