@@ -5,8 +5,7 @@
 // shared-memory layout, so transposed operands need no transpose in memory.
 //
 // One CTA computes one 128 x BN tile. Warp 0 (one thread) streams 128 x 64 / BN x 64 tiles
-// of A and B into shared memory with TMA (128-byte swizzle, STAGES-deep ring, no
-// multicast); warp 1 (one thread) issues tcgen05.mma (M = 128, N = BN, K = 16 per
+// of A and B into shared memory with TMA (128-byte swizzle, 4-deep ring, no multicast); warp 1 (one thread) issues tcgen05.mma (M = 128, N = BN, K = 16 per
 // instruction) into a TMEM accumulator and frees each stage with tcgen05.commit; then the
 // four warps read the accumulator rows back with tcgen05.ld (warp w owns TMEM lanes
 // 32w..32w+31) and run the epilogue. Every mbarrier wait is bounded: on time-out the kernel
@@ -38,7 +37,6 @@ using bf16 = cutlass::bfloat16_t;
 
 constexpr int kBM = 128;
 constexpr int kBK = 64;
-constexpr int kStages = 4;
 constexpr int kThreads = 128;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // give up on an mbarrier after 2 s
 
@@ -57,6 +55,8 @@ using TileOrder = std::conditional_t<MJ == UMMA::Major::K, GenColMajor, Step<_2,
 
 template <int BN, UMMA::Major MA = kKMajor, UMMA::Major MB = kKMajor>
 struct Cfg {
+    // stages of the TMA ring (a 3-stage ring with two 128 x 128 CTAs per SM measured slower)
+    static constexpr int kStages = 4;
     using TiledMma = decltype(make_tiled_mma(SM100_MMA_F16BF16_SS<bf16, bf16, float, kBM, BN, MA, MB>{}));
     using Tiler = Shape<Int<kBM>, Int<BN>, Int<kBK>>;
     using ShapeA = decltype(partition_shape_A(TiledMma{}, make_shape(Int<kBM>{}, Int<kBK>{})));
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int k_tiles = (int)(((long long)k_all * (blockIdx.z + 1)) / gridDim.z) - k_begin;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; s++) {
+        for (int s = 0; s < C::kStages; s++) {
             cutlass::arch::ClusterTransactionBarrier::init(&ss.full[s], 1);
             cutlass::arch::ClusterBarrier::init(&ss.empty[s], 1);
         }
@@ -173,8 +173,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 0 && lane == 0) {
         // producer: TMA loads of A and B tiles into the stage ring
         for (int k = 0; k < k_tiles; k++) {
-            const int s = k % kStages;
-            if (k >= kStages && !bar_wait(&ss.empty[s], ((k / kStages) - 1) & 1)) {
+            const int s = k % C::kStages;
+            if (k >= C::kStages && !bar_wait(&ss.empty[s], ((k / C::kStages) - 1) & 1)) {
                 atomicOr(err, kErrProducer);
                 ss.failed = 1;
                 break;
@@ -189,9 +189,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         tiled_mma.accumulate_ = UMMA::ScaleOut::Zero;
         bool ok = true;
         for (int k = 0; k < k_tiles && ok; k++) {
-            const int s = k % kStages;
+            const int s = k % C::kStages;
             // warp-uniform decision: the MMA and commit below are warp-collective
-            if (!__all_sync(0xffffffffu, bar_wait(&ss.full[s], (k / kStages) & 1))) {
+            if (!__all_sync(0xffffffffu, bar_wait(&ss.full[s], (k / C::kStages) & 1))) {
                 if (lane == 0) atomicOr(err, kErrMma);
                 ok = false;
                 break;
@@ -238,9 +238,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     // teardown: copies and MMAs in flight finish before shared memory and TMEM go away
     if (warp == 0 && lane == 0 && ss.failed) {
-        // only the last kStages loads can still be in flight (earlier stages were consumed)
-        for (int k = issued > kStages ? issued - kStages : 0; k < issued; k++)
-            bar_wait(&ss.full[k % kStages], (k / kStages) & 1);
+        // only the last ring of loads can still be in flight (earlier stages were consumed)
+        for (int k = issued > C::kStages ? issued - C::kStages : 0; k < issued; k++)
+            bar_wait(&ss.full[k % C::kStages], (k / C::kStages) & 1);
     }
     if (!acc_ok) bar_wait(&ss.acc, 0);
     tmem_fence_before_sync();
