@@ -170,9 +170,11 @@ def batch_section(P, rank, peak, cpu_threads, with_cpu):
         "tuned_pass_ms": [float(x) for x in tuned],
         "configs": [b.config(c) for c in range(2)],
     }
-    # convergence: restart from zero regrets, check every 25 iterations
+    # convergence: restart from zero regrets, average sums weighted by the iteration number,
+    # check every 25 iterations
     b2 = P.Batch(specs, ranges)
     b2.enable_average()
+    b2.set_linear_average(True)
     for c in range(2):
         cfg = b.config(c)
         b2.set_config(c, cfg["K"], cfg["per_sm"], cfg["order"])
@@ -191,6 +193,7 @@ def batch_section(P, rank, peak, cpu_threads, with_cpu):
             break
     out["exploitability_pct_pot"] = trace
     out["time_to_0.5pct_pot"] = reached
+    out["averaging"] = "linear (iteration t weighs t)"
     b2.close()
     b.close()
     if with_cpu:

@@ -212,6 +212,9 @@ int pr_batch_shape(void *batch, int s, int *num_nodes, int *num_edges, int *num_
 int pr_batch_enable_average(void *batch);
 /* CFR iterations: player 0 update, then player 1. */
 int pr_batch_iterate(void *batch, int iterations);
+/* Average sums weighted by the iteration number (on = 1: iteration t adds t x reach x
+ * strategy) or by 1 (on = 0, the default); the weight restarts at 1. */
+int pr_batch_set_linear_average(void *batch, int on);
 /* No counterpart in the reference. pr_batch_iterate for callers that may not allocate once
  * their solve loop runs: a process whose GPU memory is handed out by its own caching
  * allocator, or a loop on a shared GPU where a cudaMalloc / cudaFree (they synchronise the
@@ -337,7 +340,8 @@ int pr_full_iterate(void *game, int iterations);
 /* FP64 best responses to the average strategies over the whole game and the exploitability
  * (br0 + br1) / 2 per unit of joint range mass, in chips. resolve_iterations > 0 first
  * re-solves the river subgames of the leaves with chips behind from zero under the current
- * average flop and turn strategies (for net-leaf strategies, which stop at the turn). */
+ * average flop and turn strategies (for net-leaf strategies, which stop at the turn); this
+ * replaces those subgames' regrets and average sums. */
 int pr_full_exploitability(void *game, int resolve_iterations, double *br0, double *br1, double *expl);
 /* Device state: which 0 regrets / 1 average sums [edges][1326] f32; 2 reach [nodes][2][1326],
  * 3 leaf values [leaves][1326], 4 node values [nodes][1326] (f32, last CFR pass); 5, 6, 7

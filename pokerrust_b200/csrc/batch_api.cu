@@ -57,6 +57,8 @@ struct Batch {
     double *d_ranges64 = nullptr;  // [count][2][kBRow] double ranges of best responses inside a larger game
     bool own_weight = false;       // CFR average sums weighted by the updater's range
     const float *avg_weight = nullptr;  // device scalar weighting CFR average-sum terms (null: 1)
+    float *d_wt = nullptr;              // the batch's own weight scalar (linear averaging)
+    bool linear = false;                // iteration t adds t x its average-sum terms
     float *d_regrets = nullptr, *d_avg = nullptr;
     int *d_order = nullptr, *d_head = nullptr, *d_err = nullptr;
     void *d_sum = nullptr;   // [count] doubles
@@ -71,7 +73,7 @@ struct Batch {
         if (stream) cudaStreamSynchronize(stream);
         for (void *p : {(void *)d_subs, (void *)d_nodes, (void *)d_packs, (void *)d_ranges, (void *)d_ranges64,
                         (void *)d_regrets, (void *)d_avg, (void *)d_order, (void *)d_head, (void *)d_err, d_sum,
-                        d_root, d_child})
+                        d_root, d_child, (void *)d_wt})
             cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -138,6 +140,10 @@ struct Batch {
         if (e != cudaSuccess) return bfail("queue reset", e);
         for (int pl = 0; pl < 2; pl++)
             if (int st = pass(kBModeCFR, pl, 0, 0, nullptr, nullptr, pl)) return st;
+        if (linear) {
+            e = launch_weight_step(d_wt, stream);
+            if (e != cudaSuccess) return bfail("weight update", e);
+        }
         return 0;
     }
 };
@@ -398,6 +404,22 @@ int pr_batch_enable_average(void *batch) {
         return bfail("average-strategy allocation", e);
     b->avg_on = true;
     return 0;
+}
+
+// Average sums weighted by the iteration number (on: iteration t of the batch adds t x
+// reach x strategy; the weighting usual with regrets clipped at zero) or by 1 (off, the
+// default). The weight restarts at 1.
+int pr_batch_set_linear_average(void *batch, int on) {
+    Batch *b = (Batch *)batch;
+    if (!b) return 2;
+    cudaError_t e;
+    if (!b->d_wt && (e = cudaMalloc(&b->d_wt, sizeof(float))) != cudaSuccess) return bfail("weight allocation", e);
+    const float one = 1.0f;
+    e = cudaMemcpyAsync(b->d_wt, &one, sizeof(float), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bfail("weight reset", e);
+    b->linear = on != 0;
+    return batch_set_avg_weight(b, b->linear ? b->d_wt : nullptr);
 }
 
 int pr_batch_iterate(void *batch, int iterations) {

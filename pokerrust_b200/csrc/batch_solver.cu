@@ -694,6 +694,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
     }
 }
 
+__global__ void weight_step_kernel(float *w) { *w += 1.0f; }
+
 template <int K, typename V, int MODE, bool AVG, bool USEAVG>
 cudaError_t launch_one(const BLaunch &a, int ctas, int group, cudaStream_t stream) {
     const size_t smem = smem_bytes<V>(group);
@@ -741,6 +743,11 @@ int batch_group_leaves(int fp64) { return fp64 ? 8 : 16; }
 size_t batch_smem_bytes(int K, int fp64, int group) {
     (void)K;
     return fp64 ? smem_bytes<double>(group) : smem_bytes<float>(group);
+}
+
+cudaError_t launch_weight_step(float *w, cudaStream_t stream) {
+    weight_step_kernel<<<1, 1, 0, stream>>>(w);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_batch_pass(int mode, int K, int fp64, int avg, const BLaunch &a, int ctas, int group,

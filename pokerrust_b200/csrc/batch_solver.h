@@ -71,6 +71,9 @@ cudaError_t launch_batch_setup(const BSub *subs, int count, BPack *packs, const 
 cudaError_t launch_batch_pass(int mode, int K, int fp64, int avg, const BLaunch &a, int ctas, int max_leaves,
                               cudaStream_t stream);
 
+// Adds 1 to the device scalar *w (the next iteration's average weight), on `stream`.
+cudaError_t launch_weight_step(float *w, cudaStream_t stream);
+
 // Threads per CTA and shared memory of a configuration.
 int batch_threads(int K);
 size_t batch_smem_bytes(int K, int fp64, int group_leaves);

@@ -776,7 +776,8 @@ int pr_full_iterate(void *game, int iterations) {
 // response), and exploitability = (BR0 + BR1) / 2 per unit of joint range mass, in chips.
 // resolve_iterations > 0 first re-solves the river subgames of the leaves with chips behind
 // from zero, for that many CFR iterations, under the reach of the current average flop and
-// turn strategies (the net-leaf mode's strategies stop at the turn).
+// turn strategies (the net-leaf mode's strategies stop at the turn); their previous regrets
+// and average sums are replaced.
 int pr_full_exploitability(void *game, int resolve_iterations, double *br0, double *br1, double *expl) {
     Game *g = (Game *)game;
     if (!g || resolve_iterations < 0) return 2;

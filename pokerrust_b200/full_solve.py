@@ -124,6 +124,7 @@ def river_values(boards, ranges, pots, stacks, iterations, chunk=1024):
         rr *= ~holds[river.ravel()][:, None, :]  # hands holding the river card
         b = P.Batch(specs, rr)
         b.enable_average()
+        b.set_linear_average(True)
         b.iterate(1)
         if cfg is None:
             b.tune()

@@ -169,6 +169,8 @@ def lib():
         L.pr_batch_value_grad.argtypes = [vp, i32, vp, vp, vp]
         L.pr_batch_set_ranges.restype = i32
         L.pr_batch_set_ranges.argtypes = [vp, i32, vp]
+        L.pr_batch_set_linear_average.restype = i32
+        L.pr_batch_set_linear_average.argtypes = [vp, i32]
         L.pr_batch_iteration_bytes.restype = ctypes.c_double
         L.pr_batch_iteration_bytes.argtypes = [vp]
         L.pr_game_set_device_tree.restype = i32
@@ -609,6 +611,10 @@ class Batch:
     def iterate(self, iterations=1):
         _check(lib().pr_batch_iterate(self.ptr, int(iterations)), "pr_batch_iterate")
 
+    def set_linear_average(self, on=True):
+        """Average sums weighted by the iteration number (True) or by 1 (False, the default)."""
+        _check(lib().pr_batch_set_linear_average(self.ptr, int(bool(on))), "pr_batch_set_linear_average")
+
     def iterate_noalloc(self, iterations=1):
         """pr_batch_iterate_noalloc: eager iterations with the queue scratch in a fixed device
         array (no allocation; one call at a time)."""
@@ -904,7 +910,8 @@ class FullGame:
         self._write(1, data)
 
     def batch(self, which):
-        """The river subgames of the leaves with chips behind (0) or all-in (1), or None."""
+        """The river subgames of the leaves with chips behind (0) or all-in (1), or None. The
+        batch belongs to the game: use it only while the game is open."""
         p = lib().pr_full_batch(self.ptr, int(which))
         return Batch._borrow(p) if p else None
 

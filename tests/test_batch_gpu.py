@@ -175,3 +175,35 @@ def test_convergence_matches_oracle():
         assert abs(e_avg[s] - want) <= 0.02 * abs(want), (s, e_avg[s], want)
     assert np.all(e_avg < 0.2 * e_start)
     b.close()
+
+
+def test_linear_average():
+    """Linear averaging: the first iteration's sums equal the uniform ones (weight 1); the
+    second adds twice its terms; and the weighted average converges faster."""
+    import pokerrust_b200 as P
+    specs, ranges = P.random_subgames(6, seed=13)
+    u = P.Batch(specs, ranges)
+    u.enable_average()
+    w = P.Batch(specs, ranges)
+    w.enable_average()
+    w.set_linear_average(True)
+    u.iterate(1)
+    w.iterate(1)
+    for s in range(6):
+        assert np.array_equal(u.average(s), w.average(s))
+    a1 = [u.average(s) for s in range(6)]
+    u.iterate(1)
+    w.iterate(1)
+    for s in range(6):
+        # both ran the same regrets; the second iteration's terms are doubled
+        assert np.array_equal(u.regrets(s), w.regrets(s))
+        du = u.average(s) - a1[s]
+        dw = w.average(s) - a1[s]
+        assert np.allclose(dw, 2 * du, rtol=1e-5, atol=1e-7)
+    u.iterate(58)
+    w.iterate(58)
+    _, _, eu = u.exploitability(use_average=True)
+    _, _, ew = w.exploitability(use_average=True)
+    assert np.mean(ew) < np.mean(eu), (np.mean(ew), np.mean(eu))
+    u.close()
+    w.close()
