@@ -307,11 +307,18 @@ __device__ __forceinline__ void prefetch_rows(const float *base, int first, int 
     }
 }
 
-// Strategy of edge `e` at a node whose out-edges have positive-part sum `S`.
+// Regret matching with one division per node and hand: a node whose out-edges have
+// positive-part sum S keeps scale(S) = 1 / S, or -1 / n when S is at most the cutoff (1e-4
+// for regrets, 0 for average sums) and the strategy is uniform; an edge's probability is then
+// sigma(val, scale) = max(val, 0) x scale, or 1 / n.
 template <typename V, bool USEAVG>
-__device__ __forceinline__ V sigma(V val, V S, int n) {
+__device__ __forceinline__ V strategy_scale(V S, int n) {
     const V cut = USEAVG ? V(0) : V(1e-4f);
-    return S <= cut ? V(1) / V(n) : (val > V(0) ? val : V(0)) / S;
+    return S <= cut ? -(V(1) / V(n)) : V(1) / S;
+}
+template <typename V>
+__device__ __forceinline__ V sigma(V val, V scale) {
+    return scale < V(0) ? -scale : mul(val > V(0) ? val : V(0), scale);
 }
 
 template <int K, typename V, int MODE, bool AVG, bool USEAVG>
@@ -374,8 +381,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
 
         // walker state, per owned hand: depth-indexed stacks of the open path (indexed at run
         // time, so they live in local memory, cached in L1)
-        V po[K][DS], pp[K][DS], St[K][DS];   // top-down: opponent weight, own reach, strategy sums
-        V acc[K][DS], Sb[K][DS];             // bottom-up: node values, strategy sums
+        V po[K][DS], pp[K][DS], St[K][DS];   // top-down: opponent weight, own reach, strategy scales
+        V acc[K][DS], Sb[K][DS];             // bottom-up: node values, strategy scales
         int open_id[DS];
         int open_top = -1;
         int td = 0, bu = 0;
@@ -407,7 +414,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                     ld_k<K>(Src + ro, pos0, sv);
 #pragma unroll
                 for (int k = 0; k < K; k++)
-                    acc[k][dp] = acc[k][dp] + mul(sigma<V, USEAVG>(sv[k], Sb[k][dp], pq.nchild), v[k]);
+                    acc[k][dp] = acc[k][dp] + mul(sigma<V>(sv[k], Sb[k][dp]), v[k]);
                 if constexpr (MODE == kBModeCFR) {
                     float r[K];
 #pragma unroll
@@ -473,7 +480,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                     for (int k = 0; k < K; k++) {
                         const V po_par = po[k][d - 1];
                         const V pp_par = pp[k][d - 1];
-                        const V sg = need ? sigma<V, USEAVG>(sv[k], St[k][d - 1], pm.nchild) : V(1);
+                        const V sg = need ? sigma<V>(sv[k], St[k][d - 1]) : V(1);
                         npo[k] = own ? po_par : mul(po_par, sg);
                         npp[k] = own ? mul(pp_par, sg) : pp_par;
                     }
@@ -509,7 +516,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                     }
                     if (AVG && own) prefetch_rows<K>(A, nd.edge, min(nd.nchild, kPfRows), sub.num_edges, warp, lane);
 #pragma unroll
-                    for (int k = 0; k < K; k++) St[k][d] = sum[k];
+                    for (int k = 0; k < K; k++)
+                        St[k][d] = (!own || AVG) ? strategy_scale<V, USEAVG>(sum[k], nd.nchild) : V(0);
                 } else {
                     V xv[K];
 #pragma unroll
@@ -657,7 +665,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
                         prefetch_rows<K>(Src, nd.edge + nd.nchild, kPfRows, sub.num_edges, warp, lane);
                     }
 #pragma unroll
-                    for (int k = 0; k < K; k++) Sb[k][d] = sum[k];
+                    for (int k = 0; k < K; k++)
+                        Sb[k][d] = (own && MODE != kBModeBR) ? strategy_scale<V, USEAVG>(sum[k], nd.nchild) : V(0);
                 } else {
                     // a leaf: its value goes straight to the parent (open at depth d - 1)
                     V xv[K];

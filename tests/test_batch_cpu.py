@@ -16,9 +16,10 @@ def _specs(seed, n):
         pot = float(rng.integers(2, 201))
         stack = float(rng.integers(int(pot), 10 * int(pot) + 1))
         out.append((pot, stack, int(rng.integers(1, 8)), int(rng.integers(1, 4))))
-    # edge cases: a short stack (bets capped at all-in), coinciding sizes, all-in only
+    # edge cases: a short stack (bets capped at all-in), coinciding sizes, all-in only, no
+    # chips behind (checks to the showdown, as after an all-in on an earlier street)
     out += [(100.0, 30.0, 7, 3), (100.0, 100.0, 7, 3), (10.0, 10.0, 3, 2), (50.0, 500.0, 4, 3),
-            (2.0, 20.0, 1, 1), (200.0, 2000.0, 7, 3)]
+            (2.0, 20.0, 1, 1), (200.0, 2000.0, 7, 3), (40.0, 0.0, 3, 2)]
     return out
 
 
