@@ -201,6 +201,37 @@ def batch_section(P, rank, peak, cpu_threads, with_cpu):
     return out
 
 
+def adjoint_section(P, peak):
+    """Config 3: the adjoint pair on 1024 general river subgames at their average strategies
+    after 100 CFR iterations. Forward V = r0^T U(sigma) r1 (pr_batch_value), backward dV/dr0,
+    dV/dr1 and dV/dsigma at the root (pr_batch_value_grad), both through the C ABI with their
+    host outputs; algorithmic bytes sum_s (2 E_s 1081 4 + 4 1081 4) per forward + backward."""
+    specs, ranges = P.random_subgames(1024, seed=777)
+    b = P.Batch(specs, ranges)
+    b.enable_average()
+    b.set_linear_average(True)
+    b.iterate(100)
+    edges = sum(b.shape(i)[1] for i in range(b.count))
+    b.value(use_average=True)
+    b.value_grad(use_average=True)
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        b.value(use_average=True)
+    fwd = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        b.value_grad(use_average=True)
+    bwd = (time.perf_counter() - t0) / reps
+    nbytes = 2.0 * edges * 1081 * 4 + b.count * 4.0 * 1081 * 4
+    b.close()
+    return {"workload": "1024 river subgames (config-2 shapes), average strategies after 100 CFR iterations",
+            "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3,
+            "roofline": {"bound": "hbm", "achieved": nbytes / (fwd + bwd) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": nbytes / (fwd + bwd) / 1e9 / peak, "bytes_fwd_bwd": nbytes,
+                         "note": "API calls with host outputs (the backward copies [1024][8][1326] doubles)"}}
+
+
 def full_game_section(P):
     """The full fixed-flop game with general bets (flop and turn sweeps over batched river
     subgames): CFR iteration time, river subgames solved per second, iterations / solver
@@ -491,19 +522,21 @@ def run_gpu(args):
             torch.distributed.destroy_process_group()
         return 0
 
-    # end to end through the C ABI with host buffers
+    # end to end through the C ABI with host buffers (the caller's input and output rows are
+    # allocated once and reused every pass)
     host_in = np.ascontiguousarray(ranges)
+    out = np.zeros((n, 1326), np.float32)
     for i in range(max(1, args.warmup // 2)):
         builder.upload_all(host_in)
         P.evaluate_gpu(builder.ptr, tables, i % 2, False)
-        out = builder.download_all()
+        builder.download_all(out)
     barrier()
     e_steps = max(2, min(args.steps, 10))
     t0 = time.perf_counter()
     for i in range(e_steps):
         builder.upload_all(host_in)
         P.evaluate_gpu(builder.ptr, tables, i % 2, False)
-        out = builder.download_all()
+        builder.download_all(out)
     e2e_s = max_over_ranks((time.perf_counter() - t0) / e_steps, world, dev)
     assert np.all(np.isfinite(out))
 
@@ -529,6 +562,7 @@ def run_gpu(args):
     tp = tensor_peaks()
     vnet = value_net_section(P, tp[0], tp[1])
     full = full_game_section(P)
+    adj = adjoint_section(P, measured_peaks()[0])
 
     line = None
     if rank == 0:
@@ -566,6 +600,7 @@ def run_gpu(args):
             "batch_subgames": batch,
             "value_network": vnet,
             "full_game": full,
+            "adjoint": adj,
             "game_iteration": {"ms": dev_iter_s * 1e3,
                                "note": "one full CFR iteration of the fixed-flop game (both players): "
                                        "upper tree and river passes on the device, one CUDA graph",

@@ -599,7 +599,7 @@ void copy_rows(float *dst, size_t dst_stride, const float *src, size_t src_strid
     auto part = [&](int lo, int hi) {
         for (int i = lo; i < hi; i++) memcpy(dst + (size_t)i * dst_stride, src + (size_t)i * src_stride, kHands * sizeof(float));
     };
-    const int threads = count >= 4096 ? (int)std::min<unsigned>(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    const int threads = count >= 4096 ? (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency())) : 1;
     if (threads <= 1) {
         part(0, count);
         return;

@@ -390,8 +390,12 @@ class Builder:
         assert ranges.shape == (self.count, HANDS)
         _check(lib().pr_upload_batch(self.ptr, 0, self.count, _ptr(ranges)), "pr_upload_batch")
 
-    def download_all(self):
-        out = np.zeros((self.count, HANDS), dtype=np.float32)
+    def download_all(self, out=None):
+        """All rows of the staging ([count][1326] floats), into `out` when given (a caller that
+        reuses its buffers, as the reference's Rust caller reuses its vectors)."""
+        if out is None:
+            out = np.zeros((self.count, HANDS), dtype=np.float32)
+        assert out.shape == (self.count, HANDS) and out.dtype == np.float32 and out.flags.c_contiguous
         _check(lib().pr_download_batch(self.ptr, 0, self.count, _ptr(out)), "pr_download_batch")
         return out
 
