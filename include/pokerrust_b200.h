@@ -243,6 +243,9 @@ int pr_batch_root_values(void *batch, int player, int use_average, double *value
  * backward pass, not stored per node. Null outputs are skipped. */
 int pr_batch_value(void *batch, int use_average, double *V);
 int pr_batch_value_grad(void *batch, int use_average, double *d_r0, double *d_r1, double *d_sigma);
+/* The same backward pass with device outputs (device pointers, same layouts; null skipped),
+ * for callers that use the gradients on the GPU. Synchronous. */
+int pr_batch_value_grad_device(void *batch, int use_average, double *d_r0, double *d_r1, double *d_sigma);
 /* Replaces subgame s's ranges ([2][1326] floats). */
 int pr_batch_set_ranges(void *batch, int s, const float *r);
 /* Regrets / average sums of subgame s: [edges][1326] floats, edges in tree order. */

@@ -43,7 +43,6 @@ struct Batch {
     std::vector<BSub> subs;
     std::vector<BNode> nodes;
     std::vector<double> joint;  // sum over clash-free hand pairs of r0(h) r1(o)
-    std::vector<float> ranges0; // [count][1326] player 0's ranges (for the root adjoint)
     int total_edges = 0;
     int sms = 148;
     ClassCfg cls[kClasses];
@@ -64,6 +63,7 @@ struct Batch {
     void *d_sum = nullptr;   // [count] doubles
     void *d_root = nullptr;  // [count][kBRow] doubles, lazily
     void *d_child = nullptr; // [count][8][kBRow] doubles, lazily
+    double *d_hands = nullptr;  // [count][10][1326] doubles, lazily: results in hand order for host copies
     std::vector<uint16_t> hand;  // [count][kBRow] colex hand of each position
     cudaGraphExec_t graph = nullptr;
     bool graph_avg = false, graph_failed = false;
@@ -73,7 +73,7 @@ struct Batch {
         if (stream) cudaStreamSynchronize(stream);
         for (void *p : {(void *)d_subs, (void *)d_nodes, (void *)d_packs, (void *)d_ranges, (void *)d_ranges64,
                         (void *)d_regrets, (void *)d_avg, (void *)d_order, (void *)d_head, (void *)d_err, d_sum,
-                        d_root, d_child, (void *)d_wt})
+                        d_root, d_child, (void *)d_wt, (void *)d_hands})
             cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -147,6 +147,65 @@ struct Batch {
         return 0;
     }
 };
+
+// Position-order rows [count][rows][kBRow] -> hand-order rows [count][rows][1326] (hands that
+// touch the board are 0), times `sign`; with `weight` (position-order ranges [count][2][kBRow])
+// each value is first multiplied by player 0's range of the hand.
+__global__ void to_hands_kernel(const double *__restrict__ src, const BPack *__restrict__ packs, int rows,
+                                double sign, const float *__restrict__ weight, double *__restrict__ dst) {
+    const int s = blockIdx.x, r = blockIdx.y;
+    const uint16_t *pos_of = packs[s].pos_of;
+    const double *row = src + ((size_t)s * rows + r) * kBRow;
+    const float *w = weight ? weight + (size_t)s * 2 * kBRow : nullptr;
+    double *out = dst + ((size_t)s * rows + r) * 1326;
+    for (int h = threadIdx.x; h < 1326; h += blockDim.x) {
+        const int p = pos_of[h];
+        double v = 0.0;
+        if (p != 0xFFFF) {
+            v = row[p];
+            if (w) v = (double)w[p] * v;
+        }
+        out[h] = sign * v;
+    }
+}
+
+int to_hands(Batch *b, const void *src, int rows, double sign, const float *weight, double *dst) {
+    to_hands_kernel<<<dim3(b->count, rows), 256, 0, b->stream>>>((const double *)src, b->d_packs, rows, sign, weight,
+                                                                dst);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : bfail("hand-order copy", e);
+}
+
+int ensure_hands_buffer(Batch *b) {
+    if (b->d_hands) return 0;
+    cudaError_t e = cudaMalloc(&b->d_hands, sizeof(double) * 10 * 1326 * (size_t)b->count);
+    return e == cudaSuccess ? 0 : bfail("hand-order buffer allocation", e);
+}
+
+// The two evaluation passes of the adjoint, results in hand order on the device (null outputs
+// skipped); see pr_batch_value_grad.
+int value_grad_device(Batch *b, int use_average, double *d_r0, double *d_r1, double *d_sigma) {
+    cudaError_t e;
+    if (!b->d_root && (e = cudaMalloc(&b->d_root, sizeof(double) * kBRow * b->count)) != cudaSuccess)
+        return bfail("root value allocation", e);
+    if (!b->d_child && (e = cudaMalloc(&b->d_child, sizeof(double) * 8 * kBRow * b->count)) != cudaSuccess)
+        return bfail("root value allocation", e);
+    for (int pl = 0; pl < 2; pl++) {
+        e = cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
+        if (e == cudaSuccess && pl == 0)
+            e = cudaMemsetAsync(b->d_child, 0, sizeof(double) * 8 * kBRow * b->count, b->stream);
+        if (e != cudaSuccess) return bfail("queue reset", e);
+        if (int st = b->pass(kBModeEval, pl, 1, use_average, b->d_root, nullptr, 0, pl == 0 ? b->d_child : nullptr))
+            return st;
+        double *out = pl == 0 ? d_r0 : d_r1;
+        if (out)
+            if (int st = to_hands(b, b->d_root, 1, pl == 0 ? 1.0 : -1.0, nullptr, out)) return st;
+        if (pl == 0 && d_sigma)
+            if (int st = to_hands(b, b->d_child, 8, 1.0, b->d_ranges, d_sigma)) return st;
+    }
+    e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? 0 : bfail("adjoint", e);
+}
 
 // ---- no-allocation iteration ----
 // Work-queue scratch of pr_batch_iterate_noalloc: kClasses * 2 queue heads, then the queue
@@ -306,9 +365,6 @@ void *pr_batch_new(const pr_subgame *specs, int count, const float *ranges) {
         b->joint[s] = j;
     }
     b->total_edges = edges;
-    b->ranges0.resize((size_t)count * 1326);
-    for (int s = 0; s < count; s++)
-        memcpy(b->ranges0.data() + (size_t)s * 1326, ranges + (size_t)s * 2 * 1326, sizeof(float) * 1326);
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
@@ -505,20 +561,15 @@ int pr_batch_root_values(void *batch, int player, int use_average, double *value
     e = cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
     if (e != cudaSuccess) return bfail("queue reset", e);
     if (int st = b->pass(kBModeEval, player, 1, use_average, b->d_root, b->d_sum, 3)) return st;
-    std::vector<double> rv((size_t)kBRow * b->count);
-    e = cudaMemcpyAsync(rv.data(), b->d_root, sizeof(double) * rv.size(), cudaMemcpyDeviceToHost, b->stream);
+    if (values) {
+        if (int st = ensure_hands_buffer(b)) return st;
+        if (int st = to_hands(b, b->d_root, 1, 1.0, nullptr, b->d_hands)) return st;
+        e = cudaMemcpyAsync(values, b->d_hands, sizeof(double) * 1326 * b->count, cudaMemcpyDeviceToHost, b->stream);
+    }
     if (e == cudaSuccess && sums)
         e = cudaMemcpyAsync(sums, b->d_sum, sizeof(double) * b->count, cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-    if (e != cudaSuccess) return bfail("evaluation", e);
-    if (values) {
-        for (int s = 0; s < b->count; s++) {
-            double *out = values + (size_t)s * 1326;
-            for (int h = 0; h < 1326; h++) out[h] = 0.0;
-            for (int p = 0; p < kBLive; p++) out[b->hand[(size_t)s * kBRow + p]] = rv[(size_t)s * kBRow + p];
-        }
-    }
-    return 0;
+    return e == cudaSuccess ? 0 : bfail("evaluation", e);
 }
 
 // CFR iterations like pr_batch_iterate for callers that may not allocate once their solve
@@ -592,48 +643,24 @@ int pr_batch_value(void *batch, int use_average, double *V) {
 int pr_batch_value_grad(void *batch, int use_average, double *d_r0, double *d_r1, double *d_sigma) {
     Batch *b = (Batch *)batch;
     if (!b || (use_average && !b->avg_on)) return 2;
-    cudaError_t e;
-    if (!b->d_root && (e = cudaMalloc(&b->d_root, sizeof(double) * kBRow * b->count)) != cudaSuccess)
-        return bfail("root value allocation", e);
-    if (!b->d_child && (e = cudaMalloc(&b->d_child, sizeof(double) * 8 * kBRow * b->count)) != cudaSuccess)
-        return bfail("root value allocation", e);
-    std::vector<double> rv((size_t)kBRow * b->count), cv;
-    for (int pl = 0; pl < 2; pl++) {
-        e = cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
-        if (e == cudaSuccess && pl == 0) e = cudaMemsetAsync(b->d_child, 0, sizeof(double) * 8 * kBRow * b->count, b->stream);
-        if (e != cudaSuccess) return bfail("queue reset", e);
-        if (int st = b->pass(kBModeEval, pl, 1, use_average, b->d_root, nullptr, 0, pl == 0 ? b->d_child : nullptr))
-            return st;
-        e = cudaMemcpyAsync(rv.data(), b->d_root, sizeof(double) * rv.size(), cudaMemcpyDeviceToHost, b->stream);
-        if (e == cudaSuccess && pl == 0 && d_sigma) {
-            cv.resize((size_t)8 * kBRow * b->count);
-            e = cudaMemcpyAsync(cv.data(), b->d_child, sizeof(double) * cv.size(), cudaMemcpyDeviceToHost, b->stream);
-        }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-        if (e != cudaSuccess) return bfail("adjoint", e);
-        double *out = pl == 0 ? d_r0 : d_r1;
-        for (int s = 0; s < b->count && out; s++) {
-            double *o = out + (size_t)s * 1326;
-            for (int h = 0; h < 1326; h++) o[h] = 0.0;
-            for (int p = 0; p < kBLive; p++)
-                o[b->hand[(size_t)s * kBRow + p]] = (pl == 0 ? 1.0 : -1.0) * rv[(size_t)s * kBRow + p];
-        }
-        if (pl == 0 && d_sigma) {
-            for (int s = 0; s < b->count; s++) {
-                const float *r0 = b->ranges0.data() + (size_t)s * 1326;
-                for (int a = 0; a < 8; a++) {
-                    double *o = d_sigma + ((size_t)s * 8 + a) * 1326;
-                    for (int h = 0; h < 1326; h++) o[h] = 0.0;
-                    if (a >= b->nodes[b->subs[s].node_off].nchild) continue;
-                    for (int p = 0; p < kBLive; p++) {
-                        const int h = b->hand[(size_t)s * kBRow + p];
-                        o[h] = (double)r0[h] * cv[((size_t)s * 8 + a) * kBRow + p];
-                    }
-                }
-            }
-        }
-    }
-    return 0;
+    if (int st = ensure_hands_buffer(b)) return st;
+    const size_t n = (size_t)1326 * b->count;
+    double *h0 = b->d_hands, *h1 = h0 + n, *hs = h1 + n;
+    if (int st = value_grad_device(b, use_average, d_r0 ? h0 : nullptr, d_r1 ? h1 : nullptr, d_sigma ? hs : nullptr))
+        return st;
+    cudaError_t e = cudaSuccess;
+    if (d_r0) e = cudaMemcpy(d_r0, h0, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && d_r1) e = cudaMemcpy(d_r1, h1, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && d_sigma) e = cudaMemcpy(d_sigma, hs, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? 0 : bfail("adjoint copy", e);
+}
+
+// The same adjoint with device outputs (device pointers, same layouts), for callers that use
+// the gradients on the GPU; synchronous.
+int pr_batch_value_grad_device(void *batch, int use_average, double *d_r0, double *d_r1, double *d_sigma) {
+    Batch *b = (Batch *)batch;
+    if (!b || (use_average && !b->avg_on)) return 2;
+    return value_grad_device(b, use_average, d_r0, d_r1, d_sigma);
 }
 
 // Replaces the ranges of subgame s ([2][1326] floats, colex order).
@@ -644,7 +671,6 @@ int pr_batch_set_ranges(void *batch, int s, const float *r) {
     const uint16_t *hand = b->hand.data() + (size_t)s * kBRow;
     for (int pl = 0; pl < 2; pl++)
         for (int p = 0; p < kBLive; p++) rows[pl * kBRow + p] = r[pl * 1326 + hand[p]];
-    memcpy(b->ranges0.data() + (size_t)s * 1326, r, sizeof(float) * 1326);
     cudaStreamSynchronize(b->stream);
     cudaError_t e = cudaMemcpy(b->d_ranges + (size_t)s * 2 * kBRow, rows.data(), sizeof(float) * 2 * kBRow,
                                cudaMemcpyHostToDevice);

@@ -167,6 +167,8 @@ def lib():
         L.pr_batch_value.argtypes = [vp, i32, vp]
         L.pr_batch_value_grad.restype = i32
         L.pr_batch_value_grad.argtypes = [vp, i32, vp, vp, vp]
+        L.pr_batch_value_grad_device.restype = i32
+        L.pr_batch_value_grad_device.argtypes = [vp, i32, vp, vp, vp]
         L.pr_batch_set_ranges.restype = i32
         L.pr_batch_set_ranges.argtypes = [vp, i32, vp]
         L.pr_batch_set_linear_average.restype = i32
@@ -653,6 +655,13 @@ class Batch:
         _check(lib().pr_batch_value_grad(self.ptr, int(bool(use_average)), _ptr(g0), _ptr(g1), _ptr(gs)),
                "pr_batch_value_grad")
         return g0, g1, gs
+
+    def value_grad_device(self, d_r0, d_r1, d_sigma, use_average=False):
+        """Backward with device outputs: torch tensors (float64, [count][1326], [count][1326],
+        [count][8][1326]) or None to skip one."""
+        p = lambda t: t.data_ptr() if t is not None else None
+        _check(lib().pr_batch_value_grad_device(self.ptr, int(bool(use_average)), p(d_r0), p(d_r1), p(d_sigma)),
+               "pr_batch_value_grad_device")
 
     def set_ranges(self, s, r):
         r = np.ascontiguousarray(r, np.float32).reshape(2, HANDS)

@@ -124,3 +124,18 @@ def test_root_strategy_gradient_by_chain_rule(solved):
                 got = (vals[0] - vals[1]) / (float(hi) + float(lo))
                 scale = np.abs(gs[s, :n, h]).max() / tot
                 assert abs(got - want) <= 1e-4 * max(scale, 1e-30), (s, h, a, got, want)
+
+
+def test_device_outputs_match_host_outputs(solved):
+    """pr_batch_value_grad_device writes the same gradients into device buffers."""
+    import torch
+    b, specs, ranges = solved
+    g0, g1, gs = b.value_grad(use_average=True)
+    d0 = torch.zeros((b.count, 1326), dtype=torch.float64, device="cuda")
+    d1 = torch.zeros_like(d0)
+    ds = torch.zeros((b.count, 8, 1326), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    b.value_grad_device(d0, d1, ds, use_average=True)
+    assert np.array_equal(d0.cpu().numpy(), g0)
+    assert np.array_equal(d1.cpu().numpy(), g1)
+    assert np.array_equal(ds.cpu().numpy(), gs)
