@@ -6,7 +6,7 @@ Tolerances: before any update both sides run the same arithmetic from uniform st
 so single precision agrees to 1e-4 and double precision to 1e-9 (relative). After two
 iterations f32 rounding has been amplified through regret clipping (see
 test_river_gpu.py); exploitability, an aggregate, must still agree to 1e-3, well inside
-the north-star bound of 1%.
+the 1 % bound set for FP64 exploitability.
 """
 import os
 

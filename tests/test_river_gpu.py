@@ -4,7 +4,7 @@ through the C ABI.
 Tolerance: results and regrets are f32 sums of up to ~10^5 terms computed in a different
 order from the reference; per subgame we require
     max |gpu - oracle| <= 1e-4 * max |oracle|
-(the north-star bound of 1e-4 relative), measured against the largest value of that
+(1e-4 relative, the parity bound of this path), measured against the largest value of that
 subgame's vector so that entries that cancel to ~0 do not turn rounding into a false
 failure.
 """
