@@ -98,30 +98,38 @@ def leaf_ranges(game, n, rng, per_draw=64):
     return np.array(ids), np.stack(out)
 
 
+def river_specs(boards, ranges, pots, stacks):
+    """The 48 river subgames of each turn-leaf state, in card order: specs [n * 48] and
+    ranges [n * 48][2][1326] (the state's ranges with the river card's hands zeroed)."""
+    m = len(boards)
+    order = P.card_order()
+    holds = ((order[None, :] >> np.arange(52, dtype=np.uint64)[:, None]) & np.uint64(1)) != 0  # [card][hand]
+    b4 = np.asarray(boards, np.uint64)
+    off = ((b4[:, None] >> np.arange(52, dtype=np.uint64)[None, :]) & np.uint64(1)) == 0
+    river = np.nonzero(off)[1].reshape(m, 48)
+    specs = np.zeros(m * 48, P.SPEC_DTYPE)
+    specs["board"] = (b4[:, None] | (np.uint64(1) << river.astype(np.uint64))).ravel()
+    specs["pot"] = np.repeat(np.asarray(pots, np.float32), 48)
+    specs["stack"] = np.repeat(np.asarray(stacks, np.float32), 48)
+    specs["sizes"] = D.RIVER_SIZES
+    specs["max_raises"] = D.RIVER_RAISES
+    rr = np.repeat(np.asarray(ranges, np.float32), 48, axis=0)
+    rr *= ~holds[river.ravel()][:, None, :]
+    return specs, rr
+
+
 def river_values(boards, ranges, pots, stacks, iterations, chunk=1024):
     """Leaf values [n][2][1326] (pot-normalised, mean over the 48 rivers) of the states, by
     the batched solver in batches of `chunk` states (48 subgames each), the launch
     configuration tuned on the first batch and reused; and the seconds spent."""
     n = len(boards)
-    order = P.card_order()
-    holds = ((order[None, :] >> np.arange(52, dtype=np.uint64)[:, None]) & np.uint64(1)) != 0  # [card][hand]
     values = np.zeros((n, 2, P.HANDS), np.float32)
     cfg = None
     t0 = time.perf_counter()
     for s0 in range(0, n, chunk):
         s1 = min(n, s0 + chunk)
         m = s1 - s0
-        b4 = np.asarray(boards[s0:s1], np.uint64)
-        off = ((b4[:, None] >> np.arange(52, dtype=np.uint64)[None, :]) & np.uint64(1)) == 0
-        river = np.nonzero(off)[1].reshape(m, 48)  # the 48 river cards of each state, in card order
-        specs = np.zeros(m * 48, P.SPEC_DTYPE)
-        specs["board"] = (b4[:, None] | (np.uint64(1) << river.astype(np.uint64))).ravel()
-        specs["pot"] = np.repeat(np.asarray(pots[s0:s1], np.float32), 48)
-        specs["stack"] = np.repeat(np.asarray(stacks[s0:s1], np.float32), 48)
-        specs["sizes"] = D.RIVER_SIZES
-        specs["max_raises"] = D.RIVER_RAISES
-        rr = np.repeat(np.asarray(ranges[s0:s1], np.float32), 48, axis=0)
-        rr *= ~holds[river.ravel()][:, None, :]  # hands holding the river card
+        specs, rr = river_specs(boards[s0:s1], ranges[s0:s1], pots[s0:s1], stacks[s0:s1])
         b = P.Batch(specs, rr)
         b.enable_average()
         b.set_linear_average(True)

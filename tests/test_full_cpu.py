@@ -91,3 +91,27 @@ def test_oracle_sweeps_zero_sum_and_best_response():
         Vb, _, _ = F.sweep_up(tree, R, lv, upd, reg, False, "br")
         assert init[upd] @ Vb[0] >= vals[-1] - 1e-12
     assert abs(vals[0] + vals[1]) < 1e-9 * max(1.0, abs(vals[0]))
+
+
+def test_river_specs_of_leaf_states():
+    """The 48 river subgames of a turn-leaf state: one per card off the 4-card board, in card
+    order, with the leaf's pot and stack and the river card's hands removed from the ranges."""
+    from pokerrust_b200 import full_solve as FS
+    rng = np.random.default_rng(4)
+    boards = np.array([sum(1 << int(c) for c in rng.choice(52, 4, replace=False)) for _ in range(3)], np.uint64)
+    ranges = rng.random((3, 2, F.HANDS)).astype(np.float32)
+    pots = np.array([10.0, 25.0, 62.5], np.float32)
+    stacks = np.array([100.0, 92.5, 0.0], np.float32)
+    specs, rr = FS.river_specs(boards, ranges, pots, stacks)
+    assert len(specs) == 3 * 48 and rr.shape == (3 * 48, 2, F.HANDS)
+    k = 0
+    for i in range(3):
+        for c in range(52):
+            if (int(boards[i]) >> c) & 1:
+                continue
+            assert int(specs["board"][k]) == int(boards[i]) | (1 << c)
+            assert specs["pot"][k] == pots[i] and specs["stack"][k] == stacks[i]
+            want = ranges[i].copy()
+            want[:, F.blocked(1 << c)] = 0.0
+            assert np.array_equal(rr[k], want)
+            k += 1
