@@ -127,9 +127,10 @@ struct Batch {
             a.own_reach = own_weight;
             a.avg_weight = avg_weight;
             const int ctas = std::min(k.count, std::max(1, k.per_sm) * sms);
-            const int group = batch_group_leaves(fp64);
+            const int dense = mode == kBModeCFR && !fp64 && k.K == 4 && k.per_sm >= 3;
+            const int group = dense ? batch_dense_group() : batch_group_leaves(fp64);
             cudaError_t e = launch_batch_pass(mode, k.K, fp64, mode == kBModeCFR && avg_on, a, ctas, group,
-                                              on ? on : stream);
+                                              on ? on : stream, dense);
             if (e != cudaSuccess) return bfail("pass launch", e);
         }
         return 0;
@@ -614,7 +615,9 @@ int pr_batch_iterate_noalloc(void *batch, int iterations) {
                 a.count = k.count;
                 a.player = pl;
                 const int ctas = std::min(k.count, std::max(1, k.per_sm) * b->sms);
-                e = launch_batch_pass(kBModeCFR, k.K, 0, b->avg_on, a, ctas, batch_group_leaves(0), b->stream);
+                const int dense = k.K == 4 && k.per_sm >= 3;
+                e = launch_batch_pass(kBModeCFR, k.K, 0, b->avg_on, a, ctas,
+                                      dense ? batch_dense_group() : batch_group_leaves(0), b->stream, dense);
                 if (e != cudaSuccess) return bfail("pass launch", e);
             }
         }
@@ -769,7 +772,7 @@ int pr_batch_set_config(void *batch, int c, int K, int per_sm, int order) {
     if (!b || c < 0 || c >= kClasses || (K != 2 && K != 3 && K != 4) || per_sm < 1 || per_sm > 4 ||
         (order != 0 && order != 1))
         return 2;
-    const int fits = batch_ctas_per_sm(kBModeCFR, K, 0, b->avg_on);
+    const int fits = K == 4 && per_sm >= 3 ? batch_dense_ctas_per_sm(b->avg_on) : batch_ctas_per_sm(kBModeCFR, K, 0, b->avg_on);
     if (per_sm > fits) return 2;
     b->cls[c].K = K;
     b->cls[c].per_sm = per_sm;
@@ -815,7 +818,9 @@ int pr_batch_tune(void *batch, double *ms_out) {
         ClassCfg best_cfg = keep[c];
         for (int K : {2, 3, 4}) {
             const int fits = batch_ctas_per_sm(kBModeCFR, K, 0, b->avg_on);
-            for (int per = 1; per <= std::min(fits, 2); per++) {
+            // K = 4 also tries the dense configuration: registers capped for 3 CTAs per SM
+            const int top = K == 4 && batch_dense_ctas_per_sm(b->avg_on) >= 3 ? 3 : std::min(fits, 2);
+            for (int per = 1; per <= top; per++) {
                 for (int ord = 0; ord < 2; ord++) {
                     b->cls[c].K = K;
                     b->cls[c].per_sm = per;

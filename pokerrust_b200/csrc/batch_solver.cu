@@ -321,8 +321,10 @@ __device__ __forceinline__ V sigma(V val, V scale) {
     return scale < V(0) ? -scale : mul(val > V(0) ? val : V(0), scale);
 }
 
-template <int K, typename V, int MODE, bool AVG, bool USEAVG>
-__global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch a, int group) {
+// MINB: CTAs per SM the registers are capped for (Cfg<K>::MINB, or 3 for the dense K = 4
+// configuration with 10-leaf groups).
+template <int K, typename V, int MODE, bool AVG, bool USEAVG, int MINB>
+__global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int group) {
     constexpr int NT = Cfg<K>::NT;
     constexpr int NW = NT / 32;
     static_assert(MODE == kBModeCFR || !AVG, "average sums accumulate in CFR passes");
@@ -705,20 +707,26 @@ __global__ void __launch_bounds__(Cfg<K>::NT, Cfg<K>::MINB) batch_kernel(BLaunch
 
 __global__ void weight_step_kernel(float *w) { *w += 1.0f; }
 
-template <int K, typename V, int MODE, bool AVG, bool USEAVG>
+template <int K, typename V, int MODE, bool AVG, bool USEAVG, int MINB = Cfg<K>::MINB>
 cudaError_t launch_one(const BLaunch &a, int ctas, int group, cudaStream_t stream) {
     const size_t smem = smem_bytes<V>(group);
-    cudaError_t e = cudaFuncSetAttribute(batch_kernel<K, V, MODE, AVG, USEAVG>,
+    cudaError_t e = cudaFuncSetAttribute(batch_kernel<K, V, MODE, AVG, USEAVG, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    batch_kernel<K, V, MODE, AVG, USEAVG><<<ctas, Cfg<K>::NT, smem, stream>>>(a, group);
+    batch_kernel<K, V, MODE, AVG, USEAVG, MINB><<<ctas, Cfg<K>::NT, smem, stream>>>(a, group);
     return cudaGetLastError();
 }
 
 template <int K>
-cudaError_t launch_k(int mode, int fp64, int avg, const BLaunch &a, int ctas, int group, cudaStream_t st) {
+cudaError_t launch_k(int mode, int fp64, int avg, const BLaunch &a, int ctas, int group, cudaStream_t st,
+                     int dense) {
     if (mode == kBModeCFR) {
         if (fp64) return cudaErrorInvalidValue;
+        if constexpr (K == 4) {
+            if (dense)
+                return avg ? launch_one<4, float, kBModeCFR, true, false, 3>(a, ctas, group, st)
+                           : launch_one<4, float, kBModeCFR, false, false, 3>(a, ctas, group, st);
+        }
         return avg ? launch_one<K, float, kBModeCFR, true, false>(a, ctas, group, st)
                    : launch_one<K, float, kBModeCFR, false, false>(a, ctas, group, st);
     }
@@ -749,6 +757,8 @@ int batch_threads(int K) { return K == 2 ? Cfg<2>::NT : (K == 3 ? Cfg<3>::NT : C
 
 int batch_group_leaves(int fp64) { return fp64 ? 8 : 16; }
 
+int batch_dense_group() { return 10; }
+
 size_t batch_smem_bytes(int K, int fp64, int group) {
     (void)K;
     return fp64 ? smem_bytes<double>(group) : smem_bytes<float>(group);
@@ -760,14 +770,32 @@ cudaError_t launch_weight_step(float *w, cudaStream_t stream) {
 }
 
 cudaError_t launch_batch_pass(int mode, int K, int fp64, int avg, const BLaunch &a, int ctas, int group,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, int dense) {
     if (group < 1 || group > kBMaxLeaves || ctas < 1) return cudaErrorInvalidValue;
     switch (K) {
-        case 2: return launch_k<2>(mode, fp64, avg, a, ctas, group, stream);
-        case 3: return launch_k<3>(mode, fp64, avg, a, ctas, group, stream);
-        case 4: return launch_k<4>(mode, fp64, avg, a, ctas, group, stream);
+        case 2: return launch_k<2>(mode, fp64, avg, a, ctas, group, stream, 0);
+        case 3: return launch_k<3>(mode, fp64, avg, a, ctas, group, stream, 0);
+        case 4: return launch_k<4>(mode, fp64, avg, a, ctas, group, stream, dense);
         default: return cudaErrorInvalidValue;
     }
+}
+
+int batch_dense_ctas_per_sm(int avg) {
+    int n = 0;
+    const size_t smem = smem_bytes<float>(batch_dense_group());
+    cudaError_t e;
+    if (avg) {
+        cudaFuncSetAttribute(batch_kernel<4, float, kBModeCFR, true, false, 3>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<4, float, kBModeCFR, true, false, 3>,
+                                                          Cfg<4>::NT, smem);
+    } else {
+        cudaFuncSetAttribute(batch_kernel<4, float, kBModeCFR, false, false, 3>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<4, float, kBModeCFR, false, false, 3>,
+                                                          Cfg<4>::NT, smem);
+    }
+    return e == cudaSuccess ? n : 0;
 }
 
 int batch_ctas_per_sm(int mode, int K, int fp64, int avg) {
@@ -777,9 +805,9 @@ int batch_ctas_per_sm(int mode, int K, int fp64, int avg) {
     cudaError_t e = cudaSuccess;
 #define PRB_OCC(KK, VV, MM, AA, UU)                                                                   \
     do {                                                                                              \
-        cudaFuncSetAttribute(batch_kernel<KK, VV, MM, AA, UU>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                             (int)smem);                                                              \
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<KK, VV, MM, AA, UU>,         \
+        cudaFuncSetAttribute(batch_kernel<KK, VV, MM, AA, UU, Cfg<KK>::MINB>,                           \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                 \
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<KK, VV, MM, AA, UU, Cfg<KK>::MINB>, \
                                                           Cfg<KK>::NT, smem);                         \
     } while (0)
     if (mode == kBModeCFR) {

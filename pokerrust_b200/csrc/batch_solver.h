@@ -68,8 +68,10 @@ cudaError_t launch_batch_setup(const BSub *subs, int count, BPack *packs, const 
 
 // One pass over the queue. K = hands per thread (2, 3 or 4); fp64 selects double
 // arithmetic (best response and evaluation only). ctas = grid size (persistent CTAs).
+// dense (K = 4 CFR passes in single precision only): the configuration with registers capped
+// for 3 CTAs per SM; it expects groups of batch_dense_group() leaves.
 cudaError_t launch_batch_pass(int mode, int K, int fp64, int avg, const BLaunch &a, int ctas, int max_leaves,
-                              cudaStream_t stream);
+                              cudaStream_t stream, int dense = 0);
 
 // Adds 1 to the device scalar *w (the next iteration's average weight), on `stream`.
 cudaError_t launch_weight_step(float *w, cudaStream_t stream);
@@ -78,7 +80,11 @@ cudaError_t launch_weight_step(float *w, cudaStream_t stream);
 int batch_threads(int K);
 size_t batch_smem_bytes(int K, int fp64, int group_leaves);
 int batch_group_leaves(int fp64);
+// Leaf group of the dense K = 4 configuration (3 CTAs per SM fit in shared memory).
+int batch_dense_group();
 // Resident CTAs per SM the configuration allows (0 if it cannot launch).
 int batch_ctas_per_sm(int mode, int K, int fp64, int avg);
+// The same for the dense K = 4 CFR configuration.
+int batch_dense_ctas_per_sm(int avg);
 
 }  // namespace prb

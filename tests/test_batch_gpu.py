@@ -110,11 +110,12 @@ def test_launch_configurations_are_bit_identical():
     bs, br = _big_tree_specs(P, 40, seed=6)
     specs, ranges = np.concatenate([specs, bs]), np.concatenate([ranges, br])
     results = []
-    for K, order in [(2, 0), (3, 1), (4, 0), (2, 1)]:
+    # the last configuration is the dense one: registers capped for 3 CTAs per SM, 10-leaf groups
+    for K, per_sm, order in [(2, 1, 0), (3, 1, 1), (4, 1, 0), (2, 1, 1), (4, 3, 0)]:
         b = P.Batch(specs, ranges)
         b.enable_average()
         for c in range(2):
-            b.set_config(c, K, 1, order)
+            b.set_config(c, K, per_sm, order)
         b.iterate(3)
         results.append([b.regrets(s) for s in (0, 17, 299, 320, 339)] +
                        [b.average(s) for s in (5, 330)])
