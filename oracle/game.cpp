@@ -32,6 +32,7 @@ struct GNode {
     std::vector<std::unique_ptr<GNode>> next;
     std::vector<std::array<int, 4>> perms;
     std::vector<std::vector<float>> regrets;  // RegularStrategy, one 1326 vector per action
+    std::vector<std::vector<float>> avg;      // average-strategy sums, same shape (not in the reference)
     int river = -1;                            // index of the river root (River nodes)
 };
 
@@ -44,6 +45,12 @@ struct Game {
     std::vector<uint64_t> river_board;
     std::vector<float> river_bet;
     std::vector<float> river_regrets;  // [rivers][26][256]
+    // Average-strategy sums (not in the reference, which keeps none): at the updater's
+    // decision nodes, its reach into the node times the action probability, per hand above
+    // the river and per bucket in the river subgames ([rivers][26][256]), both in f32.
+    bool avg_on = false;
+    std::vector<float> river_avg;
+    std::vector<float> root_values[2];  // the root's values of the last CFR pass per updater
 
     static int popc(uint64_t x) { return __builtin_popcountll(x); }
 
@@ -235,7 +242,22 @@ struct Game {
     }
 
     template <typename T>
-    std::vector<T> river(GNode &s, const std::vector<T> &opp, int upd, bool exploit);
+    std::vector<T> river(GNode &s, const std::vector<T> &opp, const std::vector<T> &own, int upd,
+                         bool exploit);
+
+    void enable_average(GNode &s) {
+        if (s.terminal == NonTerminal) s.avg.assign(s.regrets.size(), std::vector<float>(OR_HANDS, 0.0f));
+        for (auto &n : s.next) enable_average(*n);
+    }
+
+    // sum of all upper-tree average sums (regrets with which = 0)
+    double upper_total(const GNode &s, int which) const {
+        double t = 0;
+        for (const auto &v : which ? s.avg : s.regrets)
+            for (float x : v) t += x;
+        for (const auto &n : s.next) t += upper_total(*n, which);
+        return t;
+    }
 
     // state.rs:219-376
     template <typename T>
@@ -270,6 +292,11 @@ struct Game {
                     } else {
                         for (int i = 0; i < OR_HANDS; i++) avg[i] += u[i];
                     }
+                }
+                if (s.actor == upd && !exploit && avg_on) {
+                    const std::vector<T> &own = s.actor == Small ? sb : bb;
+                    for (size_t k = 0; k < s.next.size(); k++)
+                        for (int i = 0; i < OR_HANDS; i++) s.avg[k][i] += float(own[i] * strat[k][i]);
                 }
                 if (s.actor == upd && !exploit) {
                     // RegularStrategy::update_add (strategy.rs:57-66)
@@ -322,25 +349,29 @@ struct Game {
                 for (auto &x : total) x *= scale;
                 return total;
             }
-            case RiverT: return river<T>(s, opp, upd, exploit);
+            case RiverT: return river<T>(s, opp, upd == Small ? sb : bb, upd, exploit);
             default: return std::vector<T>(OR_HANDS, T(0));
         }
     }
 };
 
 template <>
-std::vector<float> Game::river<float>(GNode &s, const std::vector<float> &opp, int upd,
-                                      bool exploit) {
+std::vector<float> Game::river<float>(GNode &s, const std::vector<float> &opp,
+                                      const std::vector<float> &own, int upd, bool exploit) {
     std::vector<float> out(OR_HANDS);
-    or_river_one_f32(flop, eval.data(), abstr.data(), s.cards, s.sbbet, opp.data(),
-                     river_regrets.data() + (size_t)s.river * OR_RIVER_EDGES * OR_BUCKETS, upd,
-                     exploit, out.data());
+    const size_t off = (size_t)s.river * OR_RIVER_EDGES * OR_BUCKETS;
+    if (avg_on && !exploit)
+        or_river_one_f32_avg(flop, eval.data(), abstr.data(), s.cards, s.sbbet, opp.data(), own.data(),
+                             river_regrets.data() + off, river_avg.data() + off, upd, out.data());
+    else
+        or_river_one_f32(flop, eval.data(), abstr.data(), s.cards, s.sbbet, opp.data(),
+                         river_regrets.data() + off, upd, exploit, out.data());
     return out;
 }
 
 template <>
-std::vector<double> Game::river<double>(GNode &s, const std::vector<double> &opp, int upd,
-                                        bool exploit) {
+std::vector<double> Game::river<double>(GNode &s, const std::vector<double> &opp,
+                                        const std::vector<double> &, int upd, bool exploit) {
     std::vector<double> out(OR_HANDS);
     or_river_one_f64(flop, eval.data(), abstr.data(), s.cards, s.sbbet, opp.data(),
                      river_regrets.data() + (size_t)s.river * OR_RIVER_EDGES * OR_BUCKETS, upd,
@@ -365,8 +396,43 @@ extern "C" void or_game_river_roots(void *g, uint64_t *board4, float *bet) {
 extern "C" void or_game_iterate(void *g) {
     Game *G = (Game *)g;
     std::vector<float> ones(OR_HANDS, 1.0f);
-    G->eval_state<float>(*G->root, ones, ones, Small, false);
-    G->eval_state<float>(*G->root, ones, ones, Big, false);
+    G->root_values[0] = G->eval_state<float>(*G->root, ones, ones, Small, false);
+    G->root_values[1] = G->eval_state<float>(*G->root, ones, ones, Big, false);
+}
+
+extern "C" void or_game_enable_average(void *g) {
+    Game *G = (Game *)g;
+    if (G->avg_on) return;
+    G->enable_average(*G->root);
+    G->river_avg.assign(G->river_regrets.size(), 0.0f);
+    G->avg_on = true;
+}
+
+extern "C" int or_game_root_values(void *g, float *sb, float *bb) {
+    Game *G = (Game *)g;
+    if (G->root_values[0].size() != OR_HANDS) return 2;
+    std::memcpy(sb, G->root_values[0].data(), sizeof(float) * OR_HANDS);
+    std::memcpy(bb, G->root_values[1].data(), sizeof(float) * OR_HANDS);
+    return 0;
+}
+
+extern "C" void or_game_totals(void *g, double *upper_regrets, double *upper_avg, double *river_regrets,
+                               double *river_avg) {
+    Game *G = (Game *)g;
+    *upper_regrets = G->upper_total(*G->root, 0);
+    *upper_avg = G->avg_on ? G->upper_total(*G->root, 1) : 0.0;
+    double r = 0, a = 0;
+    for (float x : G->river_regrets) r += x;
+    for (float x : G->river_avg) a += x;
+    *river_regrets = r;
+    *river_avg = a;
+}
+
+extern "C" int or_game_river_average(void *g, float *out) {
+    Game *G = (Game *)g;
+    if (!G->avg_on) return 2;
+    std::memcpy(out, G->river_avg.data(), G->river_avg.size() * sizeof(float));
+    return 0;
 }
 
 extern "C" void or_game_exploitability(void *g, int use_f64, double *sum_sb, double *sum_bb,

@@ -113,6 +113,17 @@ void or_game_exploitability(void *game, int use_f64, double *sum_sb, double *sum
                             double *mbh);
 /* Copies of the river regrets (27783*26*256 for the reference flop) in river-root order. */
 void or_game_river_regrets(void *game, float *out);
+/* Average-strategy sums (not in the reference): the updater's reach into each of its
+ * decisions times the action probability, per hand above the river and per bucket in the
+ * river subgames. Enable before iterating. */
+void or_game_enable_average(void *game);
+/* The root's values of the last iteration's SB and BB CFR passes (2 on no iteration yet). */
+int or_game_root_values(void *game, float *sb, float *bb);
+/* Sums over all upper-tree regrets / average sums and all river regrets / average sums. */
+void or_game_totals(void *game, double *upper_regrets, double *upper_avg, double *river_regrets,
+                    double *river_avg);
+/* River average sums [rivers][26][256] (2 if averages are off). */
+int or_game_river_average(void *game, float *out);
 
 #ifdef __cplusplus
 }

@@ -24,15 +24,26 @@ _lib = None
 
 
 REF_SO = os.path.join(HERE, "_ref", "libpoker_ref.so")
-REFERENCE_TREE = "/root/reference"
+
+
+def reference_tree():
+    """The reference checkout whose src/cuda the `ref` recipe compiles: the environment
+    variable POKERRUST_REFERENCE, else the default the Makefile names; None if absent."""
+    tree = os.environ.get("POKERRUST_REFERENCE")
+    if not tree:
+        out = subprocess.run(["make", "-s", "-C", HERE, "--no-print-directory", "print-reference"],
+                             capture_output=True, text=True)
+        tree = out.stdout.strip() if out.returncode == 0 else ""
+    return tree if tree and os.path.isdir(os.path.join(tree, "src", "cuda")) else None
 
 
 def build():
     """Compiles the oracle with its Makefile (g++) and, where the reference sources are
     present, the reference's own CUDA library into oracle/_ref (nvcc)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if os.path.isdir(os.path.join(REFERENCE_TREE, "src", "cuda")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={REFERENCE_TREE}"], check=True)
+    tree = reference_tree()
+    if tree:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={tree}"], check=True)
     return SO_PATH
 
 
@@ -72,6 +83,12 @@ def load():
         L.or_game_iterate.argtypes = [vp]
         L.or_game_exploitability.argtypes = [vp, i32, vp, vp, vp]
         L.or_game_river_regrets.argtypes = [vp, vp]
+        L.or_game_enable_average.argtypes = [vp]
+        L.or_game_root_values.restype = i32
+        L.or_game_root_values.argtypes = [vp, vp, vp]
+        L.or_game_totals.argtypes = [vp, vp, vp, vp, vp]
+        L.or_game_river_average.restype = i32
+        L.or_game_river_average.argtypes = [vp, vp]
         L.or_bet_tree.restype = i32
         L.or_bet_tree.argtypes = [f32, f32, ctypes.c_uint32, i32] + [vp] * 7 + [i32, vp, vp, vp]
         L.or_sub_new.restype = vp
@@ -223,6 +240,28 @@ class Game:
     def river_regrets(self):
         out = np.zeros((self.num_rivers, EDGES, BUCKETS), np.float32)
         load().or_game_river_regrets(self.ptr, _p(out))
+        return out
+
+    def enable_average(self):
+        load().or_game_enable_average(self.ptr)
+
+    def root_values(self):
+        """The root's values of the last iteration's SB and BB CFR passes, [2][1326] f32."""
+        out = np.zeros((2, HANDS), np.float32)
+        if load().or_game_root_values(self.ptr, _p(out[0]), _p(out[1])):
+            raise ValueError("no iteration yet")
+        return out
+
+    def totals(self):
+        """Sums of all upper regrets, upper average sums, river regrets, river average sums."""
+        v = [ctypes.c_double() for _ in range(4)]
+        load().or_game_totals(self.ptr, *[ctypes.byref(x) for x in v])
+        return np.array([x.value for x in v])
+
+    def river_average(self):
+        out = np.zeros((self.num_rivers, EDGES, BUCKETS), np.float32)
+        if load().or_game_river_average(self.ptr, _p(out)):
+            raise ValueError("average sums are off")
         return out
 
     def __del__(self):

@@ -25,6 +25,10 @@ void or_parallel_for(int n, int nthreads, const std::function<void(int)> &f);
 int or_river_one_f32(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, uint64_t board4,
                      float bet, const float *opp, float *regrets, int player, bool exploit,
                      float *out);
+// The same CFR pass that also adds the updater's average-strategy sums (own = its range).
+int or_river_one_f32_avg(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, uint64_t board4,
+                         float bet, const float *opp, const float *own, float *regrets, float *avg,
+                         int player, float *out);
 int or_river_one_f64(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, uint64_t board4,
                      float bet, const double *opp, const float *regrets, int player, double *out);
 

@@ -362,6 +362,13 @@ int or_river_one_f32(uint64_t flop, const uint16_t *eval, const uint16_t *abstr,
                             out);
 }
 
+int or_river_one_f32_avg(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, uint64_t board4,
+                         float bet, const float *opp, const float *own, float *regrets, float *avg,
+                         int player, float *out) {
+    return river_one<float>(flop, eval, abstr, board4, bet, opp, regrets, nullptr, player, false, out,
+                            own, avg);
+}
+
 int or_river_one_f64(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, uint64_t board4,
                      float bet, const double *opp, const float *regrets, int player, double *out) {
     return river_one<double>(flop, eval, abstr, board4, bet, opp, nullptr, regrets, player, true,
