@@ -34,7 +34,9 @@ void *init_builder(void);
 
 /* Replaces upload_c (interface.cu:87-89, cuda_interface.rs:11): copies 1326 floats (the
  * opponent range at river root `index`) into the builder's pinned staging. Safe to call
- * from many threads at once for distinct indexes, as state.rs:340-341,380-387 does. */
+ * from many threads at once for distinct indexes, as state.rs:340-341,380-387 does. A range
+ * holding a NaN, an infinity or a negative weight is not copied and sets the sticky status
+ * (pr_last_error() == 2); the reference copies it unchecked. */
 void upload_c(void *builder, int index, const float *v);
 
 /* Replaces download_c (interface.cu:91-93, cuda_interface.rs:12): copies the 1326 result
@@ -81,7 +83,8 @@ int pr_evaluate_device(void *builder, void *eval, int updating_player, int calc_
                        const float *d_ranges, float *d_results, void *stream);
 
 /* Batch forms of upload_c / download_c for rows first .. first+count-1; v holds count
- * rows of 1326 floats (the same copies the reference's caller makes one call at a time). */
+ * rows of 1326 floats (the same copies the reference's caller makes one call at a time).
+ * pr_upload_batch skips rows upload_c would refuse and then returns 2. */
 int pr_upload_batch(void *builder, int first, int count, const float *v);
 int pr_download_batch(void *builder, int first, int count, float *v);
 
@@ -162,6 +165,10 @@ void *pr_game_builder(void *game);
 void *pr_game_tables(void *game);
 /* CFR iterations (game.rs:68-119): small blind update, then big blind update. */
 int pr_game_iterate(void *game, int iterations);
+/* The root's counterfactual values (per colex hand, 1326 floats each) of the last
+ * iteration's small-blind and big-blind CFR passes: the vectors eval_state returns at the
+ * root in game.rs:68-119. 2 before the first iteration. */
+int pr_game_root_values(void *game, float *sb, float *bb);
 /* Where the preflop/flop/turn tree is traversed: 1 (default) on the device, level by level,
  * with each iteration replayed as one CUDA graph; 0 on the host through upload_c /
  * evaluate_cuda / download_c, the reference's protocol (game.rs:68-119). Both give the
@@ -204,7 +211,8 @@ typedef struct {
 /* Builds one subgame's tree on the host (16-byte nodes in pre-order; nodes_out may be null,
  * else room for 128 nodes). 0 on success, 2 if the spec is invalid. */
 int pr_batch_tree(const pr_subgame *spec, void *nodes_out, int *num_nodes, int *num_edges, int *num_leaves);
-/* ranges: [count][2][1326] floats (player 0, player 1). Null on failure. */
+/* ranges: [count][2][1326] floats (player 0, player 1), finite and non-negative. Null on
+ * failure (a bad board or tree, a NaN, infinite or negative weight, an allocation). */
 void *pr_batch_new(const pr_subgame *specs, int count, const float *ranges);
 void pr_batch_free(void *batch);
 int pr_batch_count(void *batch);
@@ -226,7 +234,8 @@ int pr_batch_set_linear_average(void *batch, int on);
  * pass; the order is rewritten on every call. The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress): make that first call before any stream
  * capture. All calls share the one array, so calls that overlap on the GPU race: issue them
- * one after another. */
+ * one after another. It runs the same iteration as pr_batch_iterate (launch configuration,
+ * linear averaging and average weights included), so both give the same results. */
 int pr_batch_iterate_noalloc(void *batch, int iterations);
 /* Per subgame: best-response sums of each player (range-weighted root values) and the
  * exploitability (br0 + br1) / 2 per unit of joint range mass, in chips; against the
@@ -253,6 +262,9 @@ int pr_batch_get_regrets(void *batch, int s, float *out);
 int pr_batch_set_regrets(void *batch, int s, const float *in);
 int pr_batch_get_average(void *batch, int s, float *out);
 int pr_batch_set_average(void *batch, int s, const float *in);
+/* Every subgame's regrets (which 0) or average sums (which 1) in one call: out[sum of the
+ * subgames' edge counts][1326] floats, subgames in batch order, edges in tree order. */
+int pr_batch_get_all(void *batch, int which, float *out);
 /* Launch configuration per tree-shape class (0: up to 16 leaves, 1: more): hands per
  * thread (2, 3, 4), resident CTAs per SM, queue order (0 most work first, 1 input order). */
 int pr_batch_config(void *batch, int c, int *K, int *per_sm, int *order, int *count);

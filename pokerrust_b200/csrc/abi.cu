@@ -468,6 +468,14 @@ void upload_c(void *builder, int index, const float *v) {
         fail(kErrArg, "upload_c: bad builder or index");
         return;
     }
+    // a range is a vector of finite, non-negative weights: refuse anything else (the slot
+    // keeps its previous contents); v - v is NaN exactly for NaN and infinities
+    float bad = 0.0f;
+    for (int i = 0; i < kHands; i++) bad += (v[i] - v[i]) + (v[i] < 0.0f ? 1.0f : 0.0f);
+    if (bad != 0.0f) {
+        fail(kErrArg, "upload_c: a range holds a NaN, an infinity or a negative weight");
+        return;
+    }
     memcpy(b->comm + (size_t)index * kRangeStride, v, kHands * sizeof(float));
 }
 
@@ -595,19 +603,34 @@ int pr_evaluate_device_own(void *builder, void *eval, int updating_player, const
 namespace {
 // Row copies between caller rows of 1326 and staging rows of kRangeStride, split over host
 // threads for large batches (one thread copies ~25 MB/s per row call otherwise idle cores).
-void copy_rows(float *dst, size_t dst_stride, const float *src, size_t src_stride, int count) {
+// With `checked`, rows that hold a NaN, an infinity or a negative weight are not copied; the
+// return value counts them.
+int copy_rows(float *dst, size_t dst_stride, const float *src, size_t src_stride, int count, bool checked = false) {
+    std::atomic<int> rejected{0};
     auto part = [&](int lo, int hi) {
-        for (int i = lo; i < hi; i++) memcpy(dst + (size_t)i * dst_stride, src + (size_t)i * src_stride, kHands * sizeof(float));
+        for (int i = lo; i < hi; i++) {
+            const float *row = src + (size_t)i * src_stride;
+            if (checked) {
+                float bad = 0.0f;
+                for (int h = 0; h < kHands; h++) bad += (row[h] - row[h]) + (row[h] < 0.0f ? 1.0f : 0.0f);
+                if (bad != 0.0f) {
+                    rejected++;
+                    continue;
+                }
+            }
+            memcpy(dst + (size_t)i * dst_stride, row, kHands * sizeof(float));
+        }
     };
     const int threads = count >= 4096 ? (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency())) : 1;
     if (threads <= 1) {
         part(0, count);
-        return;
+        return rejected.load();
     }
     std::vector<std::thread> pool;
     for (int t = 0; t < threads; t++)
         pool.emplace_back(part, (int)((long long)count * t / threads), (int)((long long)count * (t + 1) / threads));
     for (auto &th : pool) th.join();
+    return rejected.load();
 }
 }  // namespace
 
@@ -615,7 +638,8 @@ int pr_upload_batch(void *builder, int first, int count, const float *v) {
     Builder *b = (Builder *)builder;
     if (!b || !v || first < 0 || count < 0 || first + count > (int)b->desc.size())
         return fail(kErrArg, "pr_upload_batch: bad builder or range");
-    copy_rows(b->comm + (size_t)first * kRangeStride, kRangeStride, v, kHands, count);
+    if (copy_rows(b->comm + (size_t)first * kRangeStride, kRangeStride, v, kHands, count, true))
+        return fail(kErrArg, "pr_upload_batch: a range holds a NaN, an infinity or a negative weight (row not copied)");
     return kOk;
 }
 

@@ -19,6 +19,13 @@
 namespace prb {
 namespace {
 
+// True when every weight of n is finite and non-negative (v - v is NaN for NaN and infinities).
+bool valid_weights(const float *r, size_t n) {
+    float bad = 0.0f;
+    for (size_t i = 0; i < n; i++) bad += (r[i] - r[i]) + (r[i] < 0.0f ? 1.0f : 0.0f);
+    return bad == 0.0f;
+}
+
 int bfail(const char *what, cudaError_t e = cudaSuccess) {
     if (e != cudaSuccess) fprintf(stderr, "pokerrust_b200: batch: %s: %s\n", what, cudaGetErrorString(e));
     else fprintf(stderr, "pokerrust_b200: batch: %s\n", what);
@@ -102,9 +109,11 @@ struct Batch {
         return e == cudaSuccess ? 0 : bfail("queue upload", e);
     }
 
-    // one pass of `mode` for `player` over every class; heads [slot*kClasses + c] must be zero
+    // one pass of `mode` for `player` over every class; heads [slot*kClasses + c] must be zero.
+    // `queue` / `heads` replace the batch's own work-queue order and heads when given.
     int pass(int mode, int player, int fp64, int use_average, void *root_out, void *sum_out, int slot,
-             void *child_out = nullptr, cudaStream_t on = nullptr) {
+             void *child_out = nullptr, cudaStream_t on = nullptr, const int *queue = nullptr,
+             int *heads = nullptr) {
         for (int c = 0; c < kClasses; c++) {
             const ClassCfg &k = cls[c];
             if (!k.count) continue;
@@ -115,8 +124,8 @@ struct Batch {
             a.ranges = d_ranges;
             a.regrets = d_regrets;
             a.avg = (avg_on || use_average) ? d_avg : nullptr;
-            a.order = d_order + k.first;
-            a.head = d_head + slot * kClasses + c;
+            a.order = (queue ? queue : d_order) + k.first;
+            a.head = (heads ? heads : d_head) + slot * kClasses + c;
             a.count = k.count;
             a.player = player;
             a.use_average = use_average;
@@ -136,11 +145,13 @@ struct Batch {
         return 0;
     }
 
-    int iteration() {
-        cudaError_t e = cudaMemsetAsync(d_head, 0, sizeof(int) * 4 * kClasses, stream);
+    // One CFR iteration (both players, then the linear-average weight step). `queue` / `heads`
+    // (2 * kClasses ints) replace the batch's own work queue when given.
+    int iteration(const int *queue = nullptr, int *heads = nullptr) {
+        cudaError_t e = cudaMemsetAsync(heads ? heads : d_head, 0, sizeof(int) * 2 * kClasses, stream);
         if (e != cudaSuccess) return bfail("queue reset", e);
         for (int pl = 0; pl < 2; pl++)
-            if (int st = pass(kBModeCFR, pl, 0, 0, nullptr, nullptr, pl)) return st;
+            if (int st = pass(kBModeCFR, pl, 0, 0, nullptr, nullptr, pl, nullptr, nullptr, queue, heads)) return st;
         if (linear) {
             e = launch_weight_step(d_wt, stream);
             if (e != cudaSuccess) return bfail("weight update", e);
@@ -167,6 +178,24 @@ __global__ void to_hands_kernel(const double *__restrict__ src, const BPack *__r
             if (w) v = (double)w[p] * v;
         }
         out[h] = sign * v;
+    }
+}
+
+// Rows [edge][kBRow] (position order) of subgames [first, first + gridDim.x) -> rows
+// [edge - edge_base][1326] (colex order; hands on the board 0), one CTA per subgame.
+__global__ void rows_to_hands_kernel(const float *__restrict__ src, const BSub *__restrict__ subs,
+                                     const BPack *__restrict__ packs, int first, int edge_base,
+                                     float *__restrict__ dst) {
+    const int s = first + blockIdx.x;
+    const BSub d = subs[s];
+    const uint16_t *pos_of = packs[s].pos_of;
+    for (int k = 0; k < d.num_edges; k++) {
+        const float *row = src + (size_t)(d.edge_off + k) * kBRow;
+        float *out = dst + (size_t)(d.edge_off + k - edge_base) * 1326;
+        for (int h = threadIdx.x; h < 1326; h += blockDim.x) {
+            const int p = pos_of[h];
+            out[h] = p != 0xFFFF ? row[p] : 0.0f;
+        }
     }
 }
 
@@ -320,6 +349,10 @@ void *pr_batch_new(const pr_subgame *specs, int count, const float *ranges) {
         bfail("pr_batch_new: bad arguments");
         return nullptr;
     }
+    if (!valid_weights(ranges, (size_t)2 * 1326 * count)) {
+        bfail("pr_batch_new: a range holds a NaN, an infinity or a negative weight");
+        return nullptr;
+    }
     Batch *b = new Batch();
     b->count = count;
     b->specs.assign(specs, specs + count);
@@ -460,6 +493,18 @@ int pr_batch_enable_average(void *batch) {
     if ((e = cudaMalloc(&b->d_avg, rows)) != cudaSuccess || (e = cudaMemset(b->d_avg, 0, rows)) != cudaSuccess)
         return bfail("average-strategy allocation", e);
     b->avg_on = true;
+    // the average-sum kernels use more registers and shared memory: keep every class's
+    // resident CTAs per SM within what now fits
+    for (int c = 0; c < kClasses; c++) {
+        ClassCfg &k = b->cls[c];
+        const bool dense = k.K == 4 && k.per_sm >= 3;
+        const int fits = dense ? batch_dense_ctas_per_sm(1) : batch_ctas_per_sm(kBModeCFR, k.K, 0, 1);
+        if (k.per_sm > fits) k.per_sm = std::max(1, dense && fits < 3 ? std::min(fits, 2) : fits);
+    }
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
     return 0;
 }
 
@@ -595,33 +640,11 @@ int pr_batch_iterate_noalloc(void *batch, int iterations) {
     cudaError_t e = cudaMemcpyAsync(order, host_order.data(), sizeof(int) * b->count, cudaMemcpyHostToDevice,
                                     b->stream);
     if (e != cudaSuccess) return bfail("queue upload", e);
-    for (int it = 0; it < iterations; it++) {
-        // the queue heads must start at zero for every pass
-        e = cudaMemsetAsync(heads, 0, sizeof(int) * kNoAllocHeads, b->stream);
-        if (e != cudaSuccess) return bfail("queue reset", e);
-        for (int pl = 0; pl < 2; pl++) {
-            for (int c = 0; c < kClasses; c++) {
-                const ClassCfg &k = b->cls[c];
-                if (!k.count) continue;
-                BLaunch a{};
-                a.subs = b->d_subs;
-                a.nodes = b->d_nodes;
-                a.packs = b->d_packs;
-                a.ranges = b->d_ranges;
-                a.regrets = b->d_regrets;
-                a.avg = b->avg_on ? b->d_avg : nullptr;
-                a.order = order + k.first;
-                a.head = heads + pl * kClasses + c;
-                a.count = k.count;
-                a.player = pl;
-                const int ctas = std::min(k.count, std::max(1, k.per_sm) * b->sms);
-                const int dense = k.K == 4 && k.per_sm >= 3;
-                e = launch_batch_pass(kBModeCFR, k.K, 0, b->avg_on, a, ctas,
-                                      dense ? batch_dense_group() : batch_group_leaves(0), b->stream, dense);
-                if (e != cudaSuccess) return bfail("pass launch", e);
-            }
-        }
-    }
+    // the same iteration as pr_batch_iterate (launch configurations, average weights and the
+    // linear-average weight step), with the queue in the fixed array; the heads start at zero
+    // in every iteration
+    for (int it = 0; it < iterations; it++)
+        if (int st = b->iteration(order, heads)) return st;
     e = cudaStreamSynchronize(b->stream);
     return e == cudaSuccess ? 0 : bfail("iteration", e);
 }
@@ -670,6 +693,8 @@ int pr_batch_value_grad_device(void *batch, int use_average, double *d_r0, doubl
 int pr_batch_set_ranges(void *batch, int s, const float *r) {
     Batch *b = (Batch *)batch;
     if (!b || s < 0 || s >= b->count || !r) return 2;
+    if (!valid_weights(r, 2 * 1326))
+        return bfail("pr_batch_set_ranges: a range holds a NaN, an infinity or a negative weight");
     std::vector<float> rows(2 * kBRow, 0.0f);
     const uint16_t *hand = b->hand.data() + (size_t)s * kBRow;
     for (int pl = 0; pl < 2; pl++)
@@ -756,6 +781,35 @@ int pr_batch_set_average(void *batch, int s, const float *in) {
     return rows_io(b, b->d_avg, s, const_cast<float *>(in), false);
 }
 
+// All subgames' regret (which 0) or average-sum (which 1) rows at once: out[sum E_s][1326]
+// floats, colex order, subgames in batch order and each subgame's edges in its tree order.
+// Converted on the device in chunks of subgames and copied out one chunk at a time.
+int pr_batch_get_all(void *batch, int which, float *out) {
+    Batch *b = (Batch *)batch;
+    if (!b || !out || (which != 0 && which != 1) || (which == 1 && !b->avg_on)) return 2;
+    const float *src = which ? b->d_avg : b->d_regrets;
+    constexpr int kChunkRows = 8192;  // 43 MB of staging; a subgame has at most kBMaxNodes edges
+    float *stage = nullptr;
+    cudaError_t e = cudaMalloc(&stage, sizeof(float) * 1326 * kChunkRows);
+    if (e != cudaSuccess) return bfail("row staging allocation", e);
+    int s = 0;
+    while (s < b->count && e == cudaSuccess) {
+        const int base = b->subs[s].edge_off;
+        int t = s;
+        while (t < b->count && b->subs[t].edge_off + b->subs[t].num_edges - base <= kChunkRows) t++;
+        rows_to_hands_kernel<<<t - s, 256, 0, b->stream>>>(src, b->d_subs, b->d_packs, s, base, stage);
+        e = cudaGetLastError();
+        const size_t rows = (size_t)(t < b->count ? b->subs[t].edge_off : b->total_edges) - base;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out + (size_t)base * 1326, stage, sizeof(float) * 1326 * rows, cudaMemcpyDeviceToHost,
+                                b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        s = t;
+    }
+    cudaFree(stage);
+    return e == cudaSuccess ? 0 : bfail("row download", e);
+}
+
 // Configuration of class c: hands per thread, resident CTAs per SM, queue order.
 int pr_batch_config(void *batch, int c, int *K, int *per_sm, int *order, int *count) {
     Batch *b = (Batch *)batch;
@@ -818,9 +872,12 @@ int pr_batch_tune(void *batch, double *ms_out) {
         ClassCfg best_cfg = keep[c];
         for (int K : {2, 3, 4}) {
             const int fits = batch_ctas_per_sm(kBModeCFR, K, 0, b->avg_on);
-            // K = 4 also tries the dense configuration: registers capped for 3 CTAs per SM
-            const int top = K == 4 && batch_dense_ctas_per_sm(b->avg_on) >= 3 ? 3 : std::min(fits, 2);
-            for (int per = 1; per <= top; per++) {
+            // per = 1, 2 where they fit; K = 4 also tries the dense configuration (registers
+            // capped for 3 CTAs per SM) where three of its CTAs fit
+            std::vector<int> pers;
+            for (int per = 1; per <= std::min(fits, 2); per++) pers.push_back(per);
+            if (K == 4 && batch_dense_ctas_per_sm(b->avg_on) >= 3) pers.push_back(3);
+            for (int per : pers) {
                 for (int ord = 0; ord < 2; ord++) {
                     b->cls[c].K = K;
                     b->cls[c].per_sm = per;

@@ -137,6 +137,7 @@ struct DevTree {
     double *Rd = nullptr, *Vd = nullptr;  // double-precision best response (lazily allocated)
     float *opp = nullptr, *val = nullptr, *own = nullptr;  // [river][kRangeStride]
     double *opp64 = nullptr, *val64 = nullptr;
+    float *root_vals = nullptr;           // [2][kRangeStride]: the root's values of the last CFR pass per updater
     cudaGraphExec_t graph = nullptr;      // one CFR iteration, replayed
     bool graph_avg = false, graph_failed = false;
     bool ready = false;
@@ -163,6 +164,8 @@ struct Game {
     int status = 0;
     bool device_tree = true;
     DevTree dt;
+    std::vector<float> root_host[2];  // the root's values of the host traversal's last CFR pass per updater
+    int root_where = 0;               // 0: no CFR pass yet, 1: root_host, 2: dt.root_vals
     bool host_stale = false;  // the device holds newer upper regrets / sums than the host
     bool dev_stale = true;    // the host holds newer ones than the device
 
@@ -346,7 +349,7 @@ struct Game {
         for (void *p : {(void *)dt.nodes, (void *)dt.kids, (void *)dt.perm_maps, (void *)dt.levels,
                         (void *)dt.regrets, (void *)dt.avg, (void *)dt.Rf, (void *)dt.Vf, (void *)dt.Rd,
                         (void *)dt.Vd, (void *)dt.opp, (void *)dt.val, (void *)dt.own, (void *)dt.opp64,
-                        (void *)dt.val64})
+                        (void *)dt.val64, (void *)dt.root_vals})
             cudaFree(p);
         if (dt.stream) cudaStreamDestroy(dt.stream);
         dt = DevTree();
@@ -408,7 +411,8 @@ struct Game {
             (e = upload<float>(&dt.Rf, nullptr, N * 2 * kRangeStride)) ||
             (e = upload<float>(&dt.Vf, nullptr, N * kRangeStride)) ||
             (e = upload<float>(&dt.opp, nullptr, R * kRangeStride)) ||
-            (e = upload<float>(&dt.val, nullptr, R * kRangeStride)))
+            (e = upload<float>(&dt.val, nullptr, R * kRangeStride)) ||
+            (e = upload<float>(&dt.root_vals, nullptr, 2 * kRangeStride)))
             return cuda_fail("allocation", e);
         dt.ready = true;
         dev_stale = true;
@@ -483,6 +487,11 @@ struct Game {
             e = upper_up<T>(v, dt.levels + dt.level_off[d], dt.level_off[d + 1] - dt.level_off[d], upd, br ? 1 : 0,
                             R, V, val, dt.regrets, avg ? dt.avg : nullptr, dt.stream);
         if (e != cudaSuccess) return cuda_fail("bottom-up sweep", e);
+        if (!f64 && !br) {  // keep the root's values of this CFR pass (node 0 is the root)
+            e = cudaMemcpyAsync(dt.root_vals + (size_t)upd * kRangeStride, V, sizeof(float) * H,
+                                cudaMemcpyDeviceToDevice, dt.stream);
+            if (e != cudaSuccess) return cuda_fail("root values", e);
+        }
         return 0;
     }
 
@@ -532,6 +541,7 @@ struct Game {
         cudaError_t e = cudaStreamSynchronize(dt.stream);
         if (e != cudaSuccess) return cuda_fail("iteration", e);
         host_stale = true;
+        if (iterations > 0) root_where = 2;
         t_gpu += std::chrono::duration<double>(clk::now() - t0).count();
         return 0;
     }
@@ -798,14 +808,30 @@ int pr_game_iterate(void *game, int iterations) {
     Game *g = (Game *)game;
     if (!g) return 2;
     if (g->device_tree) return g->dt_iterate(iterations);
-    std::vector<float> out(prb::H);
     for (int it = 0; it < iterations; it++) {
         for (int upd = 0; upd < 2; upd++) {
-            const int st = g->half<float>(upd, false, out.data());
+            g->root_host[upd].resize(prb::H);
+            const int st = g->half<float>(upd, false, g->root_host[upd].data());
             if (st) return st;
+            g->root_where = 1;
         }
     }
     return 0;
+}
+
+int pr_game_root_values(void *game, float *sb, float *bb) {
+    Game *g = (Game *)game;
+    if (!g || !sb || !bb || !g->root_where) return 2;
+    if (g->root_where == 1) {
+        memcpy(sb, g->root_host[0].data(), sizeof(float) * prb::H);
+        memcpy(bb, g->root_host[1].data(), sizeof(float) * prb::H);
+        return 0;
+    }
+    cudaError_t e = cudaStreamSynchronize(g->dt.stream);
+    if (e == cudaSuccess) e = cudaMemcpy(sb, g->dt.root_vals, sizeof(float) * prb::H, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(bb, g->dt.root_vals + prb::kRangeStride, sizeof(float) * prb::H, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? 0 : Game::cuda_fail("root values", e);
 }
 
 int pr_game_exploitability(void *game, int fp64, double *sum_sb, double *sum_bb, double *mbh) {

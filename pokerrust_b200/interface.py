@@ -113,6 +113,8 @@ def lib():
         L.pr_game_tables.argtypes = [vp]
         L.pr_game_iterate.restype = i32
         L.pr_game_iterate.argtypes = [vp, i32]
+        L.pr_game_root_values.restype = i32
+        L.pr_game_root_values.argtypes = [vp, vp, vp]
         sg = ctypes.POINTER(SubgameSpec)
         L.pr_batch_tree.restype = i32
         L.pr_batch_tree.argtypes = [sg, vp, vp, vp, vp]
@@ -141,6 +143,8 @@ def lib():
         L.pr_batch_set_config.argtypes = [vp, i32, i32, i32, i32]
         L.pr_batch_tune.restype = i32
         L.pr_batch_tune.argtypes = [vp, vp]
+        L.pr_batch_get_all.restype = i32
+        L.pr_batch_get_all.argtypes = [vp, i32, vp]
         L.pr_batch_iterate_noalloc.restype = i32
         L.pr_batch_iterate_noalloc.argtypes = [vp, i32]
         L.pr_gemm_bf16.restype = i32
@@ -493,6 +497,12 @@ class Game:
     def iterate(self, iterations=1):
         _check(lib().pr_game_iterate(self.ptr, int(iterations)), "pr_game_iterate")
 
+    def root_values(self):
+        """The root's values of the last iteration's SB and BB CFR passes, [2][1326] f32."""
+        out = np.zeros((2, HANDS), np.float32)
+        _check(lib().pr_game_root_values(self.ptr, _ptr(out[0]), _ptr(out[1])), "pr_game_root_values")
+        return out
+
     def exploitability(self, fp64=False):
         a, b, m = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         _check(lib().pr_game_exploitability(self.ptr, int(bool(fp64)), ctypes.byref(a), ctypes.byref(b),
@@ -594,8 +604,8 @@ class Batch:
     """Many general river subgames solved together on the device (pr_batch_*)."""
 
     def __init__(self, specs, ranges):
-        specs = np.ascontiguousarray(specs, SPEC_DTYPE)
-        ranges = np.ascontiguousarray(ranges, np.float32)
+        specs = np.array(specs, SPEC_DTYPE)              # copies: set_ranges updates the batch's own
+        ranges = np.array(ranges, np.float32, order="C")  # record, never the caller's arrays
         assert ranges.shape == (len(specs), 2, HANDS)
         self.count = len(specs)
         self.specs = specs
@@ -685,6 +695,15 @@ class Batch:
 
     def average(self, s):
         return self._rows("pr_batch_get_average", s)
+
+    def all_rows(self, which, out=None):
+        """pr_batch_get_all: every subgame's regrets (which 0) or average sums (which 1),
+        [sum of edge counts][1326] f32; `out` may be a caller-owned array of that shape."""
+        if out is None:
+            edges = int(sum(self.shape(i)[1] for i in range(self.count)))
+            out = np.zeros((edges, HANDS), np.float32)
+        _check(lib().pr_batch_get_all(self.ptr, int(which), _ptr(out)), "pr_batch_get_all")
+        return out
 
     def set_average(self, s, v):
         self._rows("pr_batch_set_average", s, v)

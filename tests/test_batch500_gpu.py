@@ -1,0 +1,65 @@
+"""The 4096-subgame batch of general river subgames at its stated 500 CFR iterations
+(pr_batch_*), against the oracle (oracle/batch.cpp) on a seeded sample of 64 subgames:
+
+- exploitability of the average strategies in double precision after 500 iterations, against
+  the oracle's own 500 iterations of the same subgames (tests/golden/batch500_golden.npz, made
+  by tests/golden/make_batch500_golden.py): 1 %;
+- one teacher-forced iteration at iteration 500: the device's regrets and average sums after
+  499 iterations are loaded into the oracle, both run iteration 500, and regrets agree to 1e-4
+  and average sums to 1e-5 of their largest entry (the bounds of the single-iteration tests).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "batch500_golden.npz")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    if not os.path.exists(GOLDEN):
+        pytest.skip("500-iteration batch golden fixture missing")
+    return dict(np.load(GOLDEN))
+
+
+def _rel(got, want):
+    return np.abs(got - want).max() / max(np.abs(want).max(), 1e-30)
+
+
+def test_bench_batch_after_500_iterations(golden):
+    import pokerrust_b200 as P
+    specs, ranges = P.random_subgames(4096, seed=4321)
+    b = P.Batch(specs, ranges)
+    b.enable_average()
+    b.tune()
+    iters = int(golden["iterations"])
+    b.iterate(iters - 1)
+    sample = golden["sample"]
+    state = {int(s): (b.regrets(int(s)), b.average(int(s))) for s in sample}
+    b.iterate(1)
+
+    _, _, expl = b.exploitability(use_average=True, fp64=True)
+    err = np.abs(expl[sample] - golden["expl_avg"]) / np.abs(golden["expl_avg"])
+    print(f"\nexploitability of the average strategies after {iters} iterations, 64 sampled subgames: "
+          f"mean {expl[sample].mean():.5f} chips (oracle {golden['expl_avg'].mean():.5f}); "
+          f"relative error max {err.max():.2e}, median {np.median(err):.2e}")
+    assert err.max() < 1e-2, np.sort(err)[-5:]
+
+    order = P.card_order()
+    for s in sample:
+        s = int(s)
+        sp = specs[s]
+        o = O.Subgame(int(sp["board"]), float(sp["pot"]), float(sp["stack"]), int(sp["sizes"]),
+                      int(sp["max_raises"]), ranges[s, 0], ranges[s, 1])
+        o.regrets, o.average = state[s]
+        o.iterate(1, accumulate=True)
+        live = (order & np.uint64(sp["board"])) == 0
+        r = _rel(b.regrets(s)[:, live], o.regrets[:, live])
+        a = _rel(b.average(s)[:, live], o.average[:, live])
+        assert r < 1e-4 and a < 1e-5, (s, r, a)
+    b.close()

@@ -208,3 +208,21 @@ def test_linear_average():
     assert np.mean(ew) < np.mean(eu), (np.mean(ew), np.mean(eu))
     u.close()
     w.close()
+
+
+def test_bulk_rows_match_per_subgame_rows():
+    """pr_batch_get_all returns every subgame's rows in batch order, as the per-subgame calls do."""
+    import pokerrust_b200 as P
+    specs, ranges = P.random_subgames(40, seed=14)
+    b = P.Batch(specs, ranges)
+    b.enable_average()
+    b.iterate(3)
+    reg, avg = b.all_rows(0), b.all_rows(1)
+    off = 0
+    for s in range(b.count):
+        e = b.shape(s)[1]
+        assert np.array_equal(reg[off:off + e], b.regrets(s))
+        assert np.array_equal(avg[off:off + e], b.average(s))
+        off += e
+    assert off == reg.shape[0]
+    b.close()
