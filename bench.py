@@ -2,9 +2,10 @@
 """Benchmark of the river-subtree CFR hot path on the fixed-flop limit game.
 
 One step = one river pass (CFR regret update, alternating the updating player step by step)
-over all 27,783 river subgames of the reference's fixed-flop game, with seeded synthetic
-opponent ranges. Metric: river node visits per second (27,783 subgames x 48 rivers x 27
-nodes per pass, the count the reference's evaluate_river walks).
+over all 27,783 river subgames of the reference's fixed-flop game, with uniform opponent
+ranges over the hands the 4-card board does not block (the reference's Vector::ones).
+Metric: river node visits per second (27,783 subgames x 48 rivers x 27 nodes per pass, the
+count the reference's evaluate_river walks).
 
   value        device-resident pass (inputs already in HBM), timed with CUDA events
   e2e          the same pass through the reference-facing C ABI with host buffers:
@@ -16,6 +17,9 @@ nodes per pass, the count the reference's evaluate_river walks).
 --impl reference times the reference's CPU implementation of the path (the oracle port;
 the reference itself is Rust and cannot be built here) on the same workload.
 With torchrun (N > 1) every rank runs its own full pass (replicas, weak scaling).
+The line also carries one summary per further configuration (batched general subgames, the
+adjoint pair, the value network, the full game with general bets); --traces adds their
+exploitability trajectories and loss curves.
 """
 import argparse
 import json
@@ -39,7 +43,7 @@ WORKLOAD = "fixed-flop limit hold'em, all 27783 river subgames, one CFR pass per
 
 
 # DRAM bytes of one full river launch (27,783 subgames), read + write, from a single-pass ncu
-# capture of this program (profiles/launch_list_bench_profile.md)
+# capture of this program (dram__bytes_read.sum + dram__bytes_write.sum)
 TRAFFIC_PER_LAUNCH = 1063193600 + 509289984
 
 
@@ -114,12 +118,20 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def synthetic_ranges(order, boards, seed=1234):
-    """Seeded opponent ranges: U(0,1) per hand, zero on hands that hit the 4-card board."""
-    rng = np.random.default_rng(seed)
-    r = rng.random((len(boards), 1326), dtype=np.float32)
+def uniform_ranges(order, boards):
+    """Opponent ranges of the stated workload: 1 on every hand the 4-card board does not
+    block, 0 on the others (the reference's Vector::ones, game.rs:37-38, masked)."""
+    r = np.ones((len(boards), 1326), dtype=np.float32)
     r[(order[None, :] & boards[:, None]) != 0] = 0.0
     return r
+
+
+def bench_config(n, world):
+    """The workload description both arms print."""
+    return {"workload": WORKLOAD, "subgames": n, "flop": "2c3c4c (reference cards 0,1,2)",
+            "ranges": "uniform over the hands the 4-card board does not block",
+            "l2": "inputs larger than L2 (ranges+results+regrets ~1.04 GB)",
+            "parallelism": f"replicas x{world}"}
 
 
 def cpu_sample(boards, bets, ranges, tables, nthreads, subgames):
@@ -143,12 +155,15 @@ def sized_sample(boards, bets, ranges, tables, nthreads, seconds):
 
 
 BATCH_SUBGAMES = 4096
+BATCH_ITERATIONS = 500
 
 
-def batch_section(P, rank, peak, cpu_threads, with_cpu):
+def batch_section(P, rank, peak, cpu_threads, with_cpu, traces):
     """General river subgames (4096 seeded boards, pots, stacks and bet trees): per-hand CFR
-    iterations through the batched solver, its HBM roofline, and iterations / seconds until
-    the mean FP64 exploitability of the average strategies is at most 0.5 % of the pot."""
+    iterations through the batched solver, its HBM roofline, iterations / seconds until the
+    mean FP64 exploitability of the average strategies is at most 0.5 % of the pot, and the
+    stated 500-iteration solve end to end through the C ABI (host specs and ranges in, host
+    average sums out)."""
     specs, ranges = P.random_subgames(BATCH_SUBGAMES, seed=4321 + rank)
     b = P.Batch(specs, ranges)
     b.enable_average()
@@ -160,6 +175,7 @@ def batch_section(P, rank, peak, cpu_threads, with_cpu):
     it_s = (time.perf_counter() - t0) / steps
     nbytes = b.iteration_bytes()
     edges = sum(b.shape(i)[1] for i in range(b.count))
+    cfgs = [b.config(c) for c in range(2)]
     out = {
         "workload": f"{BATCH_SUBGAMES} river subgames, 5-card seeded boards, pot U{{2..200}}, stack U{{pot..10 pot}}, "
                     "bets from {0.5 pot, pot, all-in}, 1-3 raises, ranges U(0,1) with 25 % zeroed",
@@ -167,17 +183,17 @@ def batch_section(P, rank, peak, cpu_threads, with_cpu):
         "hand_edge_updates_per_s": edges * 1081 * 2 / it_s,
         "roofline": {"bound": "hbm", "achieved": nbytes / it_s / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": nbytes / it_s / 1e9 / peak, "bytes_per_iteration": nbytes},
-        "tuned_pass_ms": [float(x) for x in tuned],
-        "configs": [b.config(c) for c in range(2)],
+        "tuned_pass_ms": [round(float(x), 4) for x in tuned],
+        "configs": [f"K{c['K']}x{c['per_sm']}/o{c['order']}/{c['count']}" for c in cfgs],
     }
+    b.close()
     # convergence: restart from zero regrets, average sums weighted by the iteration number,
     # check every 25 iterations
     b2 = P.Batch(specs, ranges)
     b2.enable_average()
     b2.set_linear_average(True)
     for c in range(2):
-        cfg = b.config(c)
-        b2.set_config(c, cfg["K"], cfg["per_sm"], cfg["order"])
+        b2.set_config(c, cfgs[c]["K"], cfgs[c]["per_sm"], cfgs[c]["order"])
     done, t_solve, reached = 0, 0.0, None
     trace = []
     while done < 1000:
@@ -189,19 +205,37 @@ def batch_section(P, rank, peak, cpu_threads, with_cpu):
         pct = float(np.mean(ex / specs["pot"]) * 100.0)
         trace.append((done, round(pct, 4)))
         if pct <= 0.5:
-            reached = {"iterations": done, "solve_s": t_solve}
+            reached = {"iterations": done, "solve_s": round(t_solve, 4)}
             break
-    out["exploitability_pct_pot"] = trace
+    if traces:
+        out["exploitability_pct_pot"] = trace
     out["time_to_0.5pct_pot"] = reached
     out["averaging"] = "linear (iteration t weighs t)"
     b2.close()
-    b.close()
+    # end to end: the stated solve (500 iterations) from host specs and ranges to host average
+    # sums, through pr_batch_new / pr_batch_iterate / pr_batch_get_all
+    import torch
+    torch.cuda.synchronize()
+    host_avg = np.zeros((edges, 1326), np.float32)
+    t0 = time.perf_counter()
+    b3 = P.Batch(specs, ranges)
+    b3.enable_average()
+    for c in range(2):
+        b3.set_config(c, cfgs[c]["K"], cfgs[c]["per_sm"], cfgs[c]["order"])
+    b3.iterate(BATCH_ITERATIONS)
+    b3.all_rows(1, host_avg)
+    e2e_s = time.perf_counter() - t0
+    b3.close()
+    out["e2e"] = {"solve_s": e2e_s, "iterations": BATCH_ITERATIONS,
+                  "iteration_ms": e2e_s / BATCH_ITERATIONS * 1e3,
+                  "h2d_bytes": int(specs.nbytes + ranges.nbytes), "d2h_bytes": int(host_avg.nbytes),
+                  "note": "batch set-up, 500 CFR iterations and the download of every average sum"}
     if with_cpu:
         out["cpu_baseline"] = batch_cpu_sample(specs, ranges, cpu_threads)
     return out
 
 
-def adjoint_section(P, peak):
+def adjoint_section(P, peak, cpu_threads, with_cpu):
     """Config 3: the adjoint pair on 1024 general river subgames at their average strategies
     after 100 CFR iterations. Forward V = r0^T U(sigma) r1 (pr_batch_value), backward dV/dr0,
     dV/dr1 and dV/dsigma at the root (pr_batch_value_grad), both through the C ABI with their
@@ -235,16 +269,47 @@ def adjoint_section(P, peak):
         b.value_grad_device(d0, d1, ds, use_average=True)
     bwd_dev = (time.perf_counter() - t0) / reps
     nbytes = 2.0 * edges * 1081 * 4 + b.count * 4.0 * 1081 * 4
+    out = {"workload": "1024 river subgames (config-2 shapes), average strategies after 100 CFR iterations",
+           "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3, "backward_device_outputs_ms": bwd_dev * 1e3,
+           "roofline": {"bound": "hbm", "achieved": nbytes / (fwd + bwd_dev) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": nbytes / (fwd + bwd_dev) / 1e9 / peak, "bytes_fwd_bwd": nbytes,
+                        "note": "forward + backward with device outputs; backward_ms adds the host copies "
+                                "of the gradients ([1024][10][1326] doubles)"}}
+    if with_cpu:
+        out["cpu_baseline"] = adjoint_cpu_sample(b, specs, ranges, cpu_threads)
     b.close()
-    return {"workload": "1024 river subgames (config-2 shapes), average strategies after 100 CFR iterations",
-            "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3, "backward_device_outputs_ms": bwd_dev * 1e3,
-            "roofline": {"bound": "hbm", "achieved": nbytes / (fwd + bwd_dev) / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": nbytes / (fwd + bwd_dev) / 1e9 / peak, "bytes_fwd_bwd": nbytes,
-                         "note": "forward + backward with device outputs; backward_ms adds the host copies "
-                                 "of the gradients ([1024][10][1326] doubles)"}}
+    return out
 
 
-def full_game_section(P):
+def adjoint_cpu_sample(b, specs, ranges, threads):
+    """The oracle's double-precision strategy evaluation of both players (the values the
+    forward and backward pair return) from the device's average sums, on a sample of the
+    subgames sized to about 10 s, scaled to the batch."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+
+    def timed(idx):
+        subs = []
+        for s in idx:
+            sp = specs[s]
+            o = O.Subgame(int(sp["board"]), float(sp["pot"]), float(sp["stack"]), int(sp["sizes"]),
+                          int(sp["max_raises"]), ranges[s, 0], ranges[s, 1])
+            o.average = b.average(int(s))
+            subs.append(o)
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda o: (o.value(0, True), o.value(1, True)), subs))
+        return time.perf_counter() - t0
+
+    probe = max(threads, 8)
+    dt = timed(range(probe))
+    n = int(min(b.count, max(probe, probe * 10.0 / max(dt, 1e-6))))
+    dt = timed(range(n))
+    return {"fwd_bwd_ms": dt * b.count / n * 1e3, "cores": threads, "kind": "port",
+            "sample": f"{n} of {b.count} subgames, both players' FP64 evaluations, {dt:.2f} s, scaled"}
+
+
+def full_game_section(P, traces):
     """The full fixed-flop game with general bets (flop and turn sweeps over batched river
     subgames): CFR iteration time, river subgames solved per second, iterations / solver
     seconds until the FP64 exploitability of the average strategies is at most 0.5 % of the
@@ -270,7 +335,8 @@ def full_game_section(P):
     }
     g.reset()
     pts, reached = FS.trajectory(g, 300, 50, pot, 0.5)
-    out["exploitability_pct_pot"] = [(p["iterations"], round(p["pct_pot"], 4)) for p in pts]
+    if traces:
+        out["exploitability_pct_pot"] = [(p["iterations"], round(p["pct_pot"], 4)) for p in pts]
     out["time_to_0.5pct_pot"] = reached
     net = P.ValueNet(rows=512, seed=1)
     g.set_net(net)
@@ -284,10 +350,41 @@ def full_game_section(P):
     return out
 
 
-def value_net_section(P, peak_tflops, peak_sustained):
+def torch_gemm_baseline(P, rows):
+    """Library context for the training step: torch's BF16 matmuls (cuBLAS) of the step's 15
+    GEMM shapes (5 forward, 5 + 5 backward), with no element-wise work, timed with CUDA
+    events."""
+    import torch
+    shapes = [P.ValueNet.layer_shape(l) for l in range(5)]  # (out, in)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    mk = lambda *sh: torch.randn(*sh, device="cuda", dtype=torch.bfloat16, generator=g)
+    xs = [mk(rows, i) for o, i in shapes]
+    ws = [mk(o, i) for o, i in shapes]
+    dys = [mk(rows, o) for o, i in shapes]
+
+    def step():
+        for x, w in zip(xs, ws):
+            torch.matmul(x, w.t())
+        for x, w, dy in zip(xs, ws, dys):
+            torch.matmul(dy, w)
+            torch.matmul(dy.t(), x)
+
+    for _ in range(3):
+        step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(20):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 20
+
+
+def value_net_section(P, peak_tflops, peak_sustained, traces):
     """The turn-leaf value network: tensor-core throughput of training steps at batch 4096
-    (random inputs; 6 x 8.64 M x 4096 FLOP per step), and a small train / held-out run on
-    river-solver data against the baselines it replaces."""
+    (random inputs; 6 x 8.64 M x 4096 FLOP per step), torch's BF16 GEMMs of the same shapes as
+    library context, and a small train / held-out run on river-solver data against the
+    baselines it replaces."""
     import torch
     from pokerrust_b200 import train_value_net as T
     rows = 4096
@@ -308,13 +405,19 @@ def value_net_section(P, peak_tflops, peak_sustained):
     params = sum(o * i + o for o, i in (P.ValueNet.layer_shape(l) for l in range(5)))
     flops = 6.0 * params * rows
     net.close()
+    lib_ms = torch_gemm_baseline(P, rows)
     small = T.run(train_n=768, test_n=256, iterations=60, cheap=3, epochs=40, batch=256, lr=1e-3, seed=1)
+    if not traces:
+        small["train"].pop("loss_curve", None)
     return {
         "train_step_ms": step_s * 1e3, "batch": rows, "parameters": params,
         "tensor": {"achieved_tflops": flops / step_s / 1e12, "peak": peak_sustained,
                    "frac": flops / step_s / 1e12 / peak_sustained,
                    "note": "whole training step (15 GEMMs + element-wise kernels) over the measured sustained "
-                           "BF16 peak; the GEMMs alone reach 234-531 TFLOP/s on these shapes"},
+                           "BF16 peak"},
+        "library_context": {"torch_bf16_gemms_ms": lib_ms, "tflops": flops / (lib_ms / 1e3) / 1e12,
+                            "note": "torch.matmul (cuBLAS) of the step's 15 GEMM shapes only, no bias, GELU, "
+                                    "loss or Adam: a lower bound for a library-built step"},
         "heldout": small,
     }
 
@@ -371,7 +474,7 @@ def run_reference(args):
     nthreads = os.cpu_count() or 1
     game = O.Game(O.REFERENCE_FLOP, nthreads)
     boards, bets = game.river_roots()
-    ranges = synthetic_ranges(O.card_order(), boards)
+    ranges = uniform_ranges(O.card_order(), boards)
     tables = O.pack_flop_tables(O.REFERENCE_FLOP, nthreads)
     # each timed step is a bounded sample (about 10 s, less for long runs) of the pass
     per_step = min(10.0, 150.0 / max(1, args.steps))
@@ -387,12 +490,13 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": SUBGAMES * NODES_PER_SUBGAME / value * 1e3,
+        "ms_per_step": float(np.mean(times)) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "subgames": SUBGAMES},
+        "data": "synthetic", "config": bench_config(SUBGAMES, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                         "sample": f"{sample} of {SUBGAMES} river subgames per step, "
-                                   f"{float(np.mean(times)):.2f} s each, scaled to nodes/s"},
+                         "sample": f"each timed step is {sample} of the {SUBGAMES} river subgames "
+                                   f"({float(np.mean(times)):.2f} s of wall time, ms_per_step); value = "
+                                   "their node visits / that time"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -409,6 +513,11 @@ def run_batch_profile(args):
     specs, ranges = P.random_subgames(args.batch_profile, seed=4321 + rank)
     b = P.Batch(specs, ranges)
     b.enable_average()
+    if args.batch_config:
+        K, per_sm = (int(x) for x in args.batch_config.split(","))
+        for c in range(2):
+            if b.config(c)["count"]:
+                b.set_config(c, K, per_sm, 0)
     b.iterate(max(2, args.warmup))
     t0 = time.perf_counter()
     b.iterate(args.steps)
@@ -489,7 +598,7 @@ def run_gpu(args):
     else:
         builder = P.Builder.wrap(game.builder)   # owned by the game
     n = len(boards)
-    ranges = synthetic_ranges(P.card_order(), boards, seed=1234 + rank)
+    ranges = uniform_ranges(P.card_order(), boards)
     stride = P.RANGE_STRIDE
     d_ranges = torch.zeros((n, stride), dtype=torch.float32, device=dev)
     d_ranges[:, :1326] = torch.from_numpy(ranges).to(dev)
@@ -570,11 +679,12 @@ def run_gpu(args):
     h1, d1 = game.timings()
     game.set_device_tree(True)
 
-    batch = batch_section(P, rank, measured_peaks()[0], os.cpu_count() or 1, rank == 0)
+    cpu_threads = os.cpu_count() or 1
+    batch = batch_section(P, rank, measured_peaks()[0], cpu_threads, rank == 0, args.traces)
     tp = tensor_peaks()
-    vnet = value_net_section(P, tp[0], tp[1])
-    full = full_game_section(P)
-    adj = adjoint_section(P, measured_peaks()[0])
+    vnet = value_net_section(P, tp[0], tp[1], args.traces)
+    full = full_game_section(P, args.traces)
+    adj = adjoint_section(P, measured_peaks()[0], cpu_threads, rank == 0)
 
     line = None
     if rank == 0:
@@ -582,7 +692,6 @@ def run_gpu(args):
         peak, peak_kind = measured_peaks()
         ab = algorithmic_bytes(n)
         achieved = ab / (kernel_ms / 1e3) / 1e9
-        cpu_threads = os.cpu_count() or 1
         tables_host = O.pack_flop_tables(O.REFERENCE_FLOP, cpu_threads)
         cpu_n = sized_sample(boards, bets, ranges, tables_host, cpu_threads, 10.0)
         cpu_rate, cpu_dt = cpu_sample(boards, bets, ranges, tables_host, cpu_threads, cpu_n)
@@ -590,17 +699,14 @@ def run_gpu(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "subgames": n, "flop": "2c3c4c (reference cards 0,1,2)",
-                       "ranges": "seeded U(0,1) per hand, board-blocked hands zero",
-                       "l2": "inputs larger than L2 (ranges+results+regrets ~1.04 GB)",
-                       "parallelism": f"replicas x{world}"},
+            "config": bench_config(n, world),
             "e2e": {"value": world * n * NODES_PER_SUBGAME / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": int(n * 1328 * 4), "d2h_bytes_per_step": int(n * 1328 * 4),
                     "ms_per_step": e2e_s * 1e3},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH if n == SUBGAMES else None,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full launch "
-                                           "(profiles/launch_list_bench_profile.md)",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one full "
+                                           "launch of this program",
                          "peak_source": peak_kind,
                          "note": "algorithmic bytes per pass / kernel time; the pass is bound "
                                  "on-chip (shared memory and issue), not by HBM"},
@@ -639,6 +745,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch-profile", type=int, default=0,
                     help="only the batched general subgames: this many, a few timed iterations")
+    ap.add_argument("--batch-config", default="",
+                    help="with --batch-profile: hands per thread and CTAs per SM for both shape classes, e.g. 4,3")
     ap.add_argument("--net-profile", action="store_true",
                     help="only the value network: warm-up and timed training steps at batch 4096")
     ap.add_argument("--full-profile", action="store_true",
@@ -647,6 +755,8 @@ def main():
                     help="use the first N river roots only (profiling runs); 0 = all 27783")
     ap.add_argument("--profile", action="store_true",
                     help="kernel timing only: skip the end-to-end and CPU-baseline legs")
+    ap.add_argument("--traces", action="store_true",
+                    help="add exploitability trajectories and loss curves to the JSON line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
