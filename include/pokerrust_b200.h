@@ -286,6 +286,13 @@ int pr_gemm_bf16_major(const void *A, const void *B, float *D, int M, int N, int
 /* Asynchronous form; err is a device int that collects error bits of timed-out waits. */
 int pr_gemm_bf16_async(const void *A, const void *B, float *D, int M, int N, int K, int bn, int *err,
                        void *stream);
+/* Test support for the GEMM's bounded waits (no reference counterpart): the K-major product
+ * with an mbarrier wait limit of wait_ns and, with withhold_k >= 0, one tile load of CTA
+ * (0, 0) armed but never issued, so that the waits for it run out and the kernel returns
+ * with its error bits set (2 = MMA wait, 1 = producer wait) instead of hanging. Returns the
+ * error bits, -2 for bad shapes (K > 256 when a load is withheld), -1 on a CUDA error. */
+int pr_gemm_bf16_wait_test(const void *A, const void *B, float *D, int M, int N, int K, int bn,
+                           unsigned long long wait_ns, int withhold_k, void *stream);
 
 /* The network: 2706 inputs (both ranges, the 4 turn cards as 52 0/1 values, pot / 200 and
  * stack / (10 pot)) -> 4 x 1024 GELU -> 2652 outputs (both players' counterfactual values per

@@ -103,4 +103,35 @@ int pr_gemm_bf16_async(const void *A, const void *B, float *D, int M, int N, int
     return e == cudaSuccess ? 0 : (e == cudaErrorInvalidValue ? 2 : 1);
 }
 
+// Test of the bounded waits: the K-major product with wait limit `wait_ns` and, when
+// withhold_k >= 0, CTA (0, 0)'s load of k tile withhold_k armed but never issued, so that its
+// MMA warp's wait runs out. Synchronous; returns the kernel's error bits (0 when every wait
+// was met), or -2 for bad shapes (K must span more than 4 k tiles of 64 when a load is
+// withheld, so that the producer's own wait runs out too and the teardown waits for the loads
+// it issued), or -1 on a CUDA error.
+int pr_gemm_bf16_wait_test(const void *A, const void *B, float *D, int M, int N, int K, int bn,
+                           unsigned long long wait_ns, int withhold_k, void *stream) {
+    if (bn != 128 && bn != 256) return -2;
+    if (withhold_k >= 0 && (K / prb::gemm::kBK <= 4 || withhold_k >= K / prb::gemm::kBK)) return -2;
+    int *d_err = nullptr;
+    if (cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) return -1;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaMemsetAsync(d_err, 0, sizeof(int), s);
+    prb::gemm::EpiF32 epi{D, N, M, N};
+    prb::gemm::Hooks hooks;
+    hooks.wait_ns = wait_ns;
+    hooks.withhold_k = withhold_k;
+    const prb::gemm::bf16 *a = reinterpret_cast<const prb::gemm::bf16 *>(A);
+    const prb::gemm::bf16 *b = reinterpret_cast<const prb::gemm::bf16 *>(B);
+    using prb::gemm::kKMajor;
+    cudaError_t e = bn == 256 ? prb::gemm::run<256, kKMajor, kKMajor>(a, b, M, N, K, epi, d_err, s, 1, hooks)
+                              : prb::gemm::run<128, kKMajor, kKMajor>(a, b, M, N, K, epi, d_err, s, 1, hooks);
+    int err = 0;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d_err);
+    if (e == cudaErrorInvalidValue) return -2;
+    return e == cudaSuccess ? err : -1;
+}
+
 }  // extern "C"

@@ -40,6 +40,15 @@ constexpr int kBK = 64;
 constexpr int kThreads = 128;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // give up on an mbarrier after 2 s
 
+// Wait limit and a load to leave out, for the test of the bounded waits: with withhold_k =
+// k >= 0, CTA (0, 0, 0) arms stage k % kStages for k tile k but issues no copy into it, so
+// the MMA warp's wait for that stage runs out after wait_ns. Launches outside that test use
+// {kWaitNs, -1}.
+struct Hooks {
+    unsigned long long wait_ns = kWaitNs;
+    int withhold_k = -1;
+};
+
 constexpr UMMA::Major kKMajor = UMMA::Major::K;
 constexpr UMMA::Major kMNMajor = UMMA::Major::MN;
 
@@ -86,9 +95,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// Waits for the phase with parity `phase` of an mbarrier; false after kWaitNs of wall time.
+// Waits for the phase with parity `phase` of an mbarrier; false after limit_ns of wall time.
 // Each try_wait suspends for at most about a microsecond (its time hint), so the bound holds.
-__device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t phase) {
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t phase, unsigned long long limit_ns) {
     const uint32_t a = cute::cast_smem_ptr_to_uint(bar);
     unsigned long long start = 0;
     for (unsigned i = 0;; i++) {
@@ -103,7 +112,7 @@ __device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t phase) {
         if (ok) return true;
         const unsigned long long now = global_ns();
         if (i == 0) start = now;
-        else if (now - start > kWaitNs) return false;
+        else if (now - start > limit_ns) return false;
     }
 }
 
@@ -120,7 +129,7 @@ enum : int { kErrProducer = 1, kErrMma = 2, kErrEpilogue = 4 };
 template <int BN, UMMA::Major MA, UMMA::Major MB, class TmaA, class TmaB, class Epi>
 __global__ void __launch_bounds__(kThreads, 1)
     gemm_kernel(CUTE_GRID_CONSTANT TmaA const tma_a, CUTE_GRID_CONSTANT TmaB const tma_b, int M, int N, int K,
-                Epi epi, int *err) {
+                Epi epi, int *err, Hooks hooks) {
     using C = Cfg<BN, MA, MB>;
     extern __shared__ char smem_raw[];
     typename C::Shared &ss = *reinterpret_cast<typename C::Shared *>(
@@ -174,12 +183,16 @@ __global__ void __launch_bounds__(kThreads, 1)
         // producer: TMA loads of A and B tiles into the stage ring
         for (int k = 0; k < k_tiles; k++) {
             const int s = k % C::kStages;
-            if (k >= C::kStages && !bar_wait(&ss.empty[s], ((k / C::kStages) - 1) & 1)) {
+            if (k >= C::kStages && !bar_wait(&ss.empty[s], ((k / C::kStages) - 1) & 1, hooks.wait_ns)) {
                 atomicOr(err, kErrProducer);
                 ss.failed = 1;
                 break;
             }
             cutlass::arch::ClusterTransactionBarrier::arrive_and_expect_tx(&ss.full[s], C::kBytesA + C::kBytesB);
+            if (k == hooks.withhold_k && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
+                issued++;  // armed, never filled: the teardown's bounded wait gives it up
+                continue;
+            }
             copy(tma_a.with(ss.full[s]), tAgA(_, k_begin + k), tAsA(_, s));
             copy(tma_b.with(ss.full[s]), tBgB(_, k_begin + k), tBsB(_, s));
             issued++;
@@ -191,7 +204,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int k = 0; k < k_tiles && ok; k++) {
             const int s = k % C::kStages;
             // warp-uniform decision: the MMA and commit below are warp-collective
-            if (!__all_sync(0xffffffffu, bar_wait(&ss.full[s], (k / C::kStages) & 1))) {
+            if (!__all_sync(0xffffffffu, bar_wait(&ss.full[s], (k / C::kStages) & 1, hooks.wait_ns))) {
                 if (lane == 0) atomicOr(err, kErrMma);
                 ok = false;
                 break;
@@ -214,7 +227,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncwarp();
 
     // epilogue: all four warps, TMEM rows -> registers -> global, 32 columns at a time
-    const bool acc_ok = __all_sync(0xffffffffu, bar_wait(&ss.acc, 0));  // tcgen05.ld is warp-collective
+    const bool acc_ok = __all_sync(0xffffffffu, bar_wait(&ss.acc, 0, hooks.wait_ns));  // tcgen05.ld is warp-collective
     if (!acc_ok && lane == 0) atomicOr(err, kErrEpilogue);
     tmem_fence_after_sync();
     if (acc_ok) {
@@ -240,9 +253,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 0 && lane == 0 && ss.failed) {
         // only the last ring of loads can still be in flight (earlier stages were consumed)
         for (int k = issued > C::kStages ? issued - C::kStages : 0; k < issued; k++)
-            bar_wait(&ss.full[k % C::kStages], (k / C::kStages) & 1);
+            bar_wait(&ss.full[k % C::kStages], (k / C::kStages) & 1, hooks.wait_ns);
     }
-    if (!acc_ok) bar_wait(&ss.acc, 0);
+    if (!acc_ok) bar_wait(&ss.acc, 0, hooks.wait_ns);
     tmem_fence_before_sync();
     __syncthreads();
     if (warp == 1) {
@@ -266,7 +279,7 @@ inline auto operand_view(const bf16 *p, int rows, int K) {
 // the major mode of A ([M][K] or [K][M] in memory) and B ([N][K] or [K][N]).
 template <int BN, UMMA::Major MA = kKMajor, UMMA::Major MB = kKMajor, class Epi>
 inline cudaError_t run(const bf16 *A, const bf16 *B, int M, int N, int K, Epi epi, int *err, cudaStream_t stream,
-                       int splits = 1) {
+                       int splits = 1, Hooks hooks = Hooks()) {
     using C = Cfg<BN, MA, MB>;
     if (M % kBM || N % BN || K % kBK || K <= 0 || splits < 1 || splits > K / kBK) return cudaErrorInvalidValue;
     if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) return cudaErrorInvalidValue;
@@ -282,7 +295,7 @@ inline cudaError_t run(const bf16 *A, const bf16 *B, int M, int N, int K, Epi ep
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::kSmem);
     if (e != cudaSuccess) return e;
     dim3 grid(M / kBM, N / BN, splits);
-    kernel<<<grid, kThreads, C::kSmem, stream>>>(tma_a, tma_b, M, N, K, epi, err);
+    kernel<<<grid, kThreads, C::kSmem, stream>>>(tma_a, tma_b, M, N, K, epi, err, hooks);
     return cudaGetLastError();
 }
 

@@ -54,3 +54,32 @@ def test_gemm_rejects_bad_shapes():
     B = torch.zeros(128, 64, device="cuda", dtype=torch.bfloat16)
     D = torch.zeros(100, 128, device="cuda")
     assert P.lib().pr_gemm_bf16(A.data_ptr(), B.data_ptr(), D.data_ptr(), 100, 128, 64, 128, None) == 2
+
+
+def test_gemm_bounded_wait_runs_out_and_recovers():
+    """The GEMM's mbarrier waits are bounded: with one tile load of the first CTA armed but
+    never issued (test hook) and a 20 ms limit, the MMA warp's wait for it runs out, the
+    kernel sets its error bit and returns, and the context stays usable: the next product on
+    the same buffers is correct. The failure is made by withholding work, not by a fault."""
+    import torch
+    import pokerrust_b200 as P
+    M, N, K = 256, 256, 512  # 8 k tiles, more than the 4-stage ring
+    g = torch.Generator(device="cuda").manual_seed(3)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    D = torch.zeros((M, N), device="cuda", dtype=torch.float32)
+    torch.cuda.synchronize()
+    L = P.lib()
+    # without a withheld load every wait is met
+    assert L.pr_gemm_bf16_wait_test(A.data_ptr(), B.data_ptr(), D.data_ptr(), M, N, K, 128, 20_000_000, -1, None) == 0
+    want = A.float() @ B.float().T
+    assert (D - want).abs().max().item() <= 1e-5 * want.abs().max().item()
+    # the withheld load: the MMA wait (bit 2) and the producer's wait for the stage (bit 1) run out
+    bits = L.pr_gemm_bf16_wait_test(A.data_ptr(), B.data_ptr(), D.data_ptr(), M, N, K, 128, 20_000_000, 0, None)
+    assert bits & 2 and bits & 1, bits
+    torch.cuda.synchronize()  # the context is still usable
+    # bad shapes for the hook are refused before any launch
+    assert L.pr_gemm_bf16_wait_test(A.data_ptr(), B.data_ptr(), D.data_ptr(), M, N, 256, 128, 20_000_000, 0, None) == -2
+    D.zero_()
+    assert L.pr_gemm_bf16(A.data_ptr(), B.data_ptr(), D.data_ptr(), M, N, K, 128, None) == 0
+    assert (D - want).abs().max().item() <= 1e-5 * want.abs().max().item()
