@@ -311,10 +311,12 @@ __device__ __forceinline__ void prefetch_rows(const float *base, int first, int 
 // positive-part sum S keeps scale(S) = 1 / S, or -1 / n when S is at most the cutoff (1e-4
 // for regrets, 0 for average sums) and the strategy is uniform; an edge's probability is then
 // sigma(val, scale) = max(val, 0) x scale, or 1 / n.
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }  // = 1.0f / x, correctly rounded
+__device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }
 template <typename V, bool USEAVG>
 __device__ __forceinline__ V strategy_scale(V S, int n) {
     const V cut = USEAVG ? V(0) : V(1e-4f);
-    return S <= cut ? -(V(1) / V(n)) : V(1) / S;
+    return S <= cut ? -(V(1) / V(n)) : recip(S);
 }
 template <typename V>
 __device__ __forceinline__ V sigma(V val, V scale) {
@@ -382,9 +384,13 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
         }
 
         // walker state, per owned hand: depth-indexed stacks of the open path (indexed at run
-        // time, so they live in local memory, cached in L1)
-        V po[K][DS], pp[K][DS], St[K][DS];   // top-down: opponent weight, own reach, strategy scales
-        V acc[K][DS], Sb[K][DS];             // bottom-up: node values, strategy scales
+        // time, so they live in local memory, cached in L1). Depth-major with the K hands of a
+        // depth adjacent and aligned, so that one depth moves as one vector access.
+        alignas(16) V po[DS][K];
+        alignas(16) V pp[DS][K];
+        alignas(16) V St[DS][K];   // top-down: opponent weight, own reach, strategy scales
+        alignas(16) V acc[DS][K];
+        alignas(16) V Sb[DS][K];   // bottom-up: node values, strategy scales
         int open_id[DS];
         int open_top = -1;
         int td = 0, bu = 0;
@@ -401,10 +407,10 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
             }
             if (pq.actor != p) {
 #pragma unroll
-                for (int k = 0; k < K; k++) acc[k][dp] = acc[k][dp] + v[k];
+                for (int k = 0; k < K; k++) acc[dp][k] = acc[dp][k] + v[k];
             } else if (MODE == kBModeBR) {
 #pragma unroll
-                for (int k = 0; k < K; k++) acc[k][dp] = acc[k][dp] > v[k] ? acc[k][dp] : v[k];
+                for (int k = 0; k < K; k++) acc[dp][k] = acc[dp][k] > v[k] ? acc[dp][k] : v[k];
             } else {
                 // the edge's strategy from its regret (or average) row; CFR adds the child's
                 // value to the regret, which the parent's close turns into the regret update
@@ -416,7 +422,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     ld_k<K>(Src + ro, pos0, sv);
 #pragma unroll
                 for (int k = 0; k < K; k++)
-                    acc[k][dp] = acc[k][dp] + mul(sigma<V>(sv[k], Sb[k][dp]), v[k]);
+                    acc[dp][k] = acc[dp][k] + mul(sigma<V>(sv[k], Sb[dp][k]), v[k]);
                 if constexpr (MODE == kBModeCFR) {
                     float r[K];
 #pragma unroll
@@ -432,7 +438,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                 const BNode nm = S.tn[m];
                 V v[K];
 #pragma unroll
-                for (int k = 0; k < K; k++) v[k] = acc[k][open_top];
+                for (int k = 0; k < K; k++) v[k] = acc[open_top][k];
                 if (MODE == kBModeCFR && nm.actor == p) {
                     for (int e = 0; e < nm.nchild; e++) {
                         float *row = R + (size_t)(nm.edge + e) * kBRow;
@@ -480,9 +486,9 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     if (need) ld_k<K>(Src + ro, pos0, sv);
 #pragma unroll
                     for (int k = 0; k < K; k++) {
-                        const V po_par = po[k][d - 1];
-                        const V pp_par = pp[k][d - 1];
-                        const V sg = need ? sigma<V>(sv[k], St[k][d - 1]) : V(1);
+                        const V po_par = po[d - 1][k];
+                        const V pp_par = pp[d - 1][k];
+                        const V sg = need ? sigma<V>(sv[k], St[d - 1][k]) : V(1);
                         npo[k] = own ? po_par : mul(po_par, sg);
                         npp[k] = own ? mul(pp_par, sg) : pp_par;
                     }
@@ -498,8 +504,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                 }
 #pragma unroll
                 for (int k = 0; k < K; k++) {
-                    po[k][d] = npo[k];
-                    pp[k][d] = npp[k];
+                    po[d][k] = npo[k];
+                    pp[d][k] = npp[k];
                 }
                 if (nd.kind == kBDecision) {
                     // strategy sums of the node, for its children
@@ -519,7 +525,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     if (AVG && own) prefetch_rows<K>(A, nd.edge, min(nd.nchild, kPfRows), sub.num_edges, warp, lane);
 #pragma unroll
                     for (int k = 0; k < K; k++)
-                        St[k][d] = (!own || AVG) ? strategy_scale<V, USEAVG>(sum[k], nd.nchild) : V(0);
+                        St[d][k] = (!own || AVG) ? strategy_scale<V, USEAVG>(sum[k], nd.nchild) : V(0);
                 } else {
                     V xv[K];
 #pragma unroll
@@ -654,7 +660,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     V sum[K];
 #pragma unroll
                     for (int k = 0; k < K; k++) {
-                        acc[k][d] = (own && MODE == kBModeBR) ? neg_inf<V>() : V(0);
+                        acc[d][k] = (own && MODE == kBModeBR) ? neg_inf<V>() : V(0);
                         sum[k] = V(0);
                     }
                     if (own && MODE != kBModeBR) {
@@ -668,7 +674,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     }
 #pragma unroll
                     for (int k = 0; k < K; k++)
-                        Sb[k][d] = (own && MODE != kBModeBR) ? strategy_scale<V, USEAVG>(sum[k], nd.nchild) : V(0);
+                        Sb[d][k] = (own && MODE != kBModeBR) ? strategy_scale<V, USEAVG>(sum[k], nd.nchild) : V(0);
                 } else {
                     // a leaf: its value goes straight to the parent (open at depth d - 1)
                     V xv[K];
