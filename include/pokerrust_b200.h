@@ -286,6 +286,12 @@ int pr_gemm_bf16_major(const void *A, const void *B, float *D, int M, int N, int
 /* Asynchronous form; err is a device int that collects error bits of timed-out waits. */
 int pr_gemm_bf16_async(const void *A, const void *B, float *D, int M, int N, int K, int bn, int *err,
                        void *stream);
+/* The same BF16 product in the persistent form (no reference counterpart): one CTA per SM
+ * walks the output tiles with a double-buffered tensor-memory accumulator, so each tile's
+ * epilogue overlaps the next tile's main loop. D holds `splits` split-K parts [z][M][N]
+ * (f32); either operand may be MN-major. Synchronous: 0, 2 for bad shapes, 1 on error. */
+int pr_gemm_bf16_persistent(const void *A, const void *B, float *D, int M, int N, int K, int bn, int a_mn,
+                            int b_mn, int splits, void *stream);
 /* Test support for the GEMM's bounded waits (no reference counterpart): the K-major product
  * with an mbarrier wait limit of wait_ns and, with withhold_k >= 0, one tile load of CTA
  * (0, 0) armed but never issued, so that the waits for it run out and the kernel returns

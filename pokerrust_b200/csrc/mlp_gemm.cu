@@ -22,6 +22,19 @@ struct EpiF32 {
     }
 };
 
+// Split-K part z of D (f32, leading dimension ldd) goes to D + z * zstride.
+struct EpiParts {
+    float *D;
+    int ldd;
+    size_t zstride;
+    template <class R, class P>
+    __device__ void operator()(R const &reg, P const &pos, int m0, int n0, int z) const {
+        float *d = D + (size_t)z * zstride;
+#pragma unroll
+        for (int i = 0; i < size(reg); i++) d[(size_t)(m0 + get<0>(pos(i))) * ldd + n0 + get<1>(pos(i))] = reg(i);
+    }
+};
+
 }  // namespace gemm
 
 namespace {
@@ -101,6 +114,44 @@ int pr_gemm_bf16_async(const void *A, const void *B, float *D, int M, int N, int
     const cudaError_t e =
         prb::gemm_bf16_f32(A, B, D, M, N, K, N, M, N, bn, err, (cudaStream_t)stream, false, false);
     return e == cudaSuccess ? 0 : (e == cudaErrorInvalidValue ? 2 : 1);
+}
+
+// The persistent form (one CTA per SM walking the tiles, double-buffered accumulator):
+// D[z][M][N] (f32) = split-K part z of A . B^T, z < splits, either operand MN-major.
+// Synchronous; 0, 2 for bad shapes, 1 on a CUDA error or a timed-out wait.
+int pr_gemm_bf16_persistent(const void *A, const void *B, float *D, int M, int N, int K, int bn, int a_mn, int b_mn,
+                            int splits, void *stream) {
+    using namespace prb::gemm;
+    int *d_err = nullptr;
+    if (cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) return 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaMemsetAsync(d_err, 0, sizeof(int), s);
+    EpiParts epi{D, N, (size_t)M * N};
+    const bf16 *a = reinterpret_cast<const bf16 *>(A);
+    const bf16 *b = reinterpret_cast<const bf16 *>(B);
+    cudaError_t e = cudaErrorInvalidValue;
+    auto go = [&](auto bn_tag) {
+        constexpr int BN = decltype(bn_tag)::value;
+        if (!a_mn && !b_mn) return run_persistent<BN, kKMajor, kKMajor>(a, b, M, N, K, epi, d_err, s, splits);
+        if (!a_mn && b_mn) return run_persistent<BN, kKMajor, kMNMajor>(a, b, M, N, K, epi, d_err, s, splits);
+        if (a_mn && !b_mn) return run_persistent<BN, kMNMajor, kKMajor>(a, b, M, N, K, epi, d_err, s, splits);
+        return run_persistent<BN, kMNMajor, kMNMajor>(a, b, M, N, K, epi, d_err, s, splits);
+    };
+    if (bn == 256) e = go(std::integral_constant<int, 256>{});
+    else if (bn == 128) e = go(std::integral_constant<int, 128>{});
+    if (e == cudaErrorInvalidValue) {
+        cudaFree(d_err);
+        return 2;
+    }
+    int err = 0;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d_err);
+    if (e != cudaSuccess || err) {
+        fprintf(stderr, "pokerrust_b200: gemm (persistent): %s (error bits %d)\n", cudaGetErrorString(e), err);
+        return 1;
+    }
+    return 0;
 }
 
 // Test of the bounded waits: the K-major product with wait limit `wait_ns` and, when

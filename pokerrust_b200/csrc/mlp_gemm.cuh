@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include <cutlass/cutlass.h>
@@ -266,6 +267,212 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// ---- persistent form ----
+// One CTA per SM walks the output tiles (tile t, t + grid, ...; a tile is (m, n, split)) with
+// a double-buffered accumulator in tensor memory (2 x BN columns), so that the epilogue of
+// one tile runs while the main loop of the next fills the other accumulator. Roles, 256
+// threads: warp 0 streams tiles with TMA through the stage ring (stage and phase counters
+// continue across tiles), warp 1 issues tcgen05.mma and commits each finished accumulator,
+// warps 4-7 (one warpgroup: warp 4 + i reads TMEM lanes 32i..32i+31) drain accumulators with
+// tcgen05.ld through the same epilogues as gemm_kernel; warps 2-3 only take part in set-up and
+// teardown. Every wait is bounded: a role whose wait runs out records its error bit and raises
+// `abort`, the others stop at their next tile, and the teardown waits (bounded) for copies
+// and MMAs in flight before tensor memory is freed.
+constexpr int kPThreads = 256;
+
+template <int BN, UMMA::Major MA, UMMA::Major MB>
+struct PCfg {
+    using C = Cfg<BN, MA, MB>;
+    struct Shared {
+        typename C::Shared core;     // stage ring, full / empty barriers, tmem_base
+        alignas(8) uint64_t accf[2];  // accumulator b holds a finished tile (MMA commit)
+        alignas(8) uint64_t acce[2];  // accumulator b is drained (one arrival per epilogue warp)
+        alignas(8) uint64_t fin;      // every MMA issued has completed (teardown)
+        int abort;
+    };
+    static constexpr size_t kSmem = sizeof(Shared) + 1024;
+};
+
+template <int BN, UMMA::Major MA, UMMA::Major MB, class TmaA, class TmaB, class Epi>
+__global__ void __launch_bounds__(kPThreads, 1)
+    gemm_persistent_kernel(CUTE_GRID_CONSTANT TmaA const tma_a, CUTE_GRID_CONSTANT TmaB const tma_b, int M, int N,
+                           int K, int splits, Epi epi, int *err, unsigned long long wait_ns) {
+    using C = Cfg<BN, MA, MB>;
+    using PC = PCfg<BN, MA, MB>;
+    extern __shared__ char smem_raw[];
+    typename PC::Shared &ps = *reinterpret_cast<typename PC::Shared *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    typename C::Shared &ss = ps.core;
+    volatile int *abort_flag = &ps.abort;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    const int tiles_m = M / kBM, tiles_n = N / BN;
+    const int tiles = tiles_m * tiles_n * splits;
+    const int k_all = K / kBK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::kStages; s++) {
+            cutlass::arch::ClusterTransactionBarrier::init(&ss.full[s], 1);
+            cutlass::arch::ClusterBarrier::init(&ss.empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            cutlass::arch::ClusterBarrier::init(&ps.accf[b], 1);
+            cutlass::arch::ClusterBarrier::init(&ps.acce[b], 4);
+        }
+        cutlass::arch::ClusterBarrier::init(&ps.fin, 1);
+        ps.abort = 0;
+        cutlass::arch::fence_barrier_init();
+    }
+    if (warp == 1) {
+        cute::TMEM::Allocator1Sm alloc;
+        alloc.allocate(2 * BN, &ss.tmem_base);
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+
+    typename C::TiledMma tiled_mma;
+    ThrMMA cta_mma = tiled_mma.get_slice(0);
+    Tensor mA = tma_a.get_tma_tensor(make_shape(M, K));
+    Tensor mB = tma_b.get_tma_tensor(make_shape(N, K));
+    Tensor gA = local_tile(mA, typename C::Tiler{}, make_coord(_, _, _), Step<_1, X, _1>{});  // (BM, BK, m, k)
+    Tensor gB = local_tile(mB, typename C::Tiler{}, make_coord(_, _, _), Step<X, _1, _1>{});  // (BN, BK, n, k)
+    Tensor tCgA = cta_mma.partition_A(gA);
+    Tensor tCgB = cta_mma.partition_B(gB);
+    Tensor sA = make_tensor(make_smem_ptr(ss.A.begin()), typename C::SmemA{});
+    Tensor sB = make_tensor(make_smem_ptr(ss.B.begin()), typename C::SmemB{});
+    auto [tAgA, tAsA] = tma_partition(tma_a, Int<0>{}, Layout<_1>{}, group_modes<0, 3>(sA), group_modes<0, 3>(tCgA));
+    auto [tBgB, tBsB] = tma_partition(tma_b, Int<0>{}, Layout<_1>{}, group_modes<0, 3>(sB), group_modes<0, 3>(tCgB));
+    Tensor tCrA = cta_mma.make_fragment_A(sA);
+    Tensor tCrB = cta_mma.make_fragment_B(sB);
+    Tensor cC = make_identity_tensor(make_shape(Int<kBM>{}, Int<BN>{}));
+    Tensor tCcC = cta_mma.partition_C(cC);
+    Tensor tCtAcc = cta_mma.make_fragment_C(tCcC);
+
+    // tile t -> (m tile, n tile, split); the m tile varies fastest, so CTAs that run at the
+    // same time share B tiles in L2
+    auto decode = [&](int t, int &mt, int &nt, int &z, int &kb, int &kn) {
+        mt = t % tiles_m;
+        nt = (t / tiles_m) % tiles_n;
+        z = t / (tiles_m * tiles_n);
+        kb = (int)(((long long)k_all * z) / splits);
+        kn = (int)(((long long)k_all * (z + 1)) / splits) - kb;
+    };
+
+    int issued = 0;
+    if (warp == 0 && lane == 0) {
+        int it = 0;
+        for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x) {
+            int mt, nt, z, kb, kn;
+            decode(t, mt, nt, z, kb, kn);
+            for (int k = 0; k < kn; k++, it++) {
+                const int s = it % C::kStages;
+                if (it >= C::kStages && !bar_wait(&ss.empty[s], ((it / C::kStages) - 1) & 1, wait_ns)) {
+                    atomicOr(err, kErrProducer);
+                    *abort_flag = 1;
+                    break;
+                }
+                cutlass::arch::ClusterTransactionBarrier::arrive_and_expect_tx(&ss.full[s], C::kBytesA + C::kBytesB);
+                copy(tma_a.with(ss.full[s]), tAgA(_, mt, kb + k), tAsA(_, s));
+                copy(tma_b.with(ss.full[s]), tBgB(_, nt, kb + k), tBsB(_, s));
+                issued = it + 1;
+            }
+        }
+    } else if (warp == 1) {
+        int it = 0, local = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, local++) {
+            if (__any_sync(0xffffffffu, *abort_flag)) break;  // warp-uniform: the loop holds warp-collective calls
+            int mt, nt, z, kb, kn;
+            decode(t, mt, nt, z, kb, kn);
+            const int b = local & 1;
+            // the accumulator's previous tile (two tiles back) must be drained
+            if (local >= 2 && !__all_sync(0xffffffffu, bar_wait(&ps.acce[b], ((local >> 1) - 1) & 1, wait_ns))) {
+                if (lane == 0) atomicOr(err, kErrMma);
+                *abort_flag = 1;
+                break;
+            }
+            tmem_fence_after_sync();
+            tCtAcc.data() = ss.tmem_base + (uint32_t)(b * BN);
+            tiled_mma.accumulate_ = UMMA::ScaleOut::Zero;
+            for (int k = 0; k < kn; k++, it++) {
+                const int s = it % C::kStages;
+                if (!__all_sync(0xffffffffu, bar_wait(&ss.full[s], (it / C::kStages) & 1, wait_ns))) {
+                    if (lane == 0) atomicOr(err, kErrMma);
+                    *abort_flag = 1;
+                    ok = false;
+                    break;
+                }
+                tmem_fence_after_sync();
+#pragma unroll
+                for (int q = 0; q < size<2>(tCrA); q++) {
+                    cute::gemm(tiled_mma, tCrA(_, _, q, s), tCrB(_, _, q, s), tCtAcc);
+                    tiled_mma.accumulate_ = UMMA::ScaleOut::One;
+                }
+                cutlass::arch::umma_arrive(&ss.empty[s]);
+                __syncwarp();
+            }
+            if (!ok) break;
+            cutlass::arch::umma_arrive(&ps.accf[b]);
+            __syncwarp();
+        }
+        // every MMA issued so far completes before the teardown frees tensor memory
+        cutlass::arch::umma_arrive(&ps.fin);
+        __syncwarp();
+    } else if (warp >= 4) {
+        const int et = threadIdx.x - 128;  // thread within the epilogue warpgroup
+        int local = 0;
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x, local++) {
+            if (__any_sync(0xffffffffu, *abort_flag)) break;
+            int mt, nt, z, kb, kn;
+            decode(t, mt, nt, z, kb, kn);
+            const int b = local & 1;
+            if (!__all_sync(0xffffffffu, bar_wait(&ps.accf[b], (local >> 1) & 1, wait_ns))) {
+                if (lane == 0) atomicOr(err, kErrEpilogue);
+                *abort_flag = 1;
+                break;
+            }
+            tmem_fence_after_sync();
+            tCtAcc.data() = ss.tmem_base + (uint32_t)(b * BN);
+            Tensor acc = tCtAcc(make_coord(_, _), 0, 0);
+            Tensor crd = tCcC(make_coord(_, _), 0, 0);
+            const int m0 = mt * kBM, n0 = nt * BN;
+#pragma unroll 1
+            for (int j = 0; j < BN / 32; j++) {
+                Tensor acc_j = local_tile(acc, Shape<Int<kBM>, _32>{}, make_coord(0, j));
+                Tensor crd_j = local_tile(crd, Shape<Int<kBM>, _32>{}, make_coord(0, j));
+                auto t2r = make_tmem_copy(SM100_TMEM_LOAD_32dp32b32x{}, acc_j);
+                ThrCopy thr = t2r.get_slice(et);
+                Tensor src = thr.partition_S(acc_j);
+                Tensor pos = thr.partition_D(crd_j);
+                Tensor reg = make_tensor<float>(shape(pos));
+                copy(t2r, src, reg);
+                cutlass::arch::fence_view_async_tmem_load();
+                epi(reg, pos, m0, n0, z);
+            }
+            tmem_fence_before_sync();
+            __syncwarp();
+            if (lane == 0) cutlass::arch::ClusterBarrier::arrive(&ps.acce[b]);
+        }
+    }
+
+    __syncwarp();
+    // teardown: loads and MMAs in flight finish before shared memory and TMEM go away
+    if (warp == 0 && lane == 0 && *abort_flag) {
+        for (int it = issued > C::kStages ? issued - C::kStages : 0; it < issued; it++)
+            bar_wait(&ss.full[it % C::kStages], (it / C::kStages) & 1, wait_ns);
+    }
+    if (warp == 1) bar_wait(&ps.fin, 0, wait_ns);
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 1) {
+        tmem_fence_after_sync();
+        cute::TMEM::Allocator1Sm alloc;
+        alloc.release_allocation_lock();
+        alloc.free(ss.tmem_base, 2 * BN);
+    }
+}
+
 // The (rows x K) view of an operand: K-major [rows][K] or MN-major [K][rows] in memory.
 template <UMMA::Major MJ>
 inline auto operand_view(const bf16 *p, int rows, int K) {
@@ -296,6 +503,37 @@ inline cudaError_t run(const bf16 *A, const bf16 *B, int M, int N, int K, Epi ep
     if (e != cudaSuccess) return e;
     dim3 grid(M / kBM, N / BN, splits);
     kernel<<<grid, kThreads, C::kSmem, stream>>>(tma_a, tma_b, M, N, K, epi, err, hooks);
+    return cudaGetLastError();
+}
+
+// The persistent form of run(): one CTA per SM (at most one per tile) walks the tiles with a
+// double-buffered accumulator, so epilogues overlap the next tile's main loop.
+template <int BN, UMMA::Major MA = kKMajor, UMMA::Major MB = kKMajor, class Epi>
+inline cudaError_t run_persistent(const bf16 *A, const bf16 *B, int M, int N, int K, Epi epi, int *err,
+                                  cudaStream_t stream, int splits = 1, unsigned long long wait_ns = kWaitNs) {
+    using C = Cfg<BN, MA, MB>;
+    using PC = PCfg<BN, MA, MB>;
+    if (M % kBM || N % BN || K % kBK || K <= 0 || splits < 1 || splits > K / kBK) return cudaErrorInvalidValue;
+    if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) return cudaErrorInvalidValue;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    Tensor gA = operand_view<MA>(A, M, K);
+    Tensor gB = operand_view<MB>(B, N, K);
+    typename C::TiledMma mma;
+    auto cluster_vmnk = tiled_divide(make_layout(Shape<_1, _1, _1>{}), make_tile(typename C::TiledMma::AtomThrID{}));
+    auto tma_a = make_tma_atom_A_sm100<bf16>(SM90_TMA_LOAD{}, gA, typename C::SmemA{}(_, _, _, 0),
+                                             typename C::Tiler{}, mma, cluster_vmnk);
+    auto tma_b = make_tma_atom_B_sm100<bf16>(SM90_TMA_LOAD{}, gB, typename C::SmemB{}(_, _, _, 0),
+                                             typename C::Tiler{}, mma, cluster_vmnk);
+    auto kernel = gemm_persistent_kernel<BN, MA, MB, decltype(tma_a), decltype(tma_b), Epi>;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PC::kSmem);
+    if (e != cudaSuccess) return e;
+    const int tiles = (M / kBM) * (N / BN) * splits;
+    kernel<<<std::min(tiles, sms), kPThreads, PC::kSmem, stream>>>(tma_a, tma_b, M, N, K, splits, epi, err, wait_ns);
     return cudaGetLastError();
 }
 

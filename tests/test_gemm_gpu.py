@@ -83,3 +83,31 @@ def test_gemm_bounded_wait_runs_out_and_recovers():
     D.zero_()
     assert L.pr_gemm_bf16(A.data_ptr(), B.data_ptr(), D.data_ptr(), M, N, K, 128, None) == 0
     assert (D - want).abs().max().item() <= 1e-5 * want.abs().max().item()
+
+
+@pytest.mark.parametrize("M,N,K,bn,a_mn,b_mn,splits", [
+    (128, 128, 64, 128, 0, 0, 1),          # one tile
+    (4096, 1024, 1024, 128, 0, 1, 1),      # 256 tiles: more than one per SM, both accumulators in turn
+    (4096, 1024, 2816, 256, 0, 0, 1),      # the network's first layer
+    (1024, 1024, 4096, 256, 1, 1, 4),      # split-K weight gradient, both operands MN-major
+    (2048, 2048, 512, 256, 1, 0, 1),
+])
+def test_persistent_gemm_matches_fp32(M, N, K, bn, a_mn, b_mn, splits):
+    """The persistent form (one CTA per SM over all tiles, epilogues overlapping the next
+    tile's main loop through a double-buffered accumulator): the sum of its split-K parts is
+    the FP32 product of the same BF16 operands to 1e-5 of the output's scale."""
+    import torch
+    import pokerrust_b200 as P
+    g = torch.Generator(device="cuda").manual_seed(M + 3 * N + 7 * K + splits)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    As = A.T.contiguous() if a_mn else A
+    Bs = B.T.contiguous() if b_mn else B
+    D = torch.full((splits, M, N), float("nan"), device="cuda", dtype=torch.float32)
+    torch.cuda.synchronize()
+    st = P.lib().pr_gemm_bf16_persistent(As.data_ptr(), Bs.data_ptr(), D.data_ptr(), M, N, K, bn, a_mn, b_mn,
+                                         splits, None)
+    assert st == 0
+    want = A.float() @ B.float().T
+    err = (D.sum(0) - want).abs().max().item()
+    assert err <= 1e-5 * want.abs().max().item(), err
