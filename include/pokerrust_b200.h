@@ -309,6 +309,10 @@ int pr_gemm_bf16_wait_test(const void *A, const void *B, float *D, int M, int N,
 void *pr_mlp_new(int rows, uint64_t seed);
 void pr_mlp_free(void *net);
 int pr_mlp_rows(void *net);
+/* The GEMM form of the network's passes: 1 = the persistent form (pr_gemm_bf16_persistent,
+ * 128 x 128 tiles), 0 = one CTA per tile. Both give the same results bit for bit. Returns the
+ * previous setting, -1 for a null network. */
+int pr_mlp_set_persistent(void *net, int on);
 int pr_mlp_forward(void *net, const float *ranges, const uint64_t *boards, const float *scalars, float *out,
                    int n);
 /* One step: forward, loss, backward, Adam with learning rate lr (lr = 0: gradients only).

@@ -377,6 +377,15 @@ struct Net {
     float *bias_parts = nullptr;  // [kBiasChunks][cols] partial bias gradients
     int step = 0;
     static constexpr int kSplits = 4;
+    // GEMM form: one CTA per 128 x 256 tile (0), or the persistent form over 128 x 128 tiles
+    // (1), whose epilogues overlap the next tile's main loop; both give the same bits
+    int persistent = 0;
+
+    template <int BN, gemm::UMMA::Major MA = gemm::kKMajor, gemm::UMMA::Major MB = gemm::kKMajor, class Epi>
+    cudaError_t mm(const bf16 *A, const bf16 *B, int M, int N, int K, Epi epi, int splits = 1) {
+        if (persistent) return gemm::run_persistent<128, MA, MB>(A, B, M, N, K, epi, d_err, stream, splits);
+        return gemm::run<BN, MA, MB>(A, B, M, N, K, epi, d_err, stream, splits);
+    }
     std::vector<void *> owned;
 
     template <class T>
@@ -403,12 +412,12 @@ struct Net {
         const bf16 *in = X;
         for (int l = 0; l < 4 && e == cudaSuccess; l++) {
             EpiBiasGelu epi{b[l], Z[l], H[l], kN[l]};
-            e = gemm::run<256>(in, Wb[l], rows, kN[l], kK[l], epi, d_err, stream);
+            e = mm<256>(in, Wb[l], rows, kN[l], kK[l], epi);
             in = H[l];
         }
         if (e == cudaSuccess) {
             EpiBiasF32 epi{b[4], Y, kOutPad};
-            e = gemm::run<128>(in, Wb[4], rows, kOutPad, kHid, epi, d_err, stream);
+            e = mm<128>(in, Wb[4], rows, kOutPad, kHid, epi);
         }
         return check(e, "forward");
     }
@@ -418,7 +427,7 @@ struct Net {
     // whose parts stay apart: Adam sums them in part order
     cudaError_t weight_grad(const bf16 *G, const bf16 *In, int M, int N, int l) {
         EpiStore epi{parts[l], N, (size_t)M * N};
-        return gemm::run<256, gemm::kMNMajor, gemm::kMNMajor>(G, In, M, N, rows, epi, d_err, stream, kSplits);
+        return mm<256, gemm::kMNMajor, gemm::kMNMajor>(G, In, M, N, rows, epi, kSplits);
     }
 
     // the gradient of layer l's weights as one array (dW[l]), from its split-K parts
@@ -439,15 +448,14 @@ struct Net {
         bias_grad(dY, db[4], kOutPad);
         if (e == cudaSuccess) {
             EpiGeluGrad epi{Z[3], dZ[3], kHid};
-            e = gemm::run<256, gemm::kKMajor, gemm::kMNMajor>(dY, Wb[4], rows, kHid, kOutPad, epi, d_err, stream);
+            e = mm<256, gemm::kKMajor, gemm::kMNMajor>(dY, Wb[4], rows, kHid, kOutPad, epi);
         }
         for (int l = 3; l >= 0 && e == cudaSuccess; l--) {
             e = weight_grad(dZ[l], l > 0 ? H[l - 1] : X, kHid, kK[l], l);
             bias_grad(dZ[l], db[l], kHid);
             if (e == cudaSuccess && l > 0) {
                 EpiGeluGrad epi2{Z[l - 1], dZ[l - 1], kHid};
-                e = gemm::run<256, gemm::kKMajor, gemm::kMNMajor>(dZ[l], Wb[l], rows, kHid, kHid, epi2, d_err,
-                                                                 stream);
+                e = mm<256, gemm::kKMajor, gemm::kMNMajor>(dZ[l], Wb[l], rows, kHid, kHid, epi2);
             }
         }
         if (e == cudaSuccess) e = cudaGetLastError();
@@ -544,6 +552,16 @@ void *pr_mlp_new(int rows, uint64_t seed) {
 void pr_mlp_free(void *net) { delete (Net *)net; }
 
 int pr_mlp_rows(void *net) { return net ? ((Net *)net)->rows : 0; }
+
+// GEMM form of the network's passes: 1 the persistent form, 0 one CTA per tile. Returns the
+// previous setting, or -1 for a null network.
+int pr_mlp_set_persistent(void *net, int on) {
+    Net *n = (Net *)net;
+    if (!n) return -1;
+    const int was = n->persistent;
+    n->persistent = on ? 1 : 0;
+    return was;
+}
 
 namespace {
 int load_inputs(Net *n, const float *ranges, const unsigned long long *boards, const float *scalars, int count) {

@@ -157,6 +157,8 @@ def lib():
         L.pr_gemm_bf16_persistent.argtypes = [vp, vp, vp, i32, i32, i32, i32, i32, i32, i32, vp]
         L.pr_gemm_bf16_wait_test.restype = i32
         L.pr_gemm_bf16_wait_test.argtypes = [vp, vp, vp, i32, i32, i32, i32, ctypes.c_uint64, i32, vp]
+        L.pr_mlp_set_persistent.restype = i32
+        L.pr_mlp_set_persistent.argtypes = [vp, i32]
         L.pr_mlp_new.restype = vp
         L.pr_mlp_new.argtypes = [i32, u64]
         L.pr_mlp_free.argtypes = [vp]
@@ -774,6 +776,10 @@ class ValueNet:
         o, i = ctypes.c_int(), ctypes.c_int()
         _check(lib().pr_mlp_layer_shape(int(l), ctypes.byref(o), ctypes.byref(i)), "pr_mlp_layer_shape")
         return o.value, i.value
+
+    def set_persistent(self, on=True):
+        """pr_mlp_set_persistent: the persistent GEMM form (True) or one CTA per tile."""
+        return lib().pr_mlp_set_persistent(self.ptr, int(bool(on)))
 
     def forward(self, ranges, boards, scalars, out):
         """ranges [n][2][1326] f32, boards [n] int64 (4-card masks), scalars [n][2] f32,

@@ -70,3 +70,26 @@ def test_training_lowers_the_loss():
         last = net.train_step(r, b, s, t, lr=1e-3)
     assert last < 0.3 * first, (first, last)
     net.close()
+
+
+def test_persistent_gemms_give_the_same_bits():
+    """The network's passes through the persistent GEMM form (128 x 128 tiles, overlapped
+    epilogues) give the same loss, gradients and outputs bit for bit: every output element
+    is accumulated over K in the same order in both forms."""
+    import torch
+    import pokerrust_b200 as P
+    ranges, boards, scalars, targets = _batch(512, 9)
+    r, b, s, t = _dev(ranges, boards, scalars, targets)
+    res = []
+    for persistent in (False, True):
+        net = P.ValueNet(rows=512, seed=5)
+        net.set_persistent(persistent)
+        losses = [net.train_step(r, b, s, t, lr=1e-3) for _ in range(3)]
+        out = torch.zeros((512, 2652), device="cuda")
+        net.forward(r, b, s, out)
+        res.append((losses, [net.grad(l)[0] for l in range(5)], out.cpu().numpy()))
+        net.close()
+    assert res[0][0] == res[1][0]
+    for a, w in zip(res[0][1], res[1][1]):
+        assert np.array_equal(a, w)
+    assert np.array_equal(res[0][2], res[1][2])
