@@ -255,7 +255,9 @@ int pr_batch_value_grad(void *batch, int use_average, double *d_r0, double *d_r1
 /* The same backward pass with device outputs (device pointers, same layouts; null skipped),
  * for callers that use the gradients on the GPU. Synchronous. */
 int pr_batch_value_grad_device(void *batch, int use_average, double *d_r0, double *d_r1, double *d_sigma);
-/* Replaces subgame s's ranges ([2][1326] floats). */
+/* Replaces subgame s's ranges ([2][1326] floats). NaNs and infinities are refused (status
+ * 2); negative weights are accepted, since the value and its adjoint are bilinear in the
+ * ranges (central differences step below zero); CFR on them is the caller's concern. */
 int pr_batch_set_ranges(void *batch, int s, const float *r);
 /* Regrets / average sums of subgame s: [edges][1326] floats, edges in tree order. */
 int pr_batch_get_regrets(void *batch, int s, float *out);
@@ -292,6 +294,10 @@ int pr_gemm_bf16_async(const void *A, const void *B, float *D, int M, int N, int
  * (f32); either operand may be MN-major. Synchronous: 0, 2 for bad shapes, 1 on error. */
 int pr_gemm_bf16_persistent(const void *A, const void *B, float *D, int M, int N, int K, int bn, int a_mn,
                             int b_mn, int splits, void *stream);
+/* The K-major persistent product launched on `stream` without synchronising; err: a device
+ * int collecting the kernel's error bits. 0, 2 (bad shapes) or 1. */
+int pr_gemm_bf16_persistent_async(const void *A, const void *B, float *D, int M, int N, int K, int bn, int *err,
+                                  void *stream);
 /* Test support for the GEMM's bounded waits (no reference counterpart): the K-major product
  * with an mbarrier wait limit of wait_ns and, with withhold_k >= 0, one tile load of CTA
  * (0, 0) armed but never issued, so that the waits for it run out and the kernel returns

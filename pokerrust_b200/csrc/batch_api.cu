@@ -19,10 +19,11 @@
 namespace prb {
 namespace {
 
-// True when every weight of n is finite and non-negative (v - v is NaN for NaN and infinities).
-bool valid_weights(const float *r, size_t n) {
+// True when every weight of n is finite and, with `nonneg`, not negative (v - v is NaN for NaN
+// and infinities).
+bool valid_weights(const float *r, size_t n, bool nonneg = true) {
     float bad = 0.0f;
-    for (size_t i = 0; i < n; i++) bad += (r[i] - r[i]) + (r[i] < 0.0f ? 1.0f : 0.0f);
+    for (size_t i = 0; i < n; i++) bad += (r[i] - r[i]) + (nonneg && r[i] < 0.0f ? 1.0f : 0.0f);
     return bad == 0.0f;
 }
 
@@ -693,8 +694,9 @@ int pr_batch_value_grad_device(void *batch, int use_average, double *d_r0, doubl
 int pr_batch_set_ranges(void *batch, int s, const float *r) {
     Batch *b = (Batch *)batch;
     if (!b || s < 0 || s >= b->count || !r) return 2;
-    if (!valid_weights(r, 2 * 1326))
-        return bfail("pr_batch_set_ranges: a range holds a NaN, an infinity or a negative weight");
+    // finite weights only; negative ones are allowed here: the subgame value and its adjoint
+    // are bilinear in the ranges, and central differences step below zero
+    if (!valid_weights(r, 2 * 1326, false)) return bfail("pr_batch_set_ranges: a range holds a NaN or an infinity");
     std::vector<float> rows(2 * kBRow, 0.0f);
     const uint16_t *hand = b->hand.data() + (size_t)s * kBRow;
     for (int pl = 0; pl < 2; pl++)

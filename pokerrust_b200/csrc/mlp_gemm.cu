@@ -154,6 +154,20 @@ int pr_gemm_bf16_persistent(const void *A, const void *B, float *D, int M, int N
     return 0;
 }
 
+// The K-major persistent product launched asynchronously on `stream` (D = A . B^T, f32);
+// err: a device int that collects the kernel's error bits. 0, 2 (bad shapes) or 1.
+int pr_gemm_bf16_persistent_async(const void *A, const void *B, float *D, int M, int N, int K, int bn, int *err,
+                                  void *stream) {
+    using namespace prb::gemm;
+    EpiF32 epi{D, N, M, N};
+    const bf16 *a = reinterpret_cast<const bf16 *>(A);
+    const bf16 *b = reinterpret_cast<const bf16 *>(B);
+    cudaError_t e = cudaErrorInvalidValue;
+    if (bn == 256) e = run_persistent<256>(a, b, M, N, K, epi, err, (cudaStream_t)stream);
+    else if (bn == 128) e = run_persistent<128>(a, b, M, N, K, epi, err, (cudaStream_t)stream);
+    return e == cudaSuccess ? 0 : (e == cudaErrorInvalidValue ? 2 : 1);
+}
+
 // Test of the bounded waits: the K-major product with wait limit `wait_ns` and, when
 // withhold_k >= 0, CTA (0, 0)'s load of k tile withhold_k armed but never issued, so that its
 // MMA warp's wait runs out. Synchronous; returns the kernel's error bits (0 when every wait

@@ -153,6 +153,8 @@ def lib():
         L.pr_gemm_bf16_major.argtypes = [vp, vp, vp, i32, i32, i32, i32, i32, i32, vp]
         L.pr_gemm_bf16_async.restype = i32
         L.pr_gemm_bf16_async.argtypes = [vp, vp, vp, i32, i32, i32, i32, vp, vp]
+        L.pr_gemm_bf16_persistent_async.restype = i32
+        L.pr_gemm_bf16_persistent_async.argtypes = [vp, vp, vp, i32, i32, i32, i32, vp, vp]
         L.pr_gemm_bf16_persistent.restype = i32
         L.pr_gemm_bf16_persistent.argtypes = [vp, vp, vp, i32, i32, i32, i32, i32, i32, i32, vp]
         L.pr_gemm_bf16_wait_test.restype = i32
