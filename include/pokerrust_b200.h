@@ -366,6 +366,10 @@ int pr_full_shape(void *game, int *num_nodes, int *num_edges, int *num_leaves, i
                   int *allin_subgames);
 /* Net-leaf mode on (a pr_mlp_new network) or off (null). */
 int pr_full_set_net(void *game, void *net);
+/* Net leaves shifted to zero sum (on = 1): the outputs v0, v1 move by -e/2 with
+ * e = r0 . v0 + r1 . v1 over the normalised leaf ranges, which true subgame values satisfy
+ * with e = 0. Off by default. */
+int pr_full_set_zero_sum(void *game, int on);
 /* The batched solver's autotuner on both river-subgame batches; ms_out[4] (or null): the
  * chosen per-pass times of each batch's two shape classes. */
 int pr_full_tune(void *game, double *ms_out);

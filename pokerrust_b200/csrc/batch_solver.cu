@@ -536,80 +536,126 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
             __syncthreads();
 
             // ---- leaves of the group: opponent weights -> p's values ----
-            // A fold by p followed by its sibling call (a showdown) sees the same opponent
-            // weights (p's actions leave them unchanged): one scan serves both leaves.
-            int phase = 0;  // scans done in this group; their parity picks the buffers
+            // A job is a leaf, or a fold by p followed by its sibling call (a showdown): p's
+            // actions leave the opponent weights unchanged, so one scan serves both leaves.
+            // Jobs go two at a time (buffers 0 and 1): their scans interleave, and each hand's
+            // tie-group and card-list bounds are unpacked once for both. Every job's
+            // arithmetic is the same as when it runs alone.
             for (int j = g0; j < g1;) {
-                const int buf = phase & 1;
-                phase++;
-                const BNode ln = S.tn[S.leaf_node[j]];
-                bool pair = false;
-                BNode lsd = ln;  // the leaf whose kind and stake give the main value
-                if (ln.kind == kBFold && ln.actor == p && j + 1 < g1) {
-                    const BNode nx = S.tn[S.leaf_node[j + 1]];
-                    if (nx.kind == kBShowdown && nx.parent == ln.parent) {
-                        pair = true;
-                        lsd = nx;
+                bool pair[2] = {false, false};
+                BNode ln[2], lsd[2];
+                V *xs[2], *xfs[2];
+                int nj = 0;
+                while (nj < 2 && j < g1) {
+                    ln[nj] = S.tn[S.leaf_node[j]];
+                    lsd[nj] = ln[nj];  // the leaf whose kind and stake give the main value
+                    if (ln[nj].kind == kBFold && ln[nj].actor == p && j + 1 < g1) {
+                        const BNode nx = S.tn[S.leaf_node[j + 1]];
+                        if (nx.kind == kBShowdown && nx.parent == ln[nj].parent) {
+                            pair[nj] = true;
+                            lsd[nj] = nx;
+                        }
                     }
+                    xfs[nj] = S.X + (size_t)(j - g0) * kBRow;          // the fold's row when paired
+                    xs[nj] = pair[nj] ? xfs[nj] + kBRow : xfs[nj];     // the scanned leaf's row
+                    j += pair[nj] ? 2 : 1;
+                    nj++;
                 }
-                V *xf = S.X + (size_t)(j - g0) * kBRow;  // the fold's row when paired
-                V *x = pair ? xf + kBRow : xf;           // the scanned leaf's row
-                V *I = S.I + buf * kBRow;
-                V *CT = S.CT + buf * kBChunks;
-                V *SC = S.SC + buf * kBLists * 48;
                 // phase A: scans of the rank order in 64-hand chunks (two hands per lane) and
-                // scans of the card lists
+                // scans of the card lists, unit u of both jobs together
                 for (int u = warp; u < kBChunks64 + kBLists; u += NW) {
                     if (u < kBChunks64) {
-                        const V a0 = x[u * 64 + 2 * lane];
-                        const V a1 = a0 + x[u * 64 + 2 * lane + 1];
-                        V v = a1;
+                        V a0[2], v[2];
+#pragma unroll
+                        for (int q = 0; q < 2; q++) {
+                            a0[q] = v[q] = V(0);
+                            if (q < nj) {
+                                a0[q] = xs[q][u * 64 + 2 * lane];
+                                v[q] = a0[q] + xs[q][u * 64 + 2 * lane + 1];
+                            }
+                        }
 #pragma unroll
                         for (int off = 1; off < 32; off <<= 1) {
-                            const V t = __shfl_up_sync(FULL, v, off);
-                            if (lane >= off) v += t;
+#pragma unroll
+                            for (int q = 0; q < 2; q++) {
+                                const V t = __shfl_up_sync(FULL, v[q], off);
+                                if (lane >= off) v[q] += t;
+                            }
                         }
-                        V ex = __shfl_up_sync(FULL, v, 1);
-                        if (lane == 0) ex = V(0);
-                        I[u * 64 + 2 * lane] = ex + a0;
-                        I[u * 64 + 2 * lane + 1] = v;
-                        if (lane == 31) CT[u] = v;
+#pragma unroll
+                        for (int q = 0; q < 2; q++) {
+                            V ex = __shfl_up_sync(FULL, v[q], 1);
+                            if (lane == 0) ex = V(0);
+                            if (q < nj) {
+                                V *I = S.I + q * kBRow;
+                                I[u * 64 + 2 * lane] = ex + a0[q];
+                                I[u * 64 + 2 * lane + 1] = v[q];
+                                if (lane == 31) S.CT[q * kBChunks + u] = v[q];
+                            }
+                        }
                     } else {
                         const int li = u - kBChunks64;
-                        V a0 = V(0), a1 = V(0);
+                        int c0 = 0, c1 = 0;
                         if (lane < kBListLen / 2) {
-                            a0 = x[pk->clpos[li][2 * lane]];
-                            a1 = a0 + x[pk->clpos[li][2 * lane + 1]];
+                            c0 = pk->clpos[li][2 * lane];
+                            c1 = pk->clpos[li][2 * lane + 1];
                         }
-                        V v = a1;
+                        V a0[2], v[2];
+#pragma unroll
+                        for (int q = 0; q < 2; q++) {
+                            a0[q] = v[q] = V(0);
+                            if (q < nj && lane < kBListLen / 2) {
+                                a0[q] = xs[q][c0];
+                                v[q] = a0[q] + xs[q][c1];
+                            }
+                        }
 #pragma unroll
                         for (int off = 1; off < 32; off <<= 1) {
-                            const V t = __shfl_up_sync(FULL, v, off);
-                            if (lane >= off) v += t;
+#pragma unroll
+                            for (int q = 0; q < 2; q++) {
+                                const V t = __shfl_up_sync(FULL, v[q], off);
+                                if (lane >= off) v[q] += t;
+                            }
                         }
-                        V ex = __shfl_up_sync(FULL, v, 1);
-                        if (lane == 0) ex = V(0);
-                        if (lane < kBListLen / 2) {
-                            SC[li * 48 + 2 * lane] = ex + a0;
-                            SC[li * 48 + 2 * lane + 1] = v;
+#pragma unroll
+                        for (int q = 0; q < 2; q++) {
+                            V ex = __shfl_up_sync(FULL, v[q], 1);
+                            if (lane == 0) ex = V(0);
+                            if (q < nj && lane < kBListLen / 2) {
+                                V *SC = S.SC + q * kBLists * 48;
+                                SC[li * 48 + 2 * lane] = ex + a0[q];
+                                SC[li * 48 + 2 * lane + 1] = v[q];
+                            }
                         }
                     }
                 }
                 __syncthreads();
                 // phase C: chunk offsets (every warp, same arithmetic; lane c holds chunk c's),
                 // then values
-                V inc = lane < kBChunks64 ? CT[lane] : V(0);
+                V cofs[2], T[2];
+                {
+                    V inc[2];
 #pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const V t = __shfl_up_sync(FULL, inc, off);
-                    if (lane >= off) inc += t;
+                    for (int q = 0; q < 2; q++) inc[q] = (q < nj && lane < kBChunks64) ? S.CT[q * kBChunks + lane] : V(0);
+#pragma unroll
+                    for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+                        for (int q = 0; q < 2; q++) {
+                            const V t = __shfl_up_sync(FULL, inc[q], off);
+                            if (lane >= off) inc[q] += t;
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 2; q++) {
+                        cofs[q] = __shfl_up_sync(FULL, inc[q], 1);
+                        if (lane == 0) cofs[q] = V(0);
+                        T[q] = __shfl_sync(FULL, inc[q], kBChunks64 - 1);
+                    }
                 }
-                V cofs = __shfl_up_sync(FULL, inc, 1);
-                if (lane == 0) cofs = V(0);
-                const V T = __shfl_sync(FULL, inc, kBChunks64 - 1);
-                const V stake = V(lsd.stake);
-                V xv[K], fv[K];
-                ld_k<K>(x, pos0, xv);
+                V xv[2][K], fv[2][K];
+#pragma unroll
+                for (int q = 0; q < 2; q++)
+                    if (q < nj) ld_k<K>(xs[q], pos0, xv[q]);
 #pragma unroll
                 for (int k = 0; k < K; k++) {
                     const int pos = pos0 + k;
@@ -618,35 +664,46 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     const int li1 = l1 & 255, li2 = (l1 >> 8) & 255;
                     const int gs1 = (l1 >> 16) & 255, ge1 = l1 >> 24;
                     const int gs2 = l2 & 255, ge2 = (l2 >> 8) & 255;
-                    // chunk offsets by shuffle (all lanes take part)
-                    const V oe = __shfl_sync(FULL, cofs, ge >> 6);
-                    const V os = __shfl_sync(FULL, cofs, gs > 0 ? (gs - 1) >> 6 : 0);
-                    V val = V(0), fval = V(0);
-                    if (pos < kBLive) {
-                        const V *sc1 = SC + li1 * 48;
-                        const V *sc2 = SC + li2 * 48;
-                        const V T1 = sc1[kBListLen - 1], T2 = sc2[kBListLen - 1];
-                        const V free = ((T - T1) - T2) + xv[k];
-                        if (lsd.kind == kBShowdown) {
-                            const V Pe = oe + I[ge];
-                            const V Ps = gs > 0 ? os + I[gs - 1] : V(0);
-                            const V vg = (Pe + Ps) - T;
-                            const V v1 = (sc1[ge1] + (gs1 > 0 ? sc1[gs1 - 1] : V(0))) - T1;
-                            const V v2 = (sc2[ge2] + (gs2 > 0 ? sc2[gs2 - 1] : V(0))) - T2;
-                            val = mul(stake, (vg - v1) - v2);
-                        } else {
-                            val = mul(lsd.actor == p ? -stake : stake, free);
+                    const int ce = ge >> 6, cs = gs > 0 ? (gs - 1) >> 6 : 0;
+#pragma unroll
+                    for (int q = 0; q < 2; q++) {
+                        if (q >= nj) continue;
+                        // chunk offsets by shuffle (all lanes take part)
+                        const V oe = __shfl_sync(FULL, cofs[q], ce);
+                        const V os = __shfl_sync(FULL, cofs[q], cs);
+                        const V *I = S.I + q * kBRow;
+                        const V *SC = S.SC + q * kBLists * 48;
+                        V val = V(0), fval = V(0);
+                        if (pos < kBLive) {
+                            const V *sc1 = SC + li1 * 48;
+                            const V *sc2 = SC + li2 * 48;
+                            const V T1 = sc1[kBListLen - 1], T2 = sc2[kBListLen - 1];
+                            const V free = ((T[q] - T1) - T2) + xv[q][k];
+                            const V stake = V(lsd[q].stake);
+                            if (lsd[q].kind == kBShowdown) {
+                                const V Pe = oe + I[ge];
+                                const V Ps = gs > 0 ? os + I[gs - 1] : V(0);
+                                const V vg = (Pe + Ps) - T[q];
+                                const V v1 = (sc1[ge1] + (gs1 > 0 ? sc1[gs1 - 1] : V(0))) - T1;
+                                const V v2 = (sc2[ge2] + (gs2 > 0 ? sc2[gs2 - 1] : V(0))) - T2;
+                                val = mul(stake, (vg - v1) - v2);
+                            } else {
+                                val = mul(lsd[q].actor == p ? -stake : stake, free);
+                            }
+                            if (pair[q]) fval = mul(-V(ln[q].stake), free);
                         }
-                        if (pair) fval = mul(-V(ln.stake), free);
+                        xv[q][k] = val;
+                        fv[q][k] = fval;
                     }
-                    xv[k] = val;
-                    fv[k] = fval;
                 }
-                st_k<K>(x, pos0, xv);
-                if (pair) st_k<K>(xf, pos0, fv);
-                j += pair ? 2 : 1;
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    if (q >= nj) continue;
+                    st_k<K>(xs[q], pos0, xv[q]);
+                    if (pair[q]) st_k<K>(xfs[q], pos0, fv[q]);
+                }
+                __syncthreads();  // the next two jobs rewrite buffers 0 and 1
             }
-            __syncthreads();
 
             // ---- bottom-up walk over nodes [bu, end) ----
             for (; bu < end; bu++) {

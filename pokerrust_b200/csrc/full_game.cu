@@ -302,15 +302,28 @@ __global__ void __launch_bounds__(FT) net_in_kernel(const FNode *__restrict__ no
     }
 }
 
-// leaf value of `upd` = network output x pot x the opponent's reach mass
+// leaf value of `upd` = network output x pot x the opponent's reach mass. With zero_sum, the
+// outputs are first shifted by -e/2, e = r0 . v0 + r1 . v1 over the normalised input ranges:
+// true values of a zero-sum subgame have e = 0 (each player's range-weighted value is minus
+// the other's), and the shift restores that, as DeepStack's output layer does.
 __global__ void __launch_bounds__(FT) net_out_kernel(const FNode *__restrict__ nodes, const int *__restrict__ slot_node,
                                                       const float *__restrict__ out, const float *__restrict__ mass,
-                                                      int upd, float *__restrict__ leafV) {
+                                                      const float *__restrict__ rin, int zero_sum, int upd,
+                                                      float *__restrict__ leafV) {
+    __shared__ float red[FT];
     const int j = blockIdx.x;
     const FNode nd = nodes[slot_node[j]];
     const float scale = nd.stake * mass[j * 2 + (1 - upd)];
+    const float *o = out + (size_t)j * kNetIn;
+    float shift = 0.0f;
+    if (zero_sum) {
+        float part = 0.0f;
+        for (int h = threadIdx.x; h < kH; h += FT)
+            part += rin[((size_t)j * 2) * kH + h] * o[h] + rin[((size_t)j * 2 + 1) * kH + h] * o[kH + h];
+        shift = 0.5f * cta_sum(part, red);
+    }
     float *dst = leafV + (size_t)nd.edge * kH;
-    for (int h = threadIdx.x; h < kH; h += FT) dst[h] = out[(size_t)j * kNetIn + upd * kH + h] * scale;
+    for (int h = threadIdx.x; h < kH; h += FT) dst[h] = (o[upd * kH + h] - shift) * scale;
 }
 
 // the next iteration's weight of the average sums (linear averaging: iteration t has weight t)
@@ -350,6 +363,7 @@ struct Game {
     // net-leaf mode
     void *net = nullptr;
     int net_rows = 0;
+    bool zero_sum = false;  // shift the network's outputs to zero sum (net_out_kernel)
     float *d_nin = nullptr, *d_nscal = nullptr, *d_nmass = nullptr, *d_nout = nullptr;
     unsigned long long *d_nboard = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -432,7 +446,8 @@ struct Game {
                                         d_nscal + (size_t)j0 * 2, d_nout + (size_t)j0 * kNetIn, c))
                 return st;
         }
-        net_out_kernel<<<n, FT, 0, stream>>>(d_nodes, d_slots[0], d_nout, d_nmass, player, d_leafV);
+        net_out_kernel<<<n, FT, 0, stream>>>(d_nodes, d_slots[0], d_nout, d_nmass, d_nin, zero_sum ? 1 : 0, player,
+                                             d_leafV);
         e = cudaGetLastError();
         return e == cudaSuccess ? 0 : ffail("net outputs", e);
     }
@@ -696,6 +711,19 @@ int pr_full_set_net(void *game, void *net) {
             (e = cudaMalloc(&g->d_nboard, sizeof(unsigned long long) * n)) != cudaSuccess)
             return ffail("net buffers", e);
     }
+    return 0;
+}
+
+// Net leaves shifted to zero sum (on = 1; see net_out_kernel) or taken as the network gives
+// them (0, the default).
+int pr_full_set_zero_sum(void *game, int on) {
+    Game *g = (Game *)game;
+    if (!g) return 2;
+    if (g->graph) {
+        cudaGraphExecDestroy(g->graph);
+        g->graph = nullptr;
+    }
+    g->zero_sum = on != 0;
     return 0;
 }
 

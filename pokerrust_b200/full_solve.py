@@ -98,6 +98,73 @@ def leaf_ranges(game, n, rng, per_draw=64):
     return np.array(ids), np.stack(out)
 
 
+def harvest(game, leaf_ids):
+    """The current leaf ranges of the game (the reach of its last CFR pass at the leaves with
+    chips behind), normalised per player, for the leaves both players reach."""
+    R = game.reach()
+    ids, out = [], []
+    for v in leaf_ids:
+        m = R[v].astype(np.float64).sum(axis=1)
+        if np.all(m > 1e-9):
+            ids.append(int(v))
+            out.append((R[v] / m[:, None]).astype(np.float32))
+    return np.array(ids, np.int64), np.stack(out)
+
+
+def label_states(nodes, ids, ranges, iterations):
+    """Training states for leaves `ids` with the given ranges, valued by the river solver."""
+    pick = nodes[ids]
+    boards = pick["board"].astype(np.uint64)
+    pots = pick["stake"].astype(np.float32)
+    stacks = pick["stack"].astype(np.float32)
+    values, solve_s = river_values(boards, ranges, pots, stacks, iterations)
+    scalars = np.stack([pots / 200.0, stacks / (10.0 * pots)], axis=1).astype(np.float32)
+    return dict(boards=boards, ranges=np.asarray(ranges, np.float32), scalars=scalars, values=values, pots=pots,
+                stacks=stacks, solve_s=solve_s)
+
+
+def merge(a, b):
+    out = {k: np.concatenate([a[k], b[k]]) for k in ("boards", "ranges", "scalars", "values", "pots", "stacks")}
+    out["solve_s"] = a["solve_s"] + b["solve_s"]
+    return out
+
+
+def refine(g, net, spec, data, rounds, iterations, check, river_iterations, epochs, seed, zero_sum, held):
+    """On-policy refinement: `rounds` times, run the net-leaf solve for `iterations`
+    iterations, take the leaf ranges it visits every `check` iterations, value them with the
+    river solver, add them to the training data and train on. The network is then trained on
+    the ranges that CFR with its own leaf values reaches, not only on random profiles.
+    Returns the data, the training-set mask and the per-round counts and seconds."""
+    import torch
+    nodes, _, _, _ = P.full_tree(spec)
+    leaf_ids = g.batch_leaves(0)
+    log = []
+    for r in range(rounds):
+        t0 = time.perf_counter()
+        g.reset()
+        g.set_net(net)
+        g.set_zero_sum(zero_sum)
+        ids, rr = [], []
+        done = 0
+        while done < iterations:
+            g.iterate(check)
+            done += check
+            i, x = harvest(g, leaf_ids)
+            ids.append(i)
+            rr.append(x)
+        g.set_net(None)
+        new = label_states(nodes, np.concatenate(ids), np.concatenate(rr), river_iterations)
+        data = merge(data, new)
+        held = np.concatenate([held, np.zeros(len(new["boards"]), bool)])
+        label_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        T.train(net, data, np.flatnonzero(~held), epochs, 256, 1e-3 * 0.5 ** (r + 1), seed + 100 + r)
+        torch.cuda.synchronize()
+        log.append({"round": r + 1, "states": int(len(new["boards"])), "total": int(len(data["boards"])),
+                    "harvest_label_s": label_s, "train_s": time.perf_counter() - t0})
+    return data, held, log
+
+
 def river_specs(boards, ranges, pots, stacks):
     """The 48 river subgames of each turn-leaf state, in card order: specs [n * 48] and
     ranges [n * 48][2][1326] (the state's ranges with the river card's hands zeroed)."""
@@ -188,7 +255,7 @@ def leaf_dataset(spec, n, seed, iterations, game=None):
 
 
 def run(config, seed, iterations, check, target_pct, samples, river_iterations, epochs, resolve, net_iterations,
-        plain_only=False):
+        plain_only=False, refine_rounds=0, refine_iterations=200, zero_sum=False):
     import torch
     spec, ranges = seeded_game(config, seed)
     pot = CONFIGS[config]["pot"]
@@ -221,11 +288,15 @@ def run(config, seed, iterations, check, target_pct, samples, river_iterations, 
     curve = T.train(net, data, np.flatnonzero(~held), epochs, 256, 1e-3, seed)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
+    refine_log = []
+    if refine_rounds:
+        data, held, refine_log = refine(g, net, spec, data, refine_rounds, refine_iterations, 25, river_iterations,
+                                        epochs, seed, zero_sum, held)
     te = np.flatnonzero(held)
     pred = T.predict(net, data, te)
     want = data["values"][te]
     game_half = te < samples // 2
-    out["network"] = {"samples": samples, "river_iterations": river_iterations, "generation_s": gen_s,
+    out["network"] = {"samples": samples, "refine": refine_log, "zero_sum": zero_sum, "river_iterations": river_iterations, "generation_s": gen_s,
                       "epochs": epochs, "train_s": train_s, "final_loss": curve[-1] if curve else None,
                       "held_out_mse": {"network_game_ranges": T.mse(pred[game_half], want[game_half]),
                                        "zero_game_ranges": T.mse(0 * want[game_half], want[game_half]),
@@ -233,6 +304,7 @@ def run(config, seed, iterations, check, target_pct, samples, river_iterations, 
                                        "zero_random_ranges": T.mse(0 * want[~game_half], want[~game_half])}}
     g.reset()
     g.set_net(net)
+    g.set_zero_sum(zero_sum)
     pts, reached = trajectory(g, net_iterations, check, pot, target_pct, resolve=resolve)
     out["net_leaf"] = {"trajectory": pts, "reached": reached, "resolve_iterations": resolve}
     g.set_net(None)
@@ -254,9 +326,14 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--resolve", type=int, default=200)
     ap.add_argument("--plain-only", action="store_true", help="skip the network and the net-leaf solve")
+    ap.add_argument("--refine", type=int, default=0,
+                    help="rounds of on-policy refinement (leaf ranges of the net-leaf solve, valued and added)")
+    ap.add_argument("--refine-iterations", type=int, default=200)
+    ap.add_argument("--zero-sum", action="store_true", help="shift the network's leaf values to zero sum")
     a = ap.parse_args(argv)
     print(json.dumps(run(a.config, a.seed, a.iterations, a.check, a.target, a.samples, a.river_iterations,
-                         a.epochs, a.resolve, a.net_iterations, a.plain_only)), flush=True)
+                         a.epochs, a.resolve, a.net_iterations, a.plain_only, a.refine, a.refine_iterations,
+                         a.zero_sum)), flush=True)
     return 0
 
 

@@ -234,6 +234,8 @@ def lib():
         L.pr_full_free.argtypes = [vp]
         L.pr_full_shape.restype = i32
         L.pr_full_shape.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.pr_full_set_zero_sum.restype = i32
+        L.pr_full_set_zero_sum.argtypes = [vp, i32]
         L.pr_full_set_net.restype = i32
         L.pr_full_set_net.argtypes = [vp, vp]
         L.pr_full_pass.restype = i32
@@ -889,6 +891,10 @@ class FullGame:
         """Net-leaf mode with a ValueNet, or plain river subgames (None)."""
         self._net = net
         _check(lib().pr_full_set_net(self.ptr, net.ptr if net is not None else None), "pr_full_set_net")
+
+    def set_zero_sum(self, on=True):
+        """pr_full_set_zero_sum: net leaves shifted so both players' range-weighted values cancel."""
+        _check(lib().pr_full_set_zero_sum(self.ptr, int(bool(on))), "pr_full_set_zero_sum")
 
     def tune(self):
         """Autotunes the river-subgame batches; per-pass ms of each batch's two classes."""
