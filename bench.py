@@ -222,12 +222,16 @@ def batch_section(P, rank, peak, cpu_threads, with_cpu, traces):
     b3.enable_average()
     for c in range(2):
         b3.set_config(c, cfgs[c]["K"], cfgs[c]["per_sm"], cfgs[c]["order"])
+    t1 = time.perf_counter()
     b3.iterate(BATCH_ITERATIONS)
+    t2 = time.perf_counter()
     b3.all_rows(1, host_avg)
-    e2e_s = time.perf_counter() - t0
+    t3 = time.perf_counter()
+    e2e_s = t3 - t0
     b3.close()
     out["e2e"] = {"solve_s": e2e_s, "iterations": BATCH_ITERATIONS,
                   "iteration_ms": e2e_s / BATCH_ITERATIONS * 1e3,
+                  "setup_s": t1 - t0, "iterate_s": t2 - t1, "download_s": t3 - t2,
                   "h2d_bytes": int(specs.nbytes + ranges.nbytes), "d2h_bytes": int(host_avg.nbytes),
                   "note": "batch set-up, 500 CFR iterations and the download of every average sum"}
     if with_cpu:

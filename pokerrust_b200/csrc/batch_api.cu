@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <thread>
 #include <numeric>
 #include <vector>
 
@@ -72,12 +73,14 @@ struct Batch {
     void *d_root = nullptr;  // [count][kBRow] doubles, lazily
     void *d_child = nullptr; // [count][8][kBRow] doubles, lazily
     double *d_hands = nullptr;  // [count][10][1326] doubles, lazily: results in hand order for host copies
+    double *h_pinned = nullptr;  // pinned host copy of d_hands, lazily (the adjoint's host outputs)
     std::vector<uint16_t> hand;  // [count][kBRow] colex hand of each position
     cudaGraphExec_t graph = nullptr;
     bool graph_avg = false, graph_failed = false;
 
     ~Batch() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (h_pinned) cudaFreeHost(h_pinned);
         if (stream) cudaStreamSynchronize(stream);
         for (void *p : {(void *)d_subs, (void *)d_nodes, (void *)d_packs, (void *)d_ranges, (void *)d_ranges64,
                         (void *)d_regrets, (void *)d_avg, (void *)d_order, (void *)d_head, (void *)d_err, d_sum,
@@ -675,10 +678,39 @@ int pr_batch_value_grad(void *batch, int use_average, double *d_r0, double *d_r1
     double *h0 = b->d_hands, *h1 = h0 + n, *hs = h1 + n;
     if (int st = value_grad_device(b, use_average, d_r0 ? h0 : nullptr, d_r1 ? h1 : nullptr, d_sigma ? hs : nullptr))
         return st;
+    // device -> pinned host in one copy, then pinned -> the caller's arrays on host threads
+    // (pageable destinations would otherwise be copied through the driver's small staging)
     cudaError_t e = cudaSuccess;
-    if (d_r0) e = cudaMemcpy(d_r0, h0, sizeof(double) * n, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && d_r1) e = cudaMemcpy(d_r1, h1, sizeof(double) * n, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && d_sigma) e = cudaMemcpy(d_sigma, hs, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost);
+    if (!b->h_pinned) e = cudaHostAlloc(&b->h_pinned, sizeof(double) * 10 * n, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        b->h_pinned = nullptr;
+        return bfail("pinned staging allocation", e);
+    }
+    e = cudaMemcpyAsync(b->h_pinned, b->d_hands, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bfail("adjoint copy", e);
+    struct Part { double *dst; const double *src; size_t n; };
+    std::vector<Part> parts;
+    if (d_r0) parts.push_back({d_r0, b->h_pinned, n});
+    if (d_r1) parts.push_back({d_r1, b->h_pinned + n, n});
+    if (d_sigma) parts.push_back({d_sigma, b->h_pinned + 2 * n, 8 * n});
+    size_t total = 0;
+    for (auto &q : parts) total += q.n;
+    const int threads = (int)std::min<size_t>(16, std::max<size_t>(1, std::min<unsigned>(std::thread::hardware_concurrency(), total / (1u << 18))));
+    auto work = [&](int t) {
+        // thread t copies its share [total * t / threads, total * (t + 1) / threads) of the parts
+        const size_t lo = total * t / threads, hi = total * (t + 1) / threads;
+        size_t at = 0;
+        for (auto &q : parts) {
+            const size_t a = std::max(lo, at), z = std::min(hi, at + q.n);
+            if (a < z) memcpy(q.dst + (a - at), q.src + (a - at), sizeof(double) * (z - a));
+            at += q.n;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; t++) pool.emplace_back(work, t);
+    work(0);
+    for (auto &th : pool) th.join();
     return e == cudaSuccess ? 0 : bfail("adjoint copy", e);
 }
 
