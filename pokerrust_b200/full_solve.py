@@ -31,6 +31,10 @@ CONFIGS = {
     "small": dict(pot=10.0, stack=100.0, fracs=(0.75,), allin=True, raises=1),
     # the large game's sizes (0.33, 0.75, 1.5 pot, all-in) and 50x stacks, one bet or raise per street
     "large": dict(pot=10.0, stack=500.0, fracs=(0.33, 0.75, 1.5), allin=True, raises=1),
+    # the same sizes with two bets or raises on the flop and one on the turn: 548,016 river
+    # subgames, about 150 GB of solver state, the largest of these games that fits one B200
+    # (two raises on both streets: 1.87 M subgames, about 490 GB; three: 8.9 M, 1.6 TB)
+    "large2": dict(pot=10.0, stack=500.0, fracs=(0.33, 0.75, 1.5), allin=True, raises=2, turn_raises=1),
 }
 
 
@@ -49,7 +53,7 @@ def seeded_game(config, seed):
     ranges /= ranges.sum(axis=1, keepdims=True)
     spec = P.full_spec(flop, c["pot"], c["stack"], flop_fracs=c["fracs"], flop_allin=c["allin"],
                        flop_raises=c["raises"], turn_fracs=c["fracs"], turn_allin=c["allin"],
-                       turn_raises=c["raises"], river_sizes=D.RIVER_SIZES, river_raises=D.RIVER_RAISES)
+                       turn_raises=c.get("turn_raises", c["raises"]), river_sizes=D.RIVER_SIZES, river_raises=D.RIVER_RAISES)
     return spec, ranges
 
 
