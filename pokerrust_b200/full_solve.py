@@ -102,6 +102,37 @@ def leaf_ranges(game, n, rng, per_draw=64):
     return np.array(ids), np.stack(out)
 
 
+def hybrid_trajectory(game, net, net_iterations, iterations, check, pot, target_pct, zero_sum):
+    """Net leaves first, then the plain river traversal as the fallback: `net_iterations`
+    CFR iterations with network leaves, then plain iterations (the river subgames start from
+    zero regrets; flop and turn regrets and the average sums carry over), up to `iterations`
+    in all. Exploitability is the plain game's own FP64 measure of the average strategies,
+    whose river part comes from the river subgames; solver seconds include the net phase."""
+    game.reset()
+    game.set_net(net)
+    game.set_zero_sum(zero_sum)
+    t0 = time.perf_counter()
+    game.iterate(net_iterations)
+    solver_s = time.perf_counter() - t0
+    game.set_net(None)
+    points, reached = [], None
+    done = net_iterations
+    while done < iterations:
+        n = min(check, iterations - done)
+        t0 = time.perf_counter()
+        game.iterate(n)
+        solver_s += time.perf_counter() - t0
+        done += n
+        t0 = time.perf_counter()
+        _, _, ex = game.exploitability()
+        pct = 100.0 * ex / pot
+        points.append({"iterations": done, "solver_s": solver_s, "pct_pot": pct,
+                       "measure_s": time.perf_counter() - t0})
+        if reached is None and pct <= target_pct:
+            reached = {"iterations": done, "solver_s": solver_s}
+    return points, reached
+
+
 def harvest(game, leaf_ids):
     """The current leaf ranges of the game (the reach of its last CFR pass at the leaves with
     chips behind), normalised per player, for the leaves both players reach."""
@@ -259,7 +290,7 @@ def leaf_dataset(spec, n, seed, iterations, game=None):
 
 
 def run(config, seed, iterations, check, target_pct, samples, river_iterations, epochs, resolve, net_iterations,
-        plain_only=False, refine_rounds=0, refine_iterations=200, zero_sum=False):
+        plain_only=False, refine_rounds=0, refine_iterations=200, zero_sum=False, hybrid=()):
     import torch
     spec, ranges = seeded_game(config, seed)
     pot = CONFIGS[config]["pot"]
@@ -312,6 +343,11 @@ def run(config, seed, iterations, check, target_pct, samples, river_iterations, 
     pts, reached = trajectory(g, net_iterations, check, pot, target_pct, resolve=resolve)
     out["net_leaf"] = {"trajectory": pts, "reached": reached, "resolve_iterations": resolve}
     g.set_net(None)
+    out["hybrid"] = []
+    for h in hybrid:
+        hp, hr = hybrid_trajectory(g, net, h, iterations, check // 2, pot, target_pct, zero_sum)
+        out["hybrid"].append({"net_iterations": h, "trajectory": hp, "reached": hr})
+    g.set_net(None)
     g.close()
     net.close()
     return out
@@ -334,10 +370,12 @@ def main(argv=None):
                     help="rounds of on-policy refinement (leaf ranges of the net-leaf solve, valued and added)")
     ap.add_argument("--refine-iterations", type=int, default=200)
     ap.add_argument("--zero-sum", action="store_true", help="shift the network's leaf values to zero sum")
+    ap.add_argument("--hybrid", default="", help="comma-separated net-leaf iteration counts after which the solve "
+                                                 "continues with plain river subgames (e.g. 50,100)")
     a = ap.parse_args(argv)
     print(json.dumps(run(a.config, a.seed, a.iterations, a.check, a.target, a.samples, a.river_iterations,
                          a.epochs, a.resolve, a.net_iterations, a.plain_only, a.refine, a.refine_iterations,
-                         a.zero_sum)), flush=True)
+                         a.zero_sum, tuple(int(x) for x in a.hybrid.split(",") if x))), flush=True)
     return 0
 
 
