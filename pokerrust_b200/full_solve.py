@@ -57,9 +57,11 @@ def seeded_game(config, seed):
     return spec, ranges
 
 
-def trajectory(game, iterations, check, pot, target_pct, resolve=0):
+def trajectory(game, iterations, check, pot, target_pct, resolve=0, resolve_too=0):
     """CFR in steps of `check` iterations; after each step the FP64 exploitability (solver
-    seconds exclude the measurement)."""
+    seconds exclude the measurement), and with resolve_too > 0 also the same strategies
+    measured with their river subgames re-solved for that many iterations (the measure the
+    net-leaf form needs)."""
     points, reached = [], None
     done, solver_s = 0, 0.0
     while done < iterations:
@@ -73,9 +75,21 @@ def trajectory(game, iterations, check, pot, target_pct, resolve=0):
         pct = 100.0 * ex / pot
         points.append({"iterations": done, "solver_s": solver_s, "pct_pot": pct,
                        "measure_s": time.perf_counter() - t0})
+        if resolve_too:
+            _, _, ex2 = game.exploitability(resolve_iterations=resolve_too)
+            points[-1]["pct_pot_resolved"] = 100.0 * ex2 / pot
         if reached is None and pct <= target_pct:
             reached = {"iterations": done, "solver_s": solver_s}
     return points, reached
+
+
+def time_to_levels(points, key, levels):
+    """Solver seconds at which a trajectory first reaches each exploitability level."""
+    out = {}
+    for lv in levels:
+        hit = next((p for p in points if p[key] <= lv), None)
+        out[str(lv)] = None if hit is None else round(hit["solver_s"], 4)
+    return out
 
 
 def leaf_ranges(game, n, rng, per_draw=64):
@@ -302,7 +316,7 @@ def run(config, seed, iterations, check, target_pct, samples, river_iterations, 
     g.tune()
     out["game"] = {"nodes": g.nodes, "edges": g.edges, "leaves": g.leaves, "river_subgames": g.bet_subgames,
                    "allin_subgames": g.allin_subgames, "setup_s": setup_s, "tune_s": time.perf_counter() - t0}
-    pts, reached = trajectory(g, iterations, check, pot, target_pct)
+    pts, reached = trajectory(g, iterations, check, pot, target_pct, resolve_too=0 if plain_only else resolve)
     out["plain"] = {"trajectory": pts, "reached": reached}
     # the same strategies measured the net-leaf way (rivers re-solved under the flop and
     # turn strategies), to calibrate that measurement
@@ -342,6 +356,13 @@ def run(config, seed, iterations, check, target_pct, samples, river_iterations, 
     g.set_zero_sum(zero_sum)
     pts, reached = trajectory(g, net_iterations, check, pot, target_pct, resolve=resolve)
     out["net_leaf"] = {"trajectory": pts, "reached": reached, "resolve_iterations": resolve}
+    # both forms under the same measure (rivers re-solved under the flop and turn strategies)
+    levels = (4.0, 3.0, 2.5, 2.0, 1.5, 1.0)
+    plain_t = time_to_levels(out["plain"]["trajectory"], "pct_pot_resolved", levels)
+    net_t = time_to_levels(pts, "pct_pot", levels)
+    out["same_measure_seconds_to_pct_pot"] = {
+        "plain": plain_t, "net_leaf": net_t,
+        "speedup": {k: (round(plain_t[k] / net_t[k], 2) if plain_t[k] and net_t[k] else None) for k in plain_t}}
     g.set_net(None)
     out["hybrid"] = []
     for h in hybrid:
