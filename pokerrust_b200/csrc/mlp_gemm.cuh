@@ -38,7 +38,10 @@ using bf16 = cutlass::bfloat16_t;
 
 constexpr int kBM = 128;
 constexpr int kBK = 64;
-constexpr int kThreads = 128;
+// 16 warps: warp 0 streams tiles, warp 1 issues the MMAs, and all 16 run the epilogue, the
+// four warpgroups taking every fourth 32-column chunk (warp w reads TMEM lanes
+// 32 (w % 4) .. 32 (w % 4) + 31), so that transcendental epilogues have warps to overlap
+constexpr int kThreads = 512;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // give up on an mbarrier after 2 s
 
 // Wait limit and a load to leave out, for the test of the bounded waits: with withhold_k =
@@ -227,7 +230,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     __syncwarp();
 
-    // epilogue: all four warps, TMEM rows -> registers -> global, 32 columns at a time
+    // epilogue: all warps, TMEM rows -> registers -> global, 32 columns at a time; warpgroup g
+    // takes chunks g, g + 4, ...
     const bool acc_ok = __all_sync(0xffffffffu, bar_wait(&ss.acc, 0, hooks.wait_ns));  // tcgen05.ld is warp-collective
     if (!acc_ok && lane == 0) atomicOr(err, kErrEpilogue);
     tmem_fence_after_sync();
@@ -236,11 +240,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         Tensor crd = tCcC(make_coord(_, _), 0, 0);    // (BM, BN) tile coordinates
         const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
 #pragma unroll 1
-        for (int j = 0; j < BN / 32; j++) {
+        for (int j = warp / 4; j < BN / 32; j += kThreads / 128) {
             Tensor acc_j = local_tile(acc, Shape<Int<kBM>, _32>{}, make_coord(0, j));
             Tensor crd_j = local_tile(crd, Shape<Int<kBM>, _32>{}, make_coord(0, j));
             auto t2r = make_tmem_copy(SM100_TMEM_LOAD_32dp32b32x{}, acc_j);
-            ThrCopy thr = t2r.get_slice(threadIdx.x);
+            ThrCopy thr = t2r.get_slice(threadIdx.x % 128);
             Tensor src = thr.partition_S(acc_j);
             Tensor pos = thr.partition_D(crd_j);
             Tensor reg = make_tensor<float>(shape(pos));
@@ -273,12 +277,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 // one tile runs while the main loop of the next fills the other accumulator. Roles, 256
 // threads: warp 0 streams tiles with TMA through the stage ring (stage and phase counters
 // continue across tiles), warp 1 issues tcgen05.mma and commits each finished accumulator,
-// warps 4-7 (one warpgroup: warp 4 + i reads TMEM lanes 32i..32i+31) drain accumulators with
+// warps 4-19 (four warpgroups; warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31, and
+// warpgroup g takes every fourth 32-column chunk from chunk g) drain accumulators with
 // tcgen05.ld through the same epilogues as gemm_kernel; warps 2-3 only take part in set-up and
 // teardown. Every wait is bounded: a role whose wait runs out records its error bit and raises
 // `abort`, the others stop at their next tile, and the teardown waits (bounded) for copies
 // and MMAs in flight before tensor memory is freed.
-constexpr int kPThreads = 256;
+constexpr int kPThreads = 640;
+constexpr int kPEpiWarps = 16;
 
 template <int BN, UMMA::Major MA, UMMA::Major MB>
 struct PCfg {
@@ -317,7 +323,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
         }
         for (int b = 0; b < 2; b++) {
             cutlass::arch::ClusterBarrier::init(&ps.accf[b], 1);
-            cutlass::arch::ClusterBarrier::init(&ps.acce[b], 4);
+            cutlass::arch::ClusterBarrier::init(&ps.acce[b], kPEpiWarps);
         }
         cutlass::arch::ClusterBarrier::init(&ps.fin, 1);
         ps.abort = 0;
@@ -420,7 +426,8 @@ __global__ void __launch_bounds__(kPThreads, 1)
         cutlass::arch::umma_arrive(&ps.fin);
         __syncwarp();
     } else if (warp >= 4) {
-        const int et = threadIdx.x - 128;  // thread within the epilogue warpgroup
+        const int et = threadIdx.x % 128;  // thread within its epilogue warpgroup
+        const int eg = (warp - 4) / 4;       // the epilogue warpgroup
         int local = 0;
         for (int t = blockIdx.x; t < tiles; t += gridDim.x, local++) {
             if (__any_sync(0xffffffffu, *abort_flag)) break;
@@ -438,7 +445,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
             Tensor crd = tCcC(make_coord(_, _), 0, 0);
             const int m0 = mt * kBM, n0 = nt * BN;
 #pragma unroll 1
-            for (int j = 0; j < BN / 32; j++) {
+            for (int j = eg; j < BN / 32; j += kPEpiWarps / 4) {
                 Tensor acc_j = local_tile(acc, Shape<Int<kBM>, _32>{}, make_coord(0, j));
                 Tensor crd_j = local_tile(crd, Shape<Int<kBM>, _32>{}, make_coord(0, j));
                 auto t2r = make_tmem_copy(SM100_TMEM_LOAD_32dp32b32x{}, acc_j);
