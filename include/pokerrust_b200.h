@@ -271,8 +271,9 @@ int pr_batch_get_all(void *batch, int which, float *out);
  * thread (2, 3, 4), resident CTAs per SM, queue order (0 most work first, 1 input order). */
 int pr_batch_config(void *batch, int c, int *K, int *per_sm, int *order, int *count);
 int pr_batch_set_config(void *batch, int c, int K, int per_sm, int order);
-/* Autotuner: times every configuration per class and keeps the fastest; the solver state
- * is restored afterwards. ms_out[2]: the chosen per-pass times. */
+/* Autotuner: times every configuration per class on the batch's first (up to) 8192
+ * subgames and keeps the fastest; their solver state is restored afterwards. ms_out[2]: the
+ * chosen configurations' per-pass times on those subgames. */
 int pr_batch_tune(void *batch, double *ms_out);
 /* Algorithmic HBM bytes of one CFR iteration (roofline numerator). */
 double pr_batch_iteration_bytes(void *batch);
@@ -382,8 +383,10 @@ int pr_full_iterate(void *game, int iterations);
 /* FP64 best responses to the average strategies over the whole game and the exploitability
  * (br0 + br1) / 2 per unit of joint range mass, in chips. resolve_iterations > 0 first
  * re-solves the river subgames of the leaves with chips behind from zero under the current
- * average flop and turn strategies (for net-leaf strategies, which stop at the turn); this
- * replaces those subgames' regrets and average sums. */
+ * average flop and turn strategies (for net-leaf strategies, which stop at the turn). In
+ * net-leaf mode this replaces those subgames' regrets and average sums; in plain mode they are
+ * kept aside (a device copy of their rows) and restored, so measuring leaves the solve as it
+ * was. */
 int pr_full_exploitability(void *game, int resolve_iterations, double *br0, double *br1, double *expl);
 /* Device state: which 0 regrets / 1 average sums [edges][1326] f32; 2 reach [nodes][2][1326],
  * 3 leaf values [leaves][1326], 4 node values [nodes][1326] (f32, last CFR pass); 5, 6, 7

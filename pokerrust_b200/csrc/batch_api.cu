@@ -321,6 +321,15 @@ int batch_run_pass(void *batch, int mode, int player, int fp64, int use_average,
     return b->pass(mode, player, fp64, use_average, root_out, nullptr, slot, nullptr, on);
 }
 
+int batch_rows(void *batch, float **regrets, float **avg, size_t *bytes) {
+    Batch *b = (Batch *)batch;
+    if (!b) return 2;
+    *regrets = b->d_regrets;
+    *avg = b->d_avg;
+    *bytes = (size_t)b->total_edges * kBRow * sizeof(float);
+    return 0;
+}
+
 int batch_clear(void *batch, cudaStream_t on) {
     Batch *b = (Batch *)batch;
     if (!b) return 2;
@@ -873,20 +882,46 @@ int pr_batch_set_config(void *batch, int c, int K, int per_sm, int order) {
 }
 
 // Autotuner: for each shape class, times one CFR pass of every configuration (hands per
-// thread 2/3/4, resident CTAs per SM up to what fits, queue order) on a copy of the
-// current regrets and keeps the fastest; the regrets and sums are restored afterwards, so
-// tuning does not change the solve. Writes the chosen class-0 / class-1 times (ms).
+// thread 2/3/4, resident CTAs per SM up to what fits, queue order) over the class's share of
+// the first (up to) 8192 subgames and keeps the fastest; their regrets and sums are restored
+// afterwards, so tuning does not change the solve. Writes the chosen class-0 / class-1 times
+// (ms per pass over those subgames).
 int pr_batch_tune(void *batch, double *ms_out) {
     Batch *b = (Batch *)batch;
     if (!b) return 2;
-    const size_t rows = (size_t)b->total_edges * kBRow * sizeof(float);
+    // Passes are timed on the first nt subgames only (at most kTuneSubgames): their rows are
+    // contiguous, so only they are saved and restored, and a batch of any size can be tuned
+    // beside its own state.
+    constexpr int kTuneSubgames = 8192;
+    const int nt = std::min(b->count, kTuneSubgames);
+    const int rows_nt = nt < b->count ? b->subs[nt].edge_off : b->total_edges;
+    const size_t rows = (size_t)rows_nt * kBRow * sizeof(float);
     float *save_r = nullptr, *save_a = nullptr;
+    int *tune_order = nullptr;
     cudaError_t e;
     if ((e = cudaMalloc(&save_r, rows)) != cudaSuccess) return bfail("tuning allocation", e);
-    if (b->avg_on && (e = cudaMalloc(&save_a, rows)) != cudaSuccess) {
+    if ((b->avg_on && (e = cudaMalloc(&save_a, rows)) != cudaSuccess) ||
+        (e = cudaMalloc(&tune_order, sizeof(int) * nt)) != cudaSuccess) {
         cudaFree(save_r);
+        cudaFree(save_a);
         return bfail("tuning allocation", e);
     }
+    // the tuning queue: the first nt subgames in the class's queue order; class c starts at
+    // sub_first[c] and holds sub_count[c] of them
+    int sub_first[kClasses], sub_count[kClasses];
+    auto upload_tune_order = [&]() -> int {
+        std::vector<int> full, sub;
+        b->build_order(full);
+        for (int c = 0, at = 0; c < kClasses; c++) {
+            sub_first[c] = (int)sub.size();
+            for (int i = 0; i < b->cls[c].count; i++)
+                if (full[at + i] < nt) sub.push_back(full[at + i]);
+            sub_count[c] = (int)sub.size() - sub_first[c];
+            at += b->cls[c].count;
+        }
+        cudaError_t x = cudaMemcpy(tune_order, sub.data(), sizeof(int) * sub.size(), cudaMemcpyHostToDevice);
+        return x == cudaSuccess ? 0 : bfail("tuning queue upload", x);
+    };
     cudaMemcpyAsync(save_r, b->d_regrets, rows, cudaMemcpyDeviceToDevice, b->stream);
     if (save_a) cudaMemcpyAsync(save_a, b->d_avg, rows, cudaMemcpyDeviceToDevice, b->stream);
     cudaEvent_t t0, t1;
@@ -900,8 +935,6 @@ int pr_batch_tune(void *batch, double *ms_out) {
         }
         ClassCfg keep[kClasses];
         for (int i = 0; i < kClasses; i++) keep[i] = b->cls[i];
-        for (int i = 0; i < kClasses; i++)
-            if (i != c) b->cls[i].count = 0;  // time this class alone
         float best = 1e30f;
         ClassCfg best_cfg = keep[c];
         for (int K : {2, 3, 4}) {
@@ -913,15 +946,22 @@ int pr_batch_tune(void *batch, double *ms_out) {
             if (K == 4 && batch_dense_ctas_per_sm(b->avg_on) >= 3) pers.push_back(3);
             for (int per : pers) {
                 for (int ord = 0; ord < 2; ord++) {
+                    for (int i = 0; i < kClasses; i++) b->cls[i] = keep[i];
                     b->cls[c].K = K;
                     b->cls[c].per_sm = per;
                     b->cls[c].order = ord;
-                    if ((status = b->upload_order())) break;
+                    if ((status = upload_tune_order())) break;
+                    // time this class alone, on its share of the tuning queue
+                    for (int i = 0; i < kClasses; i++) {
+                        b->cls[i].first = sub_first[i];
+                        b->cls[i].count = i == c ? sub_count[i] : 0;
+                    }
+                    if (!b->cls[c].count) break;
                     float ms = 0;
                     for (int rep = 0; rep < 3 && !status; rep++) {
                         cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
                         cudaEventRecord(t0, b->stream);
-                        status = b->pass(kBModeCFR, rep & 1, 0, 0, nullptr, nullptr, 0);
+                        status = b->pass(kBModeCFR, rep & 1, 0, 0, nullptr, nullptr, 0, nullptr, nullptr, tune_order);
                         cudaEventRecord(t1, b->stream);
                         cudaEventSynchronize(t1);
                         float t = 0;
@@ -942,7 +982,7 @@ int pr_batch_tune(void *batch, double *ms_out) {
         b->cls[c].K = best_cfg.K;
         b->cls[c].per_sm = best_cfg.per_sm;
         b->cls[c].order = best_cfg.order;
-        if (ms_out) ms_out[c] = best / 2.0;
+        if (ms_out) ms_out[c] = best < 1e29f ? best / 2.0 : 0.0;
     }
     if (!status) status = b->upload_order();
     cudaMemcpyAsync(b->d_regrets, save_r, rows, cudaMemcpyDeviceToDevice, b->stream);
@@ -952,6 +992,7 @@ int pr_batch_tune(void *batch, double *ms_out) {
     cudaEventDestroy(t1);
     cudaFree(save_r);
     cudaFree(save_a);
+    cudaFree(tune_order);
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;

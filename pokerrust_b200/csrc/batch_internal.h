@@ -31,5 +31,8 @@ int batch_run_pass(void *batch, int mode, int player, int fp64, int use_average,
                    cudaStream_t on);
 // Zeroes the regrets and average sums, queued on stream `on`.
 int batch_clear(void *batch, cudaStream_t on);
+// The batch's regret and average-sum rows (avg null when averages are off) and the bytes of
+// each array.
+int batch_rows(void *batch, float **regrets, float **avg, size_t *bytes);
 
 }  // namespace prb

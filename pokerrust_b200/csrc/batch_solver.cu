@@ -538,15 +538,21 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
             // ---- leaves of the group: opponent weights -> p's values ----
             // A job is a leaf, or a fold by p followed by its sibling call (a showdown): p's
             // actions leave the opponent weights unchanged, so one scan serves both leaves.
-            // Jobs go two at a time (buffers 0 and 1): their scans interleave, and each hand's
-            // tie-group and card-list bounds are unpacked once for both. Every job's
-            // arithmetic is the same as when it runs alone.
-            for (int j = g0; j < g1;) {
+            // Jobs go kJ at a time. With kJ = 2 (buffers 0 and 1) their scans interleave and
+            // each hand's tie-group and card-list bounds are unpacked once for both; the dense
+            // configuration (MINB = 3) runs one job at a time in alternate buffers instead,
+            // which needs no barrier after the values and fits its register cap. Every job's
+            // arithmetic is the same either way.
+            constexpr int kJ = MINB >= 3 ? 1 : 2;
+            int batch_no = 0;
+            for (int j = g0; j < g1; batch_no++) {
+                // buffer of job q of this step
+                auto bufq = [&](int q) { return kJ == 1 ? (batch_no & 1) : q; };
                 bool pair[2] = {false, false};
                 BNode ln[2], lsd[2];
                 V *xs[2], *xfs[2];
                 int nj = 0;
-                while (nj < 2 && j < g1) {
+                while (nj < kJ && j < g1) {
                     ln[nj] = S.tn[S.leaf_node[j]];
                     lsd[nj] = ln[nj];  // the leaf whose kind and stake give the main value
                     if (ln[nj].kind == kBFold && ln[nj].actor == p && j + 1 < g1) {
@@ -567,7 +573,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     if (u < kBChunks64) {
                         V a0[2], v[2];
 #pragma unroll
-                        for (int q = 0; q < 2; q++) {
+                        for (int q = 0; q < kJ; q++) {
                             a0[q] = v[q] = V(0);
                             if (q < nj) {
                                 a0[q] = xs[q][u * 64 + 2 * lane];
@@ -577,20 +583,20 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
 #pragma unroll
                         for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
-                            for (int q = 0; q < 2; q++) {
+                            for (int q = 0; q < kJ; q++) {
                                 const V t = __shfl_up_sync(FULL, v[q], off);
                                 if (lane >= off) v[q] += t;
                             }
                         }
 #pragma unroll
-                        for (int q = 0; q < 2; q++) {
+                        for (int q = 0; q < kJ; q++) {
                             V ex = __shfl_up_sync(FULL, v[q], 1);
                             if (lane == 0) ex = V(0);
                             if (q < nj) {
-                                V *I = S.I + q * kBRow;
+                                V *I = S.I + bufq(q) * kBRow;
                                 I[u * 64 + 2 * lane] = ex + a0[q];
                                 I[u * 64 + 2 * lane + 1] = v[q];
-                                if (lane == 31) S.CT[q * kBChunks + u] = v[q];
+                                if (lane == 31) S.CT[bufq(q) * kBChunks + u] = v[q];
                             }
                         }
                     } else {
@@ -602,7 +608,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                         }
                         V a0[2], v[2];
 #pragma unroll
-                        for (int q = 0; q < 2; q++) {
+                        for (int q = 0; q < kJ; q++) {
                             a0[q] = v[q] = V(0);
                             if (q < nj && lane < kBListLen / 2) {
                                 a0[q] = xs[q][c0];
@@ -612,17 +618,17 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
 #pragma unroll
                         for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
-                            for (int q = 0; q < 2; q++) {
+                            for (int q = 0; q < kJ; q++) {
                                 const V t = __shfl_up_sync(FULL, v[q], off);
                                 if (lane >= off) v[q] += t;
                             }
                         }
 #pragma unroll
-                        for (int q = 0; q < 2; q++) {
+                        for (int q = 0; q < kJ; q++) {
                             V ex = __shfl_up_sync(FULL, v[q], 1);
                             if (lane == 0) ex = V(0);
                             if (q < nj && lane < kBListLen / 2) {
-                                V *SC = S.SC + q * kBLists * 48;
+                                V *SC = S.SC + bufq(q) * kBLists * 48;
                                 SC[li * 48 + 2 * lane] = ex + a0[q];
                                 SC[li * 48 + 2 * lane + 1] = v[q];
                             }
@@ -636,17 +642,17 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                 {
                     V inc[2];
 #pragma unroll
-                    for (int q = 0; q < 2; q++) inc[q] = (q < nj && lane < kBChunks64) ? S.CT[q * kBChunks + lane] : V(0);
+                    for (int q = 0; q < kJ; q++) inc[q] = (q < nj && lane < kBChunks64) ? S.CT[bufq(q) * kBChunks + lane] : V(0);
 #pragma unroll
                     for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
-                        for (int q = 0; q < 2; q++) {
+                        for (int q = 0; q < kJ; q++) {
                             const V t = __shfl_up_sync(FULL, inc[q], off);
                             if (lane >= off) inc[q] += t;
                         }
                     }
 #pragma unroll
-                    for (int q = 0; q < 2; q++) {
+                    for (int q = 0; q < kJ; q++) {
                         cofs[q] = __shfl_up_sync(FULL, inc[q], 1);
                         if (lane == 0) cofs[q] = V(0);
                         T[q] = __shfl_sync(FULL, inc[q], kBChunks64 - 1);
@@ -654,7 +660,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                 }
                 V xv[2][K], fv[2][K];
 #pragma unroll
-                for (int q = 0; q < 2; q++)
+                for (int q = 0; q < kJ; q++)
                     if (q < nj) ld_k<K>(xs[q], pos0, xv[q]);
 #pragma unroll
                 for (int k = 0; k < K; k++) {
@@ -666,13 +672,13 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     const int gs2 = l2 & 255, ge2 = (l2 >> 8) & 255;
                     const int ce = ge >> 6, cs = gs > 0 ? (gs - 1) >> 6 : 0;
 #pragma unroll
-                    for (int q = 0; q < 2; q++) {
+                    for (int q = 0; q < kJ; q++) {
                         if (q >= nj) continue;
                         // chunk offsets by shuffle (all lanes take part)
                         const V oe = __shfl_sync(FULL, cofs[q], ce);
                         const V os = __shfl_sync(FULL, cofs[q], cs);
-                        const V *I = S.I + q * kBRow;
-                        const V *SC = S.SC + q * kBLists * 48;
+                        const V *I = S.I + bufq(q) * kBRow;
+                        const V *SC = S.SC + bufq(q) * kBLists * 48;
                         V val = V(0), fval = V(0);
                         if (pos < kBLive) {
                             const V *sc1 = SC + li1 * 48;
@@ -697,12 +703,12 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     }
                 }
 #pragma unroll
-                for (int q = 0; q < 2; q++) {
+                for (int q = 0; q < kJ; q++) {
                     if (q >= nj) continue;
                     st_k<K>(xs[q], pos0, xv[q]);
                     if (pair[q]) st_k<K>(xfs[q], pos0, fv[q]);
                 }
-                __syncthreads();  // the next two jobs rewrite buffers 0 and 1
+                if constexpr (kJ == 2) __syncthreads();  // the next two jobs rewrite buffers 0 and 1
             }
 
             // ---- bottom-up walk over nodes [bu, end) ----

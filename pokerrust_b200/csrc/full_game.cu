@@ -504,6 +504,38 @@ constexpr int kMaxFullNodes = 1 << 20;
 
 using namespace prb;
 
+namespace {
+// pr_full_exploitability's measurement: optional river re-solve, then the FP64 best responses.
+int full_exploitability(Game *g, int resolve_iterations, double *br0, double *br1, double *expl) {
+    if (resolve_iterations > 0 && g->batch[0]) {
+        if (int st = g->down<float>(g->d_R, g->d_avg, 1)) return st;
+        const BatchView &v = g->view[0];
+        scatter_kernel<float><<<v.count, FT, 0, g->stream>>>(v.packs, g->d_R, g->d_slots[0], v.ranges);
+        if (int st = batch_clear(g->batch[0], g->stream)) return st;
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+        if (e != cudaSuccess) return ffail("re-solve setup", e);
+        if (int st = pr_batch_iterate(g->batch[0], resolve_iterations)) return st;
+    }
+    double br[2];
+    for (int p = 0; p < 2; p++) {
+        if (int st = g->down<double>(g->d_R64, g->d_avg, 1)) return st;
+        for (int b = 0; b < 2; b++)
+            if (int st = g->rivers<double>(b, kBModeBR, p, 1, g->d_R64, g->d_leafV64)) return st;
+        if (int st = g->up<double, kUpBR>(p, g->d_R64, g->d_V64, g->d_leafV64, g->d_avg, 1)) return st;
+        root_sum_kernel<<<1, FT, 0, g->stream>>>(g->d_V64, g->d_init, p, g->d_sum);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&br[p], g->d_sum, sizeof(double), cudaMemcpyDeviceToHost, g->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+        if (e != cudaSuccess) return ffail("best response", e);
+    }
+    if (br0) *br0 = br[0];
+    if (br1) *br1 = br[1];
+    if (expl) *expl = (br[0] + br[1]) / 2.0 / g->joint;
+    return 0;
+}
+}  // namespace
+
 extern "C" {
 
 int pr_full_tree(const pr_full_spec *spec, void *nodes_out, int max_nodes, int *num_nodes, int *num_edges,
@@ -804,38 +836,40 @@ int pr_full_iterate(void *game, int iterations) {
 // response), and exploitability = (BR0 + BR1) / 2 per unit of joint range mass, in chips.
 // resolve_iterations > 0 first re-solves the river subgames of the leaves with chips behind
 // from zero, for that many CFR iterations, under the reach of the current average flop and
-// turn strategies (the net-leaf mode's strategies stop at the turn); their previous regrets
-// and average sums are replaced.
+// turn strategies (the net-leaf mode's strategies stop at the turn). In net-leaf mode their
+// previous regrets and average sums are replaced; in plain mode, where they are part of the
+// solve, they are kept aside and restored afterwards.
 int pr_full_exploitability(void *game, int resolve_iterations, double *br0, double *br1, double *expl) {
     Game *g = (Game *)game;
     if (!g || resolve_iterations < 0) return 2;
-    if (resolve_iterations > 0 && g->batch[0]) {
-        if (int st = g->down<float>(g->d_R, g->d_avg, 1)) return st;
-        const BatchView &v = g->view[0];
-        scatter_kernel<float><<<v.count, FT, 0, g->stream>>>(v.packs, g->d_R, g->d_slots[0], v.ranges);
-        if (int st = batch_clear(g->batch[0], g->stream)) return st;
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-        if (e != cudaSuccess) return ffail("re-solve setup", e);
-        if (int st = pr_batch_iterate(g->batch[0], resolve_iterations)) return st;
+    // In plain mode the river subgames belong to the solve: their rows are kept aside during
+    // the re-solve and put back afterwards, so that measuring does not change the solve.
+    float *keep = nullptr, *rows_r = nullptr, *rows_a = nullptr;
+    size_t row_bytes = 0;
+    if (resolve_iterations > 0 && g->batch[0] && !g->net) {
+        if (int st = batch_rows(g->batch[0], &rows_r, &rows_a, &row_bytes)) return st;
+        cudaError_t e = cudaMalloc(&keep, row_bytes * (rows_a ? 2 : 1));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(keep, rows_r, row_bytes, cudaMemcpyDeviceToDevice, g->stream);
+        if (e == cudaSuccess && rows_a)
+            e = cudaMemcpyAsync((char *)keep + row_bytes, rows_a, row_bytes, cudaMemcpyDeviceToDevice, g->stream);
+        if (e != cudaSuccess) {
+            cudaFree(keep);
+            return ffail("re-solve: keeping the river rows", e);
+        }
     }
-    double br[2];
-    for (int p = 0; p < 2; p++) {
-        if (int st = g->down<double>(g->d_R64, g->d_avg, 1)) return st;
-        for (int b = 0; b < 2; b++)
-            if (int st = g->rivers<double>(b, kBModeBR, p, 1, g->d_R64, g->d_leafV64)) return st;
-        if (int st = g->up<double, kUpBR>(p, g->d_R64, g->d_V64, g->d_leafV64, g->d_avg, 1)) return st;
-        root_sum_kernel<<<1, FT, 0, g->stream>>>(g->d_V64, g->d_init, p, g->d_sum);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&br[p], g->d_sum, sizeof(double), cudaMemcpyDeviceToHost, g->stream);
+    const int st = full_exploitability(g, resolve_iterations, br0, br1, expl);
+    if (keep) {
+        cudaError_t e = cudaMemcpyAsync(rows_r, keep, row_bytes, cudaMemcpyDeviceToDevice, g->stream);
+        if (e == cudaSuccess && rows_a)
+            e = cudaMemcpyAsync(rows_a, (char *)keep + row_bytes, row_bytes, cudaMemcpyDeviceToDevice, g->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-        if (e != cudaSuccess) return ffail("best response", e);
+        cudaFree(keep);
+        if (e != cudaSuccess) return ffail("re-solve: restoring the river rows", e);
     }
-    if (br0) *br0 = br[0];
-    if (br1) *br1 = br[1];
-    if (expl) *expl = (br[0] + br[1]) / 2.0 / g->joint;
-    return 0;
+    return st;
 }
+
+
 
 // Device state, for tests and checkpoints. which: 0 regrets, 1 average sums ([edges][1326]
 // floats); 2 reach ([nodes][2][1326] floats), 3 leaf values ([leaves][1326] floats),
