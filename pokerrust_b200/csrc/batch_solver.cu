@@ -710,6 +710,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                 }
                 if constexpr (kJ == 2) __syncthreads();  // the next two jobs rewrite buffers 0 and 1
             }
+            if constexpr (kJ == 1) __syncthreads();  // the bottom-up walk reads every leaf's values
 
             // ---- bottom-up walk over nodes [bu, end) ----
             for (; bu < end; bu++) {
