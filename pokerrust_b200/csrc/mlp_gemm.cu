@@ -9,11 +9,27 @@ namespace prb {
 namespace gemm {
 
 // D (f32, leading dimension ldd) = accumulator, rows < rows_live and columns < cols_live.
+// A thread's 32 values that are 32 consecutive columns of one live row inside the live
+// columns, on a 16-byte boundary, go out as eight 16-byte stores; others one by one.
 struct EpiF32 {
     float *D;
     int ldd, rows_live, cols_live;
     template <class R, class P>
     __device__ void operator()(R const &reg, P const &pos, int m0, int n0, int) const {
+        if (size(reg) == 32) {
+            const int mr = get<0>(pos(0)), nr = get<1>(pos(0));
+            bool run = true;
+#pragma unroll
+            for (int i = 1; i < 32; i++) run &= get<0>(pos(i)) == mr && get<1>(pos(i)) == nr + i;
+            const int m = m0 + mr, n = n0 + nr;
+            float *d = D + (size_t)m * ldd + n;
+            if (run && m < rows_live && n + 32 <= cols_live && (reinterpret_cast<uintptr_t>(d) & 15) == 0) {
+                float4 *o = reinterpret_cast<float4 *>(d);
+#pragma unroll
+                for (int q = 0; q < 8; q++) o[q] = make_float4(reg(4 * q), reg(4 * q + 1), reg(4 * q + 2), reg(4 * q + 3));
+                return;
+            }
+        }
 #pragma unroll
         for (int i = 0; i < size(reg); i++) {
             const int m = m0 + get<0>(pos(i)), n = n0 + get<1>(pos(i));
@@ -30,6 +46,19 @@ struct EpiParts {
     template <class R, class P>
     __device__ void operator()(R const &reg, P const &pos, int m0, int n0, int z) const {
         float *d = D + (size_t)z * zstride;
+        if (size(reg) == 32) {
+            const int mr = get<0>(pos(0)), nr = get<1>(pos(0));
+            bool run = true;
+#pragma unroll
+            for (int i = 1; i < 32; i++) run &= get<0>(pos(i)) == mr && get<1>(pos(i)) == nr + i;
+            float *row = d + (size_t)(m0 + mr) * ldd + n0 + nr;
+            if (run && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+                float4 *o = reinterpret_cast<float4 *>(row);
+#pragma unroll
+                for (int q = 0; q < 8; q++) o[q] = make_float4(reg(4 * q), reg(4 * q + 1), reg(4 * q + 2), reg(4 * q + 3));
+                return;
+            }
+        }
 #pragma unroll
         for (int i = 0; i < size(reg); i++) d[(size_t)(m0 + get<0>(pos(i))) * ldd + n0 + get<1>(pos(i))] = reg(i);
     }
