@@ -318,13 +318,13 @@ def run(config, seed, iterations, check, target_pct, samples, river_iterations, 
                    "allin_subgames": g.allin_subgames, "setup_s": setup_s, "tune_s": time.perf_counter() - t0}
     pts, reached = trajectory(g, iterations, check, pot, target_pct, resolve_too=0 if plain_only else resolve)
     out["plain"] = {"trajectory": pts, "reached": reached}
+    if plain_only:
+        g.close()
+        return out
     # the same strategies measured the net-leaf way (rivers re-solved under the flop and
     # turn strategies), to calibrate that measurement
     _, _, ex = g.exploitability(resolve_iterations=resolve)
     out["plain"]["resolved_pct_pot"] = 100.0 * ex / pot
-    if plain_only:
-        g.close()
-        return out
     # the network: data from this game's leaves, then training
     g.reset()
     t0 = time.perf_counter()
