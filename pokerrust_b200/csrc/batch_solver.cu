@@ -4,8 +4,9 @@
 // A CTA takes subgames from a device work queue (atomicAdd on a head counter) until it is
 // empty. For one subgame, the 1081 live hands are held in rank order ("positions"); a
 // thread owns K consecutive positions. The bet tree (pre-order nodes) sits in shared
-// memory. A pass for player p walks the tree twice per thread, with all per-hand state of
-// the open path in registers:
+// memory. A pass for player p walks the tree twice per thread, with the per-hand state of
+// the open path on depth-indexed stacks (thread-local memory; the innermost open node of the
+// bottom-up walk in registers):
 //  * top-down: reach of the opponent (times its range) and of p along the path, from
 //    regret matching (or the average strategy) of the acting player; at every leaf the
 //    opponent weights x(o) go to shared memory;
@@ -399,7 +400,32 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
         for (int k = 0; k < K; k++) root[k] = V(0);
 
         // adds the values v of the child behind edge ie to its parent par, open at depth dp
-        auto deliver = [&](int par, int ie, int dp, const V(&v)[K]) {
+        // The innermost open node of the bottom-up walk keeps its value and strategy scale in
+        // registers (tacc, tsb); the stacks hold the open nodes outside it. Every child's value
+        // goes to its parent, which is always that innermost node.
+        V tacc[K], tsb[K];
+        // between the bottom-up walks of two groups the registers rest in the stack slot of the
+        // innermost open node (slot 0 when none is open: then nothing reads them)
+        auto park = [&]() {
+            const int t = open_top > 0 ? open_top : 0;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                acc[t][k] = tacc[k];
+                Sb[t][k] = tsb[k];
+            }
+        };
+        auto unpark = [&]() {
+            const int t = open_top > 0 ? open_top : 0;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                tacc[k] = acc[t][k];
+                tsb[k] = Sb[t][k];
+            }
+        };
+#pragma unroll
+        for (int k = 0; k < K; k++) tacc[k] = tsb[k] = V(0);
+        park();
+        auto deliver = [&](int par, int ie, const V(&v)[K]) {
             const BNode pq = S.tn[par];
             if (a.child_out && par == 0) {
                 V *co = reinterpret_cast<V *>(a.child_out) + ((size_t)s * 8 + (ie - pq.edge)) * kBRow;
@@ -407,10 +433,10 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
             }
             if (pq.actor != p) {
 #pragma unroll
-                for (int k = 0; k < K; k++) acc[dp][k] = acc[dp][k] + v[k];
+                for (int k = 0; k < K; k++) tacc[k] = tacc[k] + v[k];
             } else if (MODE == kBModeBR) {
 #pragma unroll
-                for (int k = 0; k < K; k++) acc[dp][k] = acc[dp][k] > v[k] ? acc[dp][k] : v[k];
+                for (int k = 0; k < K; k++) tacc[k] = tacc[k] > v[k] ? tacc[k] : v[k];
             } else {
                 // the edge's strategy from its regret (or average) row; CFR adds the child's
                 // value to the regret, which the parent's close turns into the regret update
@@ -422,7 +448,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     ld_k<K>(Src + ro, pos0, sv);
 #pragma unroll
                 for (int k = 0; k < K; k++)
-                    acc[dp][k] = acc[dp][k] + mul(sigma<V>(sv[k], Sb[dp][k]), v[k]);
+                    tacc[k] = tacc[k] + mul(sigma<V>(sv[k], tsb[k]), v[k]);
                 if constexpr (MODE == kBModeCFR) {
                     float r[K];
 #pragma unroll
@@ -438,7 +464,7 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                 const BNode nm = S.tn[m];
                 V v[K];
 #pragma unroll
-                for (int k = 0; k < K; k++) v[k] = acc[open_top][k];
+                for (int k = 0; k < K; k++) v[k] = tacc[k];
                 if (MODE == kBModeCFR && nm.actor == p) {
                     for (int e = 0; e < nm.nchild; e++) {
                         float *row = R + (size_t)(nm.edge + e) * kBRow;
@@ -454,7 +480,12 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
 #pragma unroll
                     for (int k = 0; k < K; k++) root[k] = v[k];
                 } else {
-                    deliver(nm.parent, nm.in_edge, open_top, v);
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        tacc[k] = acc[open_top][k];
+                        tsb[k] = Sb[open_top][k];
+                    }
+                    deliver(nm.parent, nm.in_edge, v);
                 }
             }
         };
@@ -462,6 +493,8 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
             const int g1 = min(L, g0 + group);
             const int end = g1 == L ? N : S.leaf_node[g1];
             // ---- top-down walk over nodes [td, end) ----
+            // Only decision nodes put their reach and strategy scale on the stacks: their
+            // children read them, and nothing reads a leaf's entry.
             for (; td < end; td++) {
                 const BNode nd = S.tn[td];
                 const int d = nd.depth;
@@ -502,11 +535,6 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                         }
                     }
                 }
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    po[d][k] = npo[k];
-                    pp[d][k] = npp[k];
-                }
                 if (nd.kind == kBDecision) {
                     // strategy sums of the node, for its children
                     const bool own = nd.actor == p;
@@ -524,8 +552,11 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     }
                     if (AVG && own) prefetch_rows<K>(A, nd.edge, min(nd.nchild, kPfRows), sub.num_edges, warp, lane);
 #pragma unroll
-                    for (int k = 0; k < K; k++)
+                    for (int k = 0; k < K; k++) {
+                        po[d][k] = npo[k];
+                        pp[d][k] = npp[k];
                         St[d][k] = (!own || AVG) ? strategy_scale<V, USEAVG>(sum[k], nd.nchild) : V(0);
+                    }
                 } else {
                     V xv[K];
 #pragma unroll
@@ -713,18 +744,27 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
             if constexpr (kJ == 1) __syncthreads();  // the bottom-up walk reads every leaf's values
 
             // ---- bottom-up walk over nodes [bu, end) ----
+            unpark();
             for (; bu < end; bu++) {
                 const BNode nd = S.tn[bu];
                 const int d = nd.depth;
                 close_to(d);
                 if (nd.kind == kBDecision) {
+                    // the parent (open at d - 1, or none at the root) moves to the stack
+                    if (open_top >= 0) {
+#pragma unroll
+                        for (int k = 0; k < K; k++) {
+                            acc[open_top][k] = tacc[k];
+                            Sb[open_top][k] = tsb[k];
+                        }
+                    }
                     open_top = d;
                     open_id[d] = bu;
                     const bool own = nd.actor == p;
                     V sum[K];
 #pragma unroll
                     for (int k = 0; k < K; k++) {
-                        acc[d][k] = (own && MODE == kBModeBR) ? neg_inf<V>() : V(0);
+                        tacc[k] = (own && MODE == kBModeBR) ? neg_inf<V>() : V(0);
                         sum[k] = V(0);
                     }
                     if (own && MODE != kBModeBR) {
@@ -738,16 +778,18 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                     }
 #pragma unroll
                     for (int k = 0; k < K; k++)
-                        Sb[d][k] = (own && MODE != kBModeBR) ? strategy_scale<V, USEAVG>(sum[k], nd.nchild) : V(0);
+                        tsb[k] = (own && MODE != kBModeBR) ? strategy_scale<V, USEAVG>(sum[k], nd.nchild) : V(0);
                 } else {
-                    // a leaf: its value goes straight to the parent (open at depth d - 1)
+                    // a leaf: its value goes straight to the parent (the innermost open node)
                     V xv[K];
                     ld_k<K>(S.X + (size_t)(nd.edge - g0) * kBRow, pos0, xv);
-                    deliver(nd.parent, nd.in_edge, d - 1, xv);
+                    deliver(nd.parent, nd.in_edge, xv);
                 }
             }
+            park();
             __syncthreads();  // X is rewritten by the next group
         }
+        unpark();
         close_to(0);
 
         // ---- outputs: root values and their range-weighted sum ----
