@@ -213,6 +213,7 @@ struct Smem {
     V *SC;    // [2][kBLists][48] inclusive scans of the card lists
     BNode *tn;
     uint16_t *leaf_node;
+    uint32_t *clpos;  // [kBLists][24] the card lists' positions, two per word (the pack's clpos)
     V *wsum;  // [32] warp partial sums
 };
 
@@ -225,6 +226,7 @@ __host__ __device__ inline size_t smem_bytes(int group) {
     b += 2 * (size_t)kBLists * 48 * sizeof(V);
     b += (size_t)kBMaxNodes * sizeof(BNode);
     b += (size_t)kBMaxLeaves * sizeof(uint16_t);
+    b += (size_t)kBLists * 48 * sizeof(uint16_t);
     b += 32 * sizeof(V);
     return (b + 15) & ~(size_t)15;
 }
@@ -245,6 +247,7 @@ __device__ inline Smem<V> carve(unsigned char *base, int group) {
     v += 32;
     S.tn = reinterpret_cast<BNode *>(v);
     S.leaf_node = reinterpret_cast<uint16_t *>(S.tn + kBMaxNodes);
+    S.clpos = reinterpret_cast<uint32_t *>(S.leaf_node + kBMaxLeaves);
     return S;
 }
 
@@ -367,6 +370,11 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
             const BNode nd = a.nodes[sub.node_off + i];
             S.tn[i] = nd;
             if (nd.kind != kBDecision) S.leaf_node[nd.edge] = (uint16_t)i;
+        }
+        // the card lists' positions, read by every leaf scan, staged once per subgame
+        {
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(&pk->clpos[0][0]);
+            for (int i = tid; i < kBLists * 24; i += NT) S.clpos[i] = __ldg(src + i);
         }
         __syncthreads();
         float *R = a.regrets + (size_t)sub.edge_off * kBRow;
@@ -634,8 +642,9 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
                         const int li = u - kBChunks64;
                         int c0 = 0, c1 = 0;
                         if (lane < kBListLen / 2) {
-                            c0 = pk->clpos[li][2 * lane];
-                            c1 = pk->clpos[li][2 * lane + 1];
+                            const uint32_t w = S.clpos[li * 24 + lane];
+                            c0 = w & 0xFFFF;
+                            c1 = w >> 16;
                         }
                         V a0[2], v[2];
 #pragma unroll
@@ -869,7 +878,7 @@ int batch_threads(int K) { return K == 2 ? Cfg<2>::NT : (K == 3 ? Cfg<3>::NT : C
 
 int batch_group_leaves(int fp64) { return fp64 ? 8 : 16; }
 
-int batch_dense_group() { return 10; }
+int batch_dense_group() { return 9; }
 
 size_t batch_smem_bytes(int K, int fp64, int group) {
     (void)K;

@@ -3,6 +3,7 @@
 // with per-hand regrets by one persistent kernel fed from a device work queue.
 #pragma once
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "batch_tree.h"
@@ -37,6 +38,8 @@ struct BPack {
     uint8_t list_card[48];
     uint16_t pos_of[1328];           // position of each colex hand (0xFFFF: blocked)
 };
+
+static_assert(offsetof(BPack, clpos) % 4 == 0 && sizeof(BPack) % 4 == 0, "card lists move as 4-byte words");
 
 enum { kBModeCFR = 0, kBModeBR = 1, kBModeEval = 2 };
 
