@@ -383,14 +383,6 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
         const float *rng = a.ranges + (size_t)s * 2 * kBRow;
         const int pos0 = tid * K;
         // this thread's hands' tie-group and card-list bounds, read once per subgame
-        uint32_t pgrp[K], plist[K], plist2[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            const int pq = pos0 + k < kBRow ? pos0 + k : kBRow - 1;
-            pgrp[k] = __ldg(&pk->grp[pq]);
-            plist[k] = __ldg(&pk->lists[pq]);
-            plist2[k] = __ldg(&pk->lists2[pq]);
-        }
 
         // walker state, per owned hand: depth-indexed stacks of the open path (indexed at run
         // time, so they live in local memory, cached in L1). Depth-major with the K hands of a
@@ -575,6 +567,16 @@ __global__ void __launch_bounds__(Cfg<K>::NT, MINB) batch_kernel(BLaunch a, int 
             __syncthreads();
 
             // ---- leaves of the group: opponent weights -> p's values ----
+            // this thread's hands' tie-group and card-list bounds (read here rather than kept
+            // in registers through the walks)
+            uint32_t pgrp[K], plist[K], plist2[K];
+    #pragma unroll
+            for (int k = 0; k < K; k++) {
+                const int pq = pos0 + k < kBRow ? pos0 + k : kBRow - 1;
+                pgrp[k] = __ldg(&pk->grp[pq]);
+                plist[k] = __ldg(&pk->lists[pq]);
+                plist2[k] = __ldg(&pk->lists2[pq]);
+            }
             // A job is a leaf, or a fold by p followed by its sibling call (a showdown): p's
             // actions leave the opponent weights unchanged, so one scan serves both leaves.
             // Jobs go kJ at a time. With kJ = 2 (buffers 0 and 1) their scans interleave and
