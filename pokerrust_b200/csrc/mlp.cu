@@ -8,7 +8,8 @@
 // Input per sample: both players' ranges over the 1326 hands, the 4 turn-board cards as a
 // 52-wide 0/1 vector, pot and stack scaled to [0, 1] (pot / 200, stack / (10 pot)).
 // Output: both players' counterfactual values per hand divided by the pot.
-// Shapes are padded for the GEMM tiles: input 2706 -> 2816 columns, output 2652 -> 2688.
+// Shapes are padded for the GEMM tiles: input 2706 -> 2816 columns, output 2652 -> 2816 (11
+// tiles of 256 columns; the padded weights and biases stay zero, as their gradients are zero).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -24,7 +25,7 @@ namespace mlp {
 
 using gemm::bf16;
 
-constexpr int kIn = 2706, kInPad = 2816, kHid = 1024, kOut = 2652, kOutPad = 2688;
+constexpr int kIn = 2706, kInPad = 2816, kHid = 1024, kOut = 2652, kOutPad = 2816;
 constexpr int kLayers = 5;
 constexpr int kK[kLayers] = {kInPad, kHid, kHid, kHid, kHid};       // padded fan-in
 constexpr int kN[kLayers] = {kHid, kHid, kHid, kHid, kOutPad};      // padded fan-out
@@ -417,7 +418,7 @@ struct Net {
         }
         if (e == cudaSuccess) {
             EpiBiasF32 epi{b[4], Y, kOutPad};
-            e = mm<128>(in, Wb[4], rows, kOutPad, kHid, epi);
+            e = mm<256>(in, Wb[4], rows, kOutPad, kHid, epi);
         }
         return check(e, "forward");
     }
