@@ -52,11 +52,17 @@ constexpr int kCPer = 6;               // card list slots per lane (8 lanes * 6 
 // sibling call (a showdown) leaves it, so that fold shares the showdown's channel: per
 // updater there are 9 showdown channels and 4 channels of folds by the opponent.
 constexpr int kNumCh = kNumSD + kNumFold / 2;
-// Opponent reach row: showdowns 0-8, pad, opponent folds 12-15; rows are 20 wide (80 bytes,
-// an odd number of 16-byte chunks) so that rows of different buckets start in all eight bank
-// groups, and only the first 16 values are loaded.
+// Opponent reach row: showdowns 0-8, pad, opponent folds 12-15 (16 values, four 16-byte
+// chunks). In double precision rows are 20 wide (an odd number of 16-byte chunks, so that rows
+// of different buckets start in all eight bank groups) and the first 16 values are loaded.
+// In single precision the rows are kept in kPioCopies interleaved copies: chunk k of bucket b
+// of copy q at chunk index (b * 4 + k) * 4 + q, which lies in bank group 4 (k & 1) + q whatever
+// the bucket. Lane position p of a quarter warp reads copy p & 3 and, for p >= 4, the chunks in
+// the order 1, 0, 3, 2, so the eight lanes of a quarter warp read eight bank groups at every
+// load (the gathers by data-dependent bucket otherwise conflict; see pio_row).
 constexpr int kPioW = 20;
 constexpr int kPioLoad = 16;
+constexpr int kPioCopies = 4;
 constexpr int kUFCol = 12;
 constexpr int kWownW = 20;             // updater reach row (CFR): showdowns 0-8, pad, the 8 folds 12-19
 constexpr int kFoldCol = 12;
@@ -110,7 +116,7 @@ __host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned gr
                                               unsigned acc = kNumLeaves) {
     Layout L;
     unsigned o = 0;
-    L.pio = take(&o, kBuckets * kPioW * vb);
+    L.pio = take(&o, vb == 4 ? kBuckets * kPioLoad * 4 * kPioCopies : kBuckets * kPioW * vb);
     L.wown = cfr ? take(&o, kBuckets * kWownW * 4) : 0;
     L.Pg = take(&o, (groups + 1) * kNumSD * vb);
     L.VG = take(&o, groups * kRowW * vb);
@@ -132,7 +138,7 @@ __host__ __device__ inline Layout make_layout(bool cfr, unsigned vb, unsigned gr
 
 template <typename V, int ACC = kNumLeaves>
 struct Smem {
-    V (*pio)[kPioW];             // opponent reach per bucket and channel
+    V *pio;                      // opponent reach per bucket and channel (layout: kPioW)
     float (*wown)[kWownW];       // updater reach * leaf scale per bucket and leaf (CFR)
     V (*Pg)[kNumSD];             // rank-list prefix sum at each tie group's start; [G] = total
     V (*VG)[kRowW];              // W - B of each rank-list tie group
@@ -150,7 +156,7 @@ struct Smem {
     int (*stage_key)[2];
 
     __device__ Smem(unsigned char *base, const Layout &L)
-        : pio(reinterpret_cast<V(*)[kPioW]>(base + L.pio)),
+        : pio(reinterpret_cast<V *>(base + L.pio)),
           wown(reinterpret_cast<float(*)[kWownW]>(base + L.wown)),
           Pg(reinterpret_cast<V(*)[kNumSD]>(base + L.Pg)),
           VG(reinterpret_cast<V(*)[kRowW]>(base + L.VG)),
@@ -192,6 +198,47 @@ __device__ __forceinline__ void load_row(const double *p, double *o, int n) {
     }
 }
 
+// Bucket b's opponent reach row (kPioLoad values). Single precision: this lane's copy, with
+// the chunk order of its half of the quarter warp, then the two halves' chunk pairs put back
+// in place (row value i of a swapped lane arrived at position i ^ 4).
+template <typename V, int ACC>
+__device__ __forceinline__ void pio_row(const Smem<V, ACC> &S, int b, V row[kPioLoad]) {
+    if constexpr (sizeof(V) == 4) {
+        const int q = threadIdx.x & 3;
+        const bool swap = (threadIdx.x >> 2) & 1;
+        const float4 *base = reinterpret_cast<const float4 *>(S.pio) + (size_t)b * (4 * kPioCopies) + q;
+        float raw[kPioLoad];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float4 t = base[(k ^ (swap ? 1 : 0)) * kPioCopies];
+            raw[4 * k] = t.x;
+            raw[4 * k + 1] = t.y;
+            raw[4 * k + 2] = t.z;
+            raw[4 * k + 3] = t.w;
+        }
+#pragma unroll
+        for (int i = 0; i < kPioLoad; i++) row[i] = swap ? raw[i ^ 4] : raw[i];
+    } else {
+        load_row(S.pio + (size_t)b * kPioW, row, kPioLoad);
+    }
+}
+
+// Writes bucket b's opponent reach row (kPioLoad values; every copy in single precision).
+template <typename V, int ACC>
+__device__ __forceinline__ void pio_store(Smem<V, ACC> &S, int b, const V row[kPioLoad]) {
+    if constexpr (sizeof(V) == 4) {
+        float4 *base = reinterpret_cast<float4 *>(S.pio) + (size_t)b * (4 * kPioCopies);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+#pragma unroll
+            for (int q = 0; q < kPioCopies; q++)
+                base[k * kPioCopies + q] = make_float4(row[4 * k], row[4 * k + 1], row[4 * k + 2], row[4 * k + 3]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < kPioW; i++) S.pio[(size_t)b * kPioW + i] = i < kPioLoad ? row[i] : V(0);
+    }
+}
+
 // x for all 13 channels of one list element (one bucket-row load).
 template <typename V, int ACC>
 __device__ __forceinline__ void elem_x(const Smem<V, ACC> &S, uint32_t e, V x[kNumCh]) {
@@ -199,7 +246,7 @@ __device__ __forceinline__ void elem_x(const Smem<V, ACC> &S, uint32_t e, V x[kN
     const int b = (e >> 11) & 255;
     const V rh = h != (int)kNoHand ? S.r[h] : V(0);
     V row[kPioLoad];
-    load_row(S.pio[b], row, kPioLoad);
+    pio_row(S, b, row);
 #pragma unroll
     for (int c = 0; c < kNumCh; c++) x[c] = rh * row[pio_col(c)];
 }
@@ -233,7 +280,7 @@ __device__ __forceinline__ int hand_values(const Smem<V, ACC> &S, const BoardPac
     for (int c = 0; c < kNumSD; c++) v[c] = g[c] - a1[c] - a2[c];  // (W - B): rank list minus card lists
     const V rh = S.r[h];
     V prow[kPioLoad], xf[kNumFold], ca[kNumFold], cb[kNumFold];
-    load_row(S.pio[b], prow, kPioLoad);
+    pio_row(S, b, prow);
 #pragma unroll
     for (int f = 0; f < kNumFold; f++) xf[f] = prow[pio_col(fold_channel(f, UPD))];
     cf_row(S.Cf, c1, ca);
@@ -324,20 +371,22 @@ __global__ void __launch_bounds__(NT, 1)
                 }
             }
         }
+        V prow[kPioLoad];
 #pragma unroll
-        for (int i = 0; i < kPioW; i++) S.pio[b][i] = V(0);
+        for (int i = 0; i < kPioLoad; i++) prow[i] = V(0);
 #pragma unroll
         for (int Lf = 0; Lf < kNumLeaves; Lf++) {
             const int s = kLeaf(Lf);
             const int col = Lf < kNumSD ? Lf : kFoldCol + (Lf - kNumSD);
             // showdowns and the opponent's folds; an updater's fold has its showdown's value
             if (Lf < kNumSD || leaf_channel(Lf, UPD) >= kNumSD)
-                S.pio[b][pio_col(leaf_channel(Lf, UPD))] = UPD == 0 ? pbb[s] : psb[s];
+                prow[pio_col(leaf_channel(Lf, UPD))] = UPD == 0 ? pbb[s] : psb[s];
             if constexpr (MODE == kModeCFR) {
                 S.wown[b][col] = float(updater == 0 ? psb[s] : pbb[s]) * leaf_scale(s, updater, bet);
                 S.abar[b][Lf] = 0.0f;
             }
         }
+        pio_store(S, b, prow);
         if constexpr (AVG) S.abar[b][kNumLeaves] = 0.0f;
         if constexpr (MODE == kModeCFR) {
 #pragma unroll
