@@ -83,8 +83,6 @@ class Pool {
         done_cv_.wait(lk, [this] { return active_ == 0; });
         job_ = nullptr;
     }
-    int size() const { return (int)workers_.size() + 1; }
-
   private:
     void loop() {
         uint64_t seen = 0;
@@ -904,6 +902,20 @@ int pr_game_get_regrets(void *game, float *upper, float *river) {
     if (int st = g->dt_pull()) return st;
     if (upper) memcpy(upper, g->regrets.data(), g->regrets.size() * sizeof(float));
     if (river) return pr_get_regrets(g->builder, river);
+    return 0;
+}
+
+int pr_game_set_regrets(void *game, const float *upper, const float *river) {
+    Game *g = (Game *)game;
+    if (!g) return 2;
+    if (upper)
+        for (size_t i = 0; i < g->regrets.size(); i++)
+            if (!std::isfinite(upper[i])) return 2;
+    if (int st = g->dt_pull()) return st;
+    if (river)
+        if (int st = pr_set_regrets(g->builder, river)) return st;
+    if (upper) memcpy(g->regrets.data(), upper, g->regrets.size() * sizeof(float));
+    g->dev_stale = true;
     return 0;
 }
 

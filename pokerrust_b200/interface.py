@@ -211,6 +211,8 @@ def lib():
         L.pr_game_load.argtypes = [vp, ctypes.c_char_p]
         L.pr_game_get_regrets.restype = i32
         L.pr_game_get_regrets.argtypes = [vp, vp, vp]
+        L.pr_game_set_regrets.restype = i32
+        L.pr_game_set_regrets.argtypes = [vp, vp, vp]
         L.pr_enable_average.restype = i32
         L.pr_enable_average.argtypes = [vp]
         L.pr_upload_own.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_float)]
@@ -529,6 +531,17 @@ class Game:
         riv = np.zeros((self.num_rivers, EDGES, BUCKETS), np.float32)
         _check(lib().pr_game_get_regrets(self.ptr, _ptr(up), _ptr(riv)), "pr_game_get_regrets")
         return up, riv
+
+    def set_regrets(self, upper=None, river=None):
+        """Replaces the upper-tree regrets and/or the river regrets (layouts of regrets())."""
+        up = None if upper is None else np.ascontiguousarray(upper, dtype=np.float32)
+        riv = None if river is None else np.ascontiguousarray(river, dtype=np.float32)
+        if up is not None:
+            assert up.shape == (lib().pr_game_upper_regret_count(self.ptr),)
+        if riv is not None:
+            assert riv.shape == (self.num_rivers, EDGES, BUCKETS)
+        _check(lib().pr_game_set_regrets(self.ptr, None if up is None else _ptr(up),
+                                         None if riv is None else _ptr(riv)), "pr_game_set_regrets")
 
     def enable_average(self):
         _check(lib().pr_game_enable_average(self.ptr), "pr_game_enable_average")

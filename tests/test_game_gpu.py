@@ -106,6 +106,33 @@ def test_checkpoint_round_trip(tmp_path):
     b.close()
 
 
+def test_set_regrets_round_trip():
+    import pokerrust_b200 as P
+    a = P.Game(O.REFERENCE_FLOP)
+    a.iterate(2)
+    up, riv = a.regrets()
+    b = P.Game(O.REFERENCE_FLOP)
+    b.set_regrets(up, riv)
+    ub, rb = b.regrets()
+    assert np.array_equal(up, ub) and np.array_equal(riv, rb)
+    # the next iteration from the same regrets is identical, on both upper-tree paths
+    a.iterate(1)
+    b.iterate(1)
+    assert np.array_equal(a.regrets()[0], b.regrets()[0]) and np.array_equal(a.regrets()[1], b.regrets()[1])
+    # either part alone; a NaN upper regret is refused and changes nothing
+    before = b.regrets()
+    bad = before[0].copy()
+    bad[0] = np.nan
+    with pytest.raises(P.PokerLibError):
+        b.set_regrets(bad, None)
+    after = b.regrets()
+    assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+    b.set_regrets(None, np.zeros_like(riv))
+    assert not b.regrets()[1].any() and np.array_equal(b.regrets()[0], before[0])
+    a.close()
+    b.close()
+
+
 def test_device_tree_matches_host_tree_bit_for_bit():
     """The device sweeps round every product like the host traversal and sum in the same
     order, so two iterations with average sums give identical regrets, sums and
