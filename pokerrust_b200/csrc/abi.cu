@@ -18,6 +18,7 @@
 #include "pack_boards.h"
 #include "river_cfr.h"
 #include "river_tree.h"
+#include "trace.h"
 
 namespace prb {
 namespace {
@@ -274,6 +275,7 @@ int sync_device(Builder *b) {
 
 int evaluate_impl(Builder *b, EvalTables *t, int player, int exploit, const float *d_in, float *d_out,
                   cudaStream_t stream, bool staged, const float *d_own = nullptr) {
+    prb::TraceRange trace(exploit ? "river pass (best response)" : "river pass (CFR)");
     if (!b || !t) return fail(kErrArg, "evaluate: null builder or tables");
     if (t->status) return fail(kErrTables, "evaluate: tables failed validation on upload");
     if (player != 0 && player != 1) return fail(kErrArg, "evaluate: updating_player must be 0 or 1");

@@ -16,6 +16,7 @@
 #include "batch_internal.h"
 #include "batch_solver.h"
 #include "device_common.cuh"
+#include "trace.h"
 
 namespace prb {
 namespace {
@@ -538,6 +539,7 @@ int pr_batch_set_linear_average(void *batch, int on) {
 }
 
 int pr_batch_iterate(void *batch, int iterations) {
+    prb::TraceRange trace("batch iterations");
     Batch *b = (Batch *)batch;
     if (!b || iterations < 0) return 2;
     if (b->graph && b->graph_avg != b->avg_on) {
@@ -581,6 +583,7 @@ int pr_batch_iterate(void *batch, int iterations) {
 // Best-response sums of both players per subgame, and exploitability = (BR0 + BR1) / 2 per
 // unit of joint range mass, in chips.
 int pr_batch_exploitability(void *batch, int use_average, int fp64, double *br0, double *br1, double *expl) {
+    prb::TraceRange trace("batch exploitability");
     Batch *b = (Batch *)batch;
     if (!b || (use_average && !b->avg_on)) return 2;
     std::vector<double> sums[2];
@@ -665,6 +668,7 @@ int pr_batch_iterate_noalloc(void *batch, int iterations) {
 // Subgame value V = r0^T U(sigma) r1 = sum_h r0(h) cfv0(h): player 0's expected chips times
 // the joint range mass, under the current or average strategies (double precision).
 int pr_batch_value(void *batch, int use_average, double *V) {
+    prb::TraceRange trace("batch value");
     Batch *b = (Batch *)batch;
     if (!b || !V || (use_average && !b->avg_on)) return 2;
     cudaError_t e = cudaMemsetAsync(b->d_head, 0, sizeof(int) * 4 * kClasses, b->stream);
@@ -680,6 +684,7 @@ int pr_batch_value(void *batch, int use_average, double *V) {
 // root; [count][8][1326], rows past the root's action count are zero). Two evaluation
 // passes; reach vectors are recomputed from the strategies, not stored per node.
 int pr_batch_value_grad(void *batch, int use_average, double *d_r0, double *d_r1, double *d_sigma) {
+    prb::TraceRange trace("batch value gradient");
     Batch *b = (Batch *)batch;
     if (!b || (use_average && !b->avg_on)) return 2;
     if (int st = ensure_hands_buffer(b)) return st;

@@ -28,6 +28,7 @@
 #include "batch_solver.h"
 #include "device_common.cuh"
 #include "full_tree.h"
+#include "trace.h"
 
 namespace prb {
 namespace {
@@ -796,6 +797,7 @@ int pr_full_pass(void *game, int player) {
 // CFR iterations (both players, alternating). Without a network each iteration is one
 // CUDA graph, captured on the first call.
 int pr_full_iterate(void *game, int iterations) {
+    prb::TraceRange trace("full game iterations");
     Game *g = (Game *)game;
     if (!g || iterations < 0) return 2;
     int it = 0;
@@ -840,6 +842,7 @@ int pr_full_iterate(void *game, int iterations) {
 // previous regrets and average sums are replaced; in plain mode, where they are part of the
 // solve, they are kept aside and restored afterwards.
 int pr_full_exploitability(void *game, int resolve_iterations, double *br0, double *br1, double *expl) {
+    prb::TraceRange trace("full game exploitability");
     Game *g = (Game *)game;
     if (!g || resolve_iterations < 0) return 2;
     // In plain mode the river subgames belong to the solve: their rows are kept aside during

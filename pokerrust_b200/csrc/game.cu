@@ -30,6 +30,7 @@
 
 #include "../../include/pokerrust_b200.h"
 #include "layout.h"
+#include "trace.h"
 #include "upper_tree.h"
 
 namespace prb {
@@ -803,6 +804,7 @@ void *pr_game_builder(void *game) { return game ? ((Game *)game)->builder : null
 void *pr_game_tables(void *game) { return game ? ((Game *)game)->tables : nullptr; }
 
 int pr_game_iterate(void *game, int iterations) {
+    prb::TraceRange trace("game iterations");
     Game *g = (Game *)game;
     if (!g) return 2;
     if (g->device_tree) return g->dt_iterate(iterations);
@@ -833,6 +835,7 @@ int pr_game_root_values(void *game, float *sb, float *bb) {
 }
 
 int pr_game_exploitability(void *game, int fp64, double *sum_sb, double *sum_bb, double *mbh) {
+    prb::TraceRange trace("game exploitability");
     Game *g = (Game *)game;
     if (!g) return 2;
     if (fp64) {

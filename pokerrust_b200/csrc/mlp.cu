@@ -19,6 +19,7 @@
 
 #include "../../include/pokerrust_b200.h"
 #include "mlp_gemm.cuh"
+#include "trace.h"
 
 namespace prb {
 namespace mlp {
@@ -587,6 +588,7 @@ int finish(Net *n) {
 // scalars [count][2]); out [count][2652] on the device. count <= rows.
 int pr_mlp_forward(void *net, const float *ranges, const uint64_t *boards, const float *scalars, float *out,
                    int count) {
+    prb::TraceRange trace("value network forward");
     Net *n = (Net *)net;
     if (!n || !ranges || !boards || !scalars || !out) return 2;
     if (int st = load_inputs(n, ranges, (const unsigned long long *)boards, scalars, count)) return st;
@@ -599,6 +601,7 @@ int pr_mlp_forward(void *net, const float *ranges, const uint64_t *boards, const
 // loss, backward, Adam (lr). loss: mean squared error before the update.
 int pr_mlp_train_step(void *net, const float *ranges, const uint64_t *boards, const float *scalars,
                       const float *targets, int count, float lr, double *loss) {
+    prb::TraceRange trace("value network training step");
     Net *n = (Net *)net;
     if (!n || !ranges || !boards || !scalars || !targets) return 2;
     if (int st = load_inputs(n, ranges, (const unsigned long long *)boards, scalars, count)) return st;

@@ -60,3 +60,19 @@ def test_error_strings_without_gpu(so_path):
     assert lib().pr_error_string(0) == b"ok"
     assert lib().pr_range_stride() == 1328
     assert lib().pr_river_smem_bytes(None, 0, 0) == 0      # no tables: nothing to size
+
+
+def test_null_handles_are_refused_without_gpu(so_path):
+    # the entry points check their arguments before any CUDA call (inside the trace range
+    # each one opens), so a null handle is refused with status 2 on a machine without a GPU
+    from pokerrust_b200 import lib
+    L = lib()
+    assert L.pr_evaluate(None, None, 0, 0) == 2
+    assert L.pr_batch_iterate(None, 1) == 2
+    assert L.pr_batch_value(None, 0, None) == 2
+    assert L.pr_game_iterate(None, 1) == 2
+    assert L.pr_full_iterate(None, 1) == 2
+    assert L.pr_mlp_forward(None, None, None, None, None, 0) == 2
+    assert L.pr_game_set_regrets(None, None, None) == 2
+    L.pr_clear_error()
+    assert L.pr_last_error() == 0
