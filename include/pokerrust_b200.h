@@ -184,7 +184,7 @@ size_t pr_game_upper_regret_count(void *game);
 int pr_game_get_regrets(void *game, float *upper, float *river);
 /* Replaces the upper-tree regrets and/or the river regrets (either pointer may be null; same
  * layouts as pr_game_get_regrets), e.g. to restore a state kept by the caller. Returns 2 for a
- * null game or a NaN or infinite upper regret (nothing is changed then). */
+ * null game or a NaN or infinite regret in either array (nothing is changed then). */
 int pr_game_set_regrets(void *game, const float *upper, const float *river);
 /* Average strategies for the whole game: upper-tree sums (per hand, regret layout) and
  * river sums (per bucket, pr_get_average layout) from the next iteration on. */

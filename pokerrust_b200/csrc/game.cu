@@ -914,6 +914,9 @@ int pr_game_set_regrets(void *game, const float *upper, const float *river) {
     if (upper)
         for (size_t i = 0; i < g->regrets.size(); i++)
             if (!std::isfinite(upper[i])) return 2;
+    if (river)
+        for (size_t i = 0, n = g->river_board.size() * 26 * 256; i < n; i++)
+            if (!std::isfinite(river[i])) return 2;
     if (int st = g->dt_pull()) return st;
     if (river)
         if (int st = pr_set_regrets(g->builder, river)) return st;

@@ -125,6 +125,10 @@ def test_set_regrets_round_trip():
     bad[0] = np.nan
     with pytest.raises(P.PokerLibError):
         b.set_regrets(bad, None)
+    bad_river = before[1].copy()
+    bad_river[5, 3, 7] = np.inf
+    with pytest.raises(P.PokerLibError):
+        b.set_regrets(before[0], bad_river)
     after = b.regrets()
     assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
     b.set_regrets(None, np.zeros_like(riv))
