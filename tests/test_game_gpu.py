@@ -115,11 +115,11 @@ def test_set_regrets_round_trip():
     b.set_regrets(up, riv)
     ub, rb = b.regrets()
     assert np.array_equal(up, ub) and np.array_equal(riv, rb)
-    # the next iteration from the same regrets is identical, on both upper-tree paths
+    # the next iteration from the same regrets is identical
     a.iterate(1)
     b.iterate(1)
     assert np.array_equal(a.regrets()[0], b.regrets()[0]) and np.array_equal(a.regrets()[1], b.regrets()[1])
-    # either part alone; a NaN upper regret is refused and changes nothing
+    # a NaN or infinite regret in either part is refused and changes nothing; either part alone
     before = b.regrets()
     bad = before[0].copy()
     bad[0] = np.nan
