@@ -45,6 +45,11 @@ WORKLOAD = "fixed-flop limit hold'em, all 27783 river subgames, one CFR pass per
 # DRAM bytes of one full river launch (27,783 subgames), read + write, from a single-pass ncu
 # capture of this program (dram__bytes_read.sum + dram__bytes_write.sum)
 TRAFFIC_PER_LAUNCH = 1063193600 + 509289984
+# The on-chip bound of the river pass: its shared-memory data pipe's share of peak
+# (l1tex__data_pipe_lsu_wavefronts_mem_shared.avg.pct_of_peak_sustained_elapsed) and
+# wavefronts per subgame-river card, from an ncu capture of the 4096-subgame case
+SMEM_PIPE_FRAC = 0.674
+SMEM_WAVEFRONTS_PER_RIVER_CARD = 2289425218 / (4096 * 48)
 
 
 def algorithmic_bytes(n):
@@ -713,7 +718,11 @@ def run_gpu(args):
                                            "launch of this program",
                          "peak_source": peak_kind,
                          "note": "algorithmic bytes per pass / kernel time; the pass is bound "
-                                 "on-chip (shared memory and issue), not by HBM"},
+                                 "on-chip (shared memory and issue), not by HBM",
+                         "onchip": {"bound": "shared-memory data pipe", "frac": SMEM_PIPE_FRAC,
+                                    "wavefronts_per_river_card": round(SMEM_WAVEFRONTS_PER_RIVER_CARD),
+                                    "source": "ncu l1tex__data_pipe_lsu_wavefronts_mem_shared, "
+                                              "one 4096-subgame CFR pass"}},
             "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": cpu_threads, "kind": "port",
                              "sample": f"{cpu_n} of {n} river subgames, one pass, "
                                        f"{cpu_dt:.2f} s, scaled to nodes/s"},
