@@ -67,6 +67,11 @@ void or_pack_flop_tables(uint64_t flop, uint16_t *eval, uint16_t *coll, uint16_t
                          int nthreads);
 
 /* --- river subtree --- */
+/* Order of the river cards within a river pass: 0 ascending (state.rs), 1 descending. The
+ * same sum in another f32 rounding, for measuring the trajectory's dependence on summation
+ * order. Applies to every later pass of every game and batch in the process. */
+void or_set_river_order(int descending);
+
 /* Describes the 28-state river tree in builder.cu order. For state s:
  * terminal[s] (0 NonTerminal, 1 SBWins, 2 BBWins, 3 Showdown, 4 River),
  * actor[s] (0 small, 1 big), parent[s], sb_raise[s], bb_raise[s] (bets minus the root bet),

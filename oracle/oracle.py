@@ -68,6 +68,7 @@ def load():
         L.or_board_tables.argtypes = [u64, vp, vp, vp]
         L.or_pack_flop_tables.argtypes = [u64, vp, vp, vp, i32]
         L.or_river_tree.argtypes = [vp] * 8
+        L.or_set_river_order.argtypes = [i32]
         L.or_river_batch.restype = i32
         L.or_river_batch.argtypes = [u64, vp, vp, i32, vp, vp, vp, vp, i32, i32, vp, i32]
         L.or_river_batch_avg.restype = i32
@@ -151,6 +152,12 @@ def pack_flop_tables(flop=REFERENCE_FLOP, nthreads=0):
     a = np.zeros(HANDS * HANDS, np.uint16)
     load().or_pack_flop_tables(int(flop), _p(e), _p(c), _p(a), nthreads)
     return e, c, a
+
+
+def set_river_order(descending):
+    """Visit the 48 river cards of every later river pass in descending order (True) or in
+    the reference's ascending order (False): the same sums in another f32 rounding."""
+    load().or_set_river_order(int(bool(descending)))
 
 
 def river_tree():

@@ -16,6 +16,12 @@
 
 namespace {
 
+// Order in which a river pass visits the 48 river cards: ascending (0, the order of
+// state.rs:377-433) or descending (1). Both give the same sum; the descending order changes
+// only the f32 rounding of the sums over rivers, which lets a test measure how far the game's
+// trajectory depends on summation order alone. Set by or_set_river_order.
+std::atomic<int> g_river_descending{0};
+
 enum Term { NonTerminal = 0, SBWins = 1, BBWins = 2, Showdown = 3, River = 4 };
 enum Act { Fold = 0, Check = 1, Call = 2, Raise = 3, DealRiver = 4 };
 enum Player { Small = 0, Big = 1 };
@@ -307,7 +313,9 @@ int river_one(uint64_t flop, const uint16_t *eval, const uint16_t *abstr, uint64
     Vec<T> own(OR_HANDS, T(1));
     int count = 0, err = 0;
     Board bd;
-    for (int rc = 0; rc < 52; rc++) {
+    const bool descending = g_river_descending.load(std::memory_order_relaxed) != 0;
+    for (int j = 0; j < 52; j++) {
+        const int rc = descending ? 51 - j : j;
         uint64_t rb = 1ull << rc;
         if (rb & board4) continue;
         count++;
@@ -374,6 +382,8 @@ int or_river_one_f64(uint64_t flop, const uint16_t *eval, const uint16_t *abstr,
     return river_one<double>(flop, eval, abstr, board4, bet, opp, nullptr, regrets, player, true,
                              out);
 }
+
+extern "C" void or_set_river_order(int descending) { g_river_descending.store(descending ? 1 : 0); }
 
 extern "C" void or_river_tree(int *terminal, int *actor, int *parent, float *sb_off,
                               float *bb_off, int *nchild, int *child, int *edge) {

@@ -1,11 +1,13 @@
 """Generates tests/golden/game_reference_flop_checkpoints.npz with the oracle (the CPU
 restatement of src/game.rs, src/state.rs and the river path): the fixed-flop game from zero
-regrets with average-strategy sums on, after 10 CFR iterations (game.rs:68-119):
+regrets with average-strategy sums on, after 1, 5 and 10 CFR iterations (game.rs:68-119):
   - exploitability in double precision (game.rs:120-178, formula at :175);
   - the root's values of the last iteration's SB and BB passes (per hand);
   - sums of all upper-tree and river regrets and average sums.
-About 25 minutes on 8 cores. Run from the repository root:
-    python tests/golden/make_game_checkpoints_golden.py [nthreads]
+With --descending the river passes visit the river cards in descending order (the same sums
+in another f32 rounding) and the file is game_reference_flop_checkpoints_descending.npz.
+About 30 minutes on 8 cores. Run from the repository root:
+    python tests/golden/make_game_checkpoints_golden.py [--descending] [nthreads]
 """
 import os
 import sys
@@ -17,11 +19,15 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
-CHECKPOINTS = (10,)
+CHECKPOINTS = (1, 5, 10)
 
 
 def main():
-    nthreads = int(sys.argv[1]) if len(sys.argv) > 1 else 0
+    args = sys.argv[1:]
+    descending = "--descending" in args
+    args = [a for a in args if a != "--descending"]
+    nthreads = int(args[0]) if args else 0
+    O.set_river_order(descending)
     t0 = time.time()
     g = O.Game(O.REFERENCE_FLOP, nthreads)
     g.enable_average()
@@ -34,7 +40,8 @@ def main():
             out[f"it{it}_root_values"] = g.root_values()
             out[f"it{it}_expl_f64"] = np.array(g.exploitability(True))
             print(it, out[f"it{it}_expl_f64"], f"{time.time() - t0:.0f}s", flush=True)
-    np.savez_compressed(os.path.join(ROOT, "tests", "golden", "game_reference_flop_checkpoints.npz"), **out)
+    name = "game_reference_flop_checkpoints_descending.npz" if descending else "game_reference_flop_checkpoints.npz"
+    np.savez_compressed(os.path.join(ROOT, "tests", "golden", name), **out)
 
 
 if __name__ == "__main__":

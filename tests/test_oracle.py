@@ -208,3 +208,25 @@ def test_game_structure():
     assert all(bin(int(b)).count("1") == 4 for b in boards[:100])
     # preflop raises +1 (bb 1 .. 4), flop +1, turn +2 (state.rs:128-132)
     assert set(np.unique(bets).tolist()) == set(float(x) for x in range(1, 17))
+
+
+def test_river_order_changes_only_the_rounding(flop_tables):
+    # the descending river order (or_set_river_order) sums the same 48 river values: the
+    # results agree to f32 rounding, and differ from the reference's order in some bits
+    rng = np.random.default_rng(4)
+    e, _, a = flop_tables
+    board4, bet, opp = _river_case(rng, 3, flop_tables)
+    reg0 = rng.random((3, 26, 256)).astype(np.float32) * 5
+    try:
+        out = {}
+        for descending in (False, True):
+            O.set_river_order(descending)
+            reg = reg0.copy()
+            v = O.river_batch(O.REFERENCE_FLOP, e, a, board4, bet, opp, reg, 0, False)
+            out[descending] = (v, reg)
+    finally:
+        O.set_river_order(False)
+    (va, ra), (vd, rd) = out[False], out[True]
+    assert np.abs(va - vd).max() <= 1e-5 * np.abs(va).max()
+    assert np.abs(ra - rd).max() <= 1e-5 * np.abs(ra).max()
+    assert not np.array_equal(va, vd)
