@@ -1,4 +1,4 @@
-"""The fixed-flop game after 10 and the stated 100 CFR iterations on the device
+"""The fixed-flop game after 1, 10 and the stated 100 CFR iterations on the device
 (pr_game_*), against the oracle's own runs of the same game (tests/golden/
 game_reference_flop_checkpoints.npz and game_reference_flop_100.npz, made by
 tests/golden/make_game_checkpoints_golden.py and make_game100_golden.py): FP64
@@ -7,16 +7,19 @@ the sums of the regrets and average sums above and inside the river subgames, an
 average sums of 64 sampled river roots.
 
 Tolerances. After one and two iterations the device and the oracle agree to about 1e-6 in
-every aggregate and 2.5e-6 per river root (test_game_gpu.py holds 1e-3 and 1e-4). From the
-third iteration on they part, and the cause is the reference's regret matching, not the
-arithmetic: where two actions tie, the regret is a cancellation residue whose sign depends on
-the summation order (after one iteration 129 of the 64 sampled roots' 425,984 river regrets
-are zero on one side and up to 0.027 on the other), and regret matching maps a zero sum to the
-uniform strategy but any sum above 1e-4 to a pure one (strategy.rs:138-146). Flipping such
-zero / residue pairs in the device's own state after one iteration, at that rate, moves its
-100-iteration exploitability by up to 7.8 % and its per-root average sums by 15-27 %; one-ulp
-changes of every positive river regret every ten iterations move the exploitability by up to
-13.5 %. So:
+every aggregate and 2.5e-6 per river root (held here to 1e-4 after one iteration, with
+exploitability to 1e-3; test_game_gpu.py checks two iterations). From the third iteration on
+they part, and the cause is the reference's regret matching, not the arithmetic: where two
+actions tie, the regret is a cancellation residue whose sign depends on the summation order
+(after one iteration 129 of the 64 sampled roots' 425,984 river regrets are zero on one side
+and up to 0.027 on the other), and regret matching maps a zero sum to the uniform strategy but
+any sum above 1e-4 to a pure one (strategy.rs:138-146). Flipping such zero / residue pairs in
+the device's own state after one iteration, at that rate, moves its 100-iteration
+exploitability by up to 7.8 % and its per-root average sums by 15-27 %; one-ulp changes of
+every positive river regret every ten iterations move the exploitability by up to
+13.5 %. The oracle against itself, with only the order of the 48 rivers in each sum reversed,
+has root values 2.1 % apart after five iterations (the device: 7.8 %) and 0.16 % after ten
+(tests/test_oracle.py). So:
 - root values and whole-game sums, which average that out, are held to the 1 % bound
   (measured: root values 6e-3 after 10 iterations, 1e-3 after 100; sums 4.5e-3);
 - FP64 exploitability of the current strategies is held to 5 % (measured 2.2 % after 10
@@ -41,6 +44,8 @@ GOLDEN_CHECKPOINTS = os.path.join(HERE, "game_reference_flop_checkpoints.npz")
 TOL_AGGREGATE = 1e-2
 TOL_EXPLOITABILITY = 5e-2
 TOL_ROOT_AVERAGE = 1e-1
+# checkpoints of the early run and their tolerances: exploitability, root values, sums
+EARLY = {1: (1e-3, 1e-4, 1e-4), 10: (TOL_EXPLOITABILITY, TOL_AGGREGATE, TOL_AGGREGATE)}
 
 
 def _load(path):
@@ -53,16 +58,17 @@ def rel(a, b):
     return abs(a - b) / max(abs(b), 1e-30)
 
 
-def _check(g, expl, root_want, totals_want, label):
+def _check(g, expl, root_want, totals_want, label, tols=(TOL_EXPLOITABILITY, TOL_AGGREGATE, TOL_AGGREGATE)):
+    tol_expl, tol_root, tol_sums = tols
     d1, d2, dm = g.exploitability(fp64=True)
     print(f"\n{label}: FP64 exploitability {dm:.4f} mb/h (oracle {expl[2]:.4f}), relative {rel(dm, expl[2]):.2e}")
-    assert rel(dm, expl[2]) < TOL_EXPLOITABILITY, (label, d1, d2, dm, expl)
+    assert rel(dm, expl[2]) < tol_expl, (label, d1, d2, dm, expl)
 
     root = g.root_values()
     for p in range(2):
         err = np.abs(root[p] - root_want[p]).max() / np.abs(root_want[p]).max()
         print(f"{label}: root values, player {p}: max error {err:.2e} of the largest value")
-        assert err < TOL_AGGREGATE, (label, p, err)
+        assert err < tol_root, (label, p, err)
 
     up, river = g.regrets()
     aup, ariver = g.average_sums()
@@ -71,22 +77,21 @@ def _check(g, expl, root_want, totals_want, label):
     for name, a, b in zip(("upper regrets", "upper average sums", "river regrets", "river average sums"),
                           got, totals_want):
         print(f"{label}: {name}: {a:.6e} (oracle {b:.6e})")
-        assert rel(a, b) < TOL_AGGREGATE, (label, name, a, b)
+        assert rel(a, b) < tol_sums, (label, name, a, b)
     return ariver
 
 
-def test_ten_iterations_match_the_oracle():
+def test_one_and_ten_iterations_match_the_oracle():
     import pokerrust_b200 as P
     golden = _load(GOLDEN_CHECKPOINTS)
     g = P.Game(O.REFERENCE_FLOP)
     g.enable_average()
     done = 0
-    for it in golden["checkpoints"]:
-        it = int(it)
+    for it, tols in sorted(EARLY.items()):
         g.iterate(it - done)
         done = it
         _check(g, golden[f"it{it}_expl_f64"], golden[f"it{it}_root_values"], golden[f"it{it}_totals"],
-               f"{it} iterations")
+               f"{it} iterations", tols)
     g.close()
 
 
