@@ -18,7 +18,8 @@ the device's own state after one iteration, at that rate, moves its 100-iteratio
 exploitability by up to 7.8 % and its per-root average sums by 15-27 %; one-ulp changes of
 every positive river regret every ten iterations move the exploitability by up to
 13.5 %. The oracle against itself, with only the order of the 48 rivers in each sum reversed,
-has root values 2.1 % apart after five iterations (the device: 7.8 %) and 0.16 % after ten
+has root values 2.1 % apart after five iterations (the device against the oracle: 7.8 %) and
+0.16 % after ten
 (tests/test_oracle.py). So:
 - root values and whole-game sums, which average that out, are held to the 1 % bound
   (measured: root values 6e-3 after 10 iterations, 1e-3 after 100; sums 4.5e-3);
