@@ -245,7 +245,7 @@ def batch_section(P, rank, peak, cpu_threads, with_cpu, traces):
 
 
 def adjoint_section(P, peak, cpu_threads, with_cpu):
-    """Config 3: the adjoint pair on 1024 general river subgames at their average strategies
+    """The adjoint pair on 1024 general river subgames at their average strategies
     after 100 CFR iterations. Forward V = r0^T U(sigma) r1 (pr_batch_value), backward dV/dr0,
     dV/dr1 and dV/dsigma at the root (pr_batch_value_grad), both through the C ABI with their
     host outputs; algorithmic bytes sum_s (2 E_s 1081 4 + 4 1081 4) per forward + backward."""
@@ -278,7 +278,7 @@ def adjoint_section(P, peak, cpu_threads, with_cpu):
         b.value_grad_device(d0, d1, ds, use_average=True)
     bwd_dev = (time.perf_counter() - t0) / reps
     nbytes = 2.0 * edges * 1081 * 4 + b.count * 4.0 * 1081 * 4
-    out = {"workload": "1024 river subgames (config-2 shapes), average strategies after 100 CFR iterations",
+    out = {"workload": "1024 general river subgames (random_subgames: pots 2-200, 1-3 bets and raises), average strategies after 100 CFR iterations",
            "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3, "backward_device_outputs_ms": bwd_dev * 1e3,
            "roofline": {"bound": "hbm", "achieved": nbytes / (fwd + bwd_dev) / 1e9, "peak": peak, "unit": "GB/s",
                         "frac": nbytes / (fwd + bwd_dev) / 1e9 / peak, "bytes_fwd_bwd": nbytes,
