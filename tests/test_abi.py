@@ -76,3 +76,26 @@ def test_null_handles_are_refused_without_gpu(so_path):
     assert L.pr_game_set_regrets(None, None, None) == 2
     L.pr_clear_error()
     assert L.pr_last_error() == 0
+
+
+@pytest.mark.parametrize("name", [
+    "pr_batch_exploitability", "pr_batch_tune", "pr_batch_get_all", "pr_batch_set_ranges",
+    "pr_batch_get_regrets", "pr_batch_set_linear_average", "pr_batch_enable_average",
+    "pr_batch_iterate_noalloc", "pr_batch_value_grad", "pr_full_exploitability", "pr_full_set_zero_sum",
+    "pr_full_set_net", "pr_full_tune", "pr_game_root_values", "pr_game_get_regrets", "pr_game_get_average",
+    "pr_game_enable_average", "pr_game_exploitability", "pr_mlp_train_step", "pr_mlp_get_layer",
+    "pr_mlp_set_layer", "pr_mlp_get_grad", "pr_get_regrets", "pr_set_regrets", "pr_upload_batch"])
+def test_every_handle_entry_point_refuses_null(so_path, name):
+    # null handle, null buffers, zero sizes: status 2 before any CUDA call
+    from pokerrust_b200 import lib
+    f = getattr(lib(), name)
+    args = [0.0 if t in (ctypes.c_float, ctypes.c_double) else (None if t is ctypes.c_void_p else 0)
+            for t in f.argtypes]
+    assert f(*args) == 2
+    lib().pr_clear_error()
+
+
+def test_setters_return_minus_one_for_a_null_handle(so_path):
+    from pokerrust_b200 import lib
+    assert lib().pr_game_set_device_tree(None, 1) == -1
+    assert lib().pr_mlp_set_persistent(None, 1) == -1
