@@ -360,11 +360,15 @@ typedef struct {
 } pr_full_spec;
 
 /* The flop and turn nodes on the host: 48-byte nodes in pre-order and the child list (see
- * full_tree.h for the layout); null outputs are skipped. 2 if the spec is bad or the
- * outputs are too small. */
+ * full_tree.h for the layout); null outputs are skipped. 2 if the spec is bad (a flop of
+ * other than 3 cards, a pot that is not positive and finite, a negative or infinite stack,
+ * fractions that are not positive and finite, street raises outside 0..4, river sizes
+ * outside bits 0-2 or none, river raises outside 1..3) or the outputs are too small. */
 int pr_full_tree(const pr_full_spec *spec, void *nodes_out, int max_nodes, int *num_nodes, int *num_edges,
                  int *num_leaves, int *kids_out, int max_kids);
-/* ranges: [2][1326] floats (hands touching the flop are ignored). Null on failure. */
+/* ranges: [2][1326] floats (hands touching the flop are ignored). Null on failure: a bad
+ * spec (as pr_full_tree), a range holding a NaN, an infinity or a negative weight, or an
+ * allocation that fails. */
 void *pr_full_new(const pr_full_spec *spec, const float *ranges);
 void pr_full_free(void *game);
 int pr_full_shape(void *game, int *num_nodes, int *num_edges, int *num_leaves, int *bet_subgames,

@@ -21,6 +21,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "../../include/pokerrust_b200.h"
@@ -495,6 +496,9 @@ bool rules_of(const pr_street &s, StreetRules *r) {
 bool build(const pr_full_spec *spec, int max_nodes, FullTree *t) {
     StreetRules fr, tr;
     if (!spec || !rules_of(spec->street[0], &fr) || !rules_of(spec->street[1], &tr)) return false;
+    // the river subgames' rules (pr_subgame.sizes and max_raises)
+    if ((spec->river_sizes & 7u) == 0 || (spec->river_sizes & ~7u) || spec->river_raises < 1 || spec->river_raises > 3)
+        return false;
     return build_full_tree(spec->flop, spec->pot, spec->stack, fr, tr, max_nodes, t);
 }
 
@@ -562,6 +566,11 @@ void *pr_full_new(const pr_full_spec *spec, const float *ranges) {
         ffail("pr_full_new: bad arguments");
         return nullptr;
     }
+    for (int i = 0; i < 2 * kH; i++)
+        if (!std::isfinite(ranges[i]) || ranges[i] < 0.0f) {
+            ffail("pr_full_new: a range holds a NaN, an infinity or a negative weight");
+            return nullptr;
+        }
     Game *g = new Game();
     g->spec = *spec;
     if (!build(spec, kMaxFullNodes, &g->tree)) {

@@ -23,6 +23,7 @@
 #pragma once
 #include <stdint.h>
 
+#include <cmath>
 #include <vector>
 
 namespace prb {
@@ -229,11 +230,13 @@ inline bool build_full_tree(uint64_t flop, float pot, float stack, const StreetR
     t->kids.clear();
     t->leaves.clear();
     t->num_edges = t->levels = 0;
-    if (__builtin_popcountll(flop) != 3 || (flop >> 52) || !(pot > 0.0f) || !(stack >= 0.0f)) return false;
+    if (__builtin_popcountll(flop) != 3 || (flop >> 52) || !(pot > 0.0f) || !(stack >= 0.0f) ||
+        !std::isfinite(pot) || !std::isfinite(stack))
+        return false;
     for (const StreetRules *r : {&flop_rules, &turn_rules}) {
         if (r->nfrac < 0 || r->nfrac > kFMaxFracs || r->max_raises < 0 || r->max_raises > 4) return false;
         for (int k = 0; k < r->nfrac; k++)
-            if (!(r->fracs[k] > 0.0f)) return false;
+            if (!(r->fracs[k] > 0.0f) || !std::isfinite(r->fracs[k])) return false;
     }
     fulltree_detail::Builder b{t, flop, {flop_rules, turn_rules}, max_nodes};
     const int root = b.add(kFDecision, 0, -1, 0, 0, flop);

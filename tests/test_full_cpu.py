@@ -62,6 +62,20 @@ def test_bad_specs_are_rejected():
         P.full_tree(P.full_spec(FLOP, 0.0, 100.0))    # no pot
     with pytest.raises(P.PokerLibError):
         P.full_tree(P.full_spec(FLOP, 10.0, -1.0))    # negative stack
+    bad = [P.full_spec(FLOP, float("nan"), 100.0), P.full_spec(FLOP, float("inf"), 100.0),
+           P.full_spec(FLOP, 10.0, float("inf")),                      # non-finite pot or stack
+           P.full_spec(FLOP, 10.0, 100.0, flop_fracs=(0.0,)), P.full_spec(FLOP, 10.0, 100.0, turn_fracs=(float("inf"),)),
+           P.full_spec(FLOP, 10.0, 100.0, flop_raises=5),              # street raises 0..4
+           P.full_spec(FLOP, 10.0, 100.0, river_sizes=0), P.full_spec(FLOP, 10.0, 100.0, river_sizes=0b1001),
+           P.full_spec(FLOP, 10.0, 100.0, river_raises=0), P.full_spec(FLOP, 10.0, 100.0, river_raises=4)]
+    for spec in bad:
+        with pytest.raises(P.PokerLibError):
+            P.full_tree(spec)
+    # the limits themselves are accepted
+    for spec in (P.full_spec(FLOP, 10.0, 0.0), P.full_spec(FLOP, 10.0, 100.0, flop_raises=4, turn_raises=0),
+                 P.full_spec(FLOP, 10.0, 100.0, river_sizes=0b111, river_raises=3),
+                 P.full_spec(FLOP, 10.0, 100.0, river_sizes=0b100, river_raises=1)):
+        P.full_tree(spec)
 
 
 def test_oracle_sweeps_zero_sum_and_best_response():
