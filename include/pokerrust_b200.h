@@ -206,9 +206,10 @@ int pr_game_load(void *game, const char *path);
  * Hands are colex indexes (1326; hands that touch the board are ignored). */
 typedef struct {
     uint64_t board;     /* 5 cards, bit i = card i (13 * suit + rank) */
-    float pot;          /* chips in the pot before the river, pot/2 from each player */
-    float stack;        /* chips behind each player */
-    uint32_t sizes;     /* bet sizes enabled: bit 0 half pot, bit 1 pot, bit 2 all-in */
+    float pot;          /* chips in the pot before the river, pot/2 from each player; > 0, finite */
+    float stack;        /* chips behind each player; >= 0, finite */
+    uint32_t sizes;     /* bet sizes enabled: bit 0 half pot, bit 1 pot, bit 2 all-in; at least
+                           one, no other bits */
     int32_t max_raises; /* bets + raises on the river, 1..3 */
 } pr_subgame;
 

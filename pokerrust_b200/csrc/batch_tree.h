@@ -20,6 +20,7 @@
 #pragma once
 #include <stdint.h>
 
+#include <cmath>
 #include <vector>
 
 namespace prb {
@@ -54,7 +55,9 @@ inline bool build_bet_tree(float pot, float stack, uint32_t sizes, int max_raise
     t->nodes.clear();
     t->edge_owner.clear();
     t->num_edges = t->num_leaves = t->depth = 0;
-    if (!(pot > 0.0f) || !(stack >= 0.0f) || (sizes & 7u) == 0 || max_raises < 1) return false;
+    if (!(pot > 0.0f) || !(stack >= 0.0f) || !std::isfinite(pot) || !std::isfinite(stack) || (sizes & 7u) == 0 ||
+        (sizes & ~7u) || max_raises < 1)
+        return false;
     struct St {
         float c[2];    // river chips of each player
         int actor, raises;

@@ -52,6 +52,18 @@ def test_tree_matches_oracle(seed):
     assert checked > 100
 
 
+def test_bad_subgame_specs_are_refused():
+    # pot positive and finite, stack non-negative and finite, a bet size among bits 0-2,
+    # 1..3 bets and raises
+    for pot, stack, sizes, raises in [(0.0, 10.0, 3, 2), (float("nan"), 10.0, 3, 2), (float("inf"), 10.0, 3, 2),
+                                      (10.0, -1.0, 3, 2), (10.0, float("inf"), 3, 2), (10.0, 100.0, 0, 2),
+                                      (10.0, 100.0, 8, 2), (10.0, 100.0, 11, 2), (10.0, 100.0, 3, 0),
+                                      (10.0, 100.0, 3, 4)]:
+        with pytest.raises(P.PokerLibError):
+            P.bet_tree(pot, stack, sizes, raises)
+    P.bet_tree(10.0, 0.0, 1, 1)  # no chips behind: checks to the showdown
+
+
 def test_generator_shapes():
     specs, ranges = P.random_subgames(64, seed=3)
     assert ranges.shape == (64, 2, 1326)
